@@ -1,0 +1,215 @@
+"""ctypes binding of libdeepgreen.so (include/deepgreen.h).
+
+Loads the in-tree library built by ``make -C deep-green_b200``.  There is no
+fallback: if the library or a CUDA device is missing, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+PKG_ROOT = Path(__file__).resolve().parents[2]          # deep-green_b200/
+LIB_PATH = PKG_ROOT / "lib" / "libdeepgreen.so"
+HEADER_PATH = PKG_ROOT.parent / "include" / "deepgreen.h"
+
+DG_OK = 0
+DG_ERR_INVALID = -1
+DG_ERR_CUDA = -2
+DG_ERR_NO_STATE = -3
+DG_ERR_TIMEOUT = -4
+DG_ERR_NO_DEVICE = -5
+
+PERIODIC, OUTFLOW, WALL = 0, 1, 2
+LIMITER_NONE, LIMITER_MINMOD = 0, 1
+F32, F64 = 0, 1
+STATUS_NONFINITE = 0x1
+STATUS_TIMEOUT = 0x2
+
+
+class SimInfo(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
+        ("nghosts", ctypes.c_int32),
+        ("ds", ctypes.c_double), ("gamma", ctypes.c_double), ("cfl", ctypes.c_double),
+        ("g", ctypes.c_double),
+        ("bcs", ctypes.c_int32 * 6),
+        ("gravity", ctypes.c_int32), ("limiter", ctypes.c_int32),
+        ("precision", ctypes.c_int32), ("device", ctypes.c_int32),
+    ]
+
+
+class DgError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"deepgreen error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+# (name, argtypes) of every entry point the header declares
+_P = ctypes.c_void_p
+_I = ctypes.c_int32
+_PP5 = ctypes.c_void_p * 5
+SIGNATURES = {
+    "dg_abi_version": [],
+    "dg_create": [ctypes.POINTER(SimInfo), ctypes.POINTER(ctypes.c_void_p)],
+    "dg_destroy": [_P],
+    "dg_set_primitives": [_P, _PP5],
+    "dg_set_conserved": [_P, _PP5],
+    "dg_compute_step": [_P, _I, ctypes.POINTER(ctypes.c_double)],
+    "dg_get_conserved": [_P, _PP5],
+    "dg_get_primitives": [_P, _PP5],
+    "dg_conservation_sums": [_P, ctypes.POINTER(ctypes.c_double)],
+    "dg_set_conserved_device": [_P, _PP5],
+    "dg_get_conserved_device": [_P, _PP5],
+    "dg_enqueue_steps": [_P, _I],
+    "dg_get_dts": [_P, _I, ctypes.POINTER(ctypes.c_double)],
+    "dg_synchronize": [_P],
+    "dg_get_stream": [_P, ctypes.POINTER(ctypes.c_void_p)],
+    "dg_step_launch_shape": [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)],
+    "dg_set_chunk": [_P, _I],
+    "dg_status": [_P, ctypes.POINTER(ctypes.c_uint32)],
+    "dg_last_error": [_P],
+}
+
+
+def load(path: os.PathLike | None = None):
+    """Load libdeepgreen.so once and declare every signature."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise FileNotFoundError(f"{p} not built; run `make -C {PKG_ROOT}` (no CPU fallback exists)")
+    lib = ctypes.CDLL(str(p))
+    for name, args in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = ctypes.c_char_p if name == "dg_last_error" else ctypes.c_int32
+    _lib = lib
+    return lib
+
+
+def _ptrs(arrays):
+    return _PP5(*[a.ctypes.data for a in arrays])
+
+
+class Context:
+    """Owner of one dg_ctx (one grid on one device)."""
+
+    def __init__(self, shape, ds, bcs, gamma=5.0 / 3.0, cfl=0.2, g=-0.1, gravity=False,
+                 limiter=LIMITER_NONE, precision=F32, device=0):
+        self.lib = load()
+        self.shape = tuple(int(s) for s in shape)
+        self.n = tuple(s + 4 for s in self.shape)
+        self.dtype = np.float64 if precision == F64 else np.float32
+        info = SimInfo()
+        info.nx, info.ny, info.nz = self.shape
+        info.nghosts = 2
+        info.ds, info.gamma, info.cfl, info.g = float(ds), float(gamma), float(cfl), float(g)
+        for i, b in enumerate(bcs):
+            info.bcs[i] = int(b)
+        info.gravity = int(bool(gravity))
+        info.limiter = int(limiter)
+        info.precision = int(precision)
+        info.device = int(device)
+        self.info = info
+        h = ctypes.c_void_p()
+        rc = self.lib.dg_create(ctypes.byref(info), ctypes.byref(h))
+        if rc != DG_OK:
+            raise DgError(rc, self.lib.dg_last_error(None).decode())
+        self.h = h
+
+    # -- helpers -------------------------------------------------------------
+    def _check(self, rc):
+        if rc != DG_OK:
+            raise DgError(rc, self.lib.dg_last_error(self.h).decode())
+
+    def _fields(self, fields):
+        out = []
+        for a in fields:
+            a = np.ascontiguousarray(a, dtype=self.dtype)
+            if a.shape != self.n:
+                raise ValueError(f"field shape {a.shape} != {self.n}")
+            out.append(a)
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.dg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- state ---------------------------------------------------------------
+    def set_primitives(self, prim):
+        prim = self._fields(prim)
+        self._check(self.lib.dg_set_primitives(self.h, _ptrs(prim)))
+
+    def set_conserved(self, cons):
+        cons = self._fields(cons)
+        self._check(self.lib.dg_set_conserved(self.h, _ptrs(cons)))
+
+    def get_conserved(self):
+        out = [np.empty(self.n, dtype=self.dtype) for _ in range(5)]
+        self._check(self.lib.dg_get_conserved(self.h, _ptrs(out)))
+        return out
+
+    def get_primitives(self):
+        out = [np.empty(self.n, dtype=self.dtype) for _ in range(5)]
+        self._check(self.lib.dg_get_primitives(self.h, _ptrs(out)))
+        return out
+
+    def set_conserved_device(self, ptrs):
+        self._check(self.lib.dg_set_conserved_device(self.h, _PP5(*ptrs)))
+
+    def get_conserved_device(self, ptrs):
+        self._check(self.lib.dg_get_conserved_device(self.h, _PP5(*ptrs)))
+
+    # -- stepping ------------------------------------------------------------
+    def compute_step(self, nsteps=1):
+        dts = np.zeros(max(nsteps, 1), dtype=np.float64)
+        self._check(self.lib.dg_compute_step(self.h, int(nsteps),
+                                             dts.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return dts[:nsteps]
+
+    def enqueue_steps(self, nsteps):
+        self._check(self.lib.dg_enqueue_steps(self.h, int(nsteps)))
+
+    def get_dts(self, nsteps):
+        dts = np.zeros(max(nsteps, 1), dtype=np.float64)
+        self._check(self.lib.dg_get_dts(self.h, int(nsteps), dts.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return dts[:nsteps]
+
+    def synchronize(self):
+        self._check(self.lib.dg_synchronize(self.h))
+
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        self._check(self.lib.dg_get_stream(self.h, ctypes.byref(s)))
+        return s.value or 0
+
+    def launch_shape(self):
+        b, t, c = _I(), _I(), _I()
+        self._check(self.lib.dg_step_launch_shape(self.h, ctypes.byref(b), ctypes.byref(t), ctypes.byref(c)))
+        return b.value, t.value, c.value
+
+    def set_chunk(self, chunk):
+        self._check(self.lib.dg_set_chunk(self.h, int(chunk)))
+
+    def conservation_sums(self):
+        out = np.zeros(5, dtype=np.float64)
+        self._check(self.lib.dg_conservation_sums(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return out
+
+    def status(self) -> int:
+        f = ctypes.c_uint32()
+        self._check(self.lib.dg_status(self.h, ctypes.byref(f)))
+        return f.value

@@ -1,0 +1,154 @@
+"""Initial states of the workloads this library is measured and checked on.
+
+All generators return the five primitive fields (rho, vx, vy, vz, p) as
+FP64 arrays of the ghosted shape (n+4 per axis), filled on every cell
+(ghosts included, as the reference's init_* functions do, e.g.
+src/rs/src/init.rs:401-444); only interior values matter because ghosts are
+refilled by the boundary rules.  Cell centres of interior cell i are at
+(i - 2 + 1/2) * ds from the lower domain edge.
+
+Workloads
+  kelvin_helmholtz   3D KH shear layer, periodic unit box (gamma 1.4)
+  sod                3D Sod shock tube along x, outflow on all faces
+  isentropic_vortex  Shu's isentropic vortex advected along (1, 1, 0),
+                     periodic box [-5, 5]^3, strength 5
+  riemann_random     random two-state Riemann problem split by a plane
+The reference's own KH set-up shears in z and has no noise; these follow
+the workload definitions instead (shear in y, seeded noise).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+PERIODIC, OUTFLOW, WALL = 0, 1, 2
+
+_MASK64 = (1 << 64) - 1
+
+
+def splitmix64(x: np.ndarray) -> np.ndarray:
+    """SplitMix64 finaliser on uint64 arrays (Steele, Lea & Flood 2014)."""
+    x = (x + np.uint64(0x9E3779B97F4A7C15)) & np.uint64(_MASK64)
+    x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return x ^ (x >> np.uint64(31))
+
+
+def counter_uniform(seed: int, index: np.ndarray, comp: int) -> np.ndarray:
+    """Uniform [0, 1) from (seed, cell index, component), counter-based."""
+    with np.errstate(over="ignore"):
+        key = np.uint64(seed & _MASK64) * np.uint64(0x9E3779B97F4A7C15) + index.astype(np.uint64) * np.uint64(3) \
+            + np.uint64(comp)
+        r = splitmix64(key)
+    return (r >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
+def centres(n_int: int, ds: float, lo: float = 0.0) -> np.ndarray:
+    """Cell-centre coordinates of all n_int + 4 ghosted cells along an axis."""
+    return lo + (np.arange(n_int + 4, dtype=np.float64) - 2 + 0.5) * ds
+
+
+def kelvin_helmholtz(n: int = 64, seed: int = 1, noise: float = 1e-3, ny: int | None = None,
+                     nz: int | None = None):
+    """KH layer: rho=2, vx=+0.5 for |y-0.5|<0.25, else rho=1, vx=-0.5;
+    p=2.5; vy=0.01 sin(4 pi x)(exp(-(y-0.25)^2/0.005)+exp(-(y-0.75)^2/0.005));
+    vz=0; plus uniform noise in [-noise, noise] on vx, vy, vz.
+    Returns (prims, ds, bcs)."""
+    ny = ny or n
+    nz = nz or n
+    ds = 1.0 / n
+    x = centres(n, ds)[:, None, None]
+    y = centres(ny, ds)[None, :, None]
+    shape = (n + 4, ny + 4, nz + 4)
+    inner = np.abs(y - 0.5) < 0.25
+    rho = np.broadcast_to(np.where(inner, 2.0, 1.0), shape).copy()
+    vx = np.broadcast_to(np.where(inner, 0.5, -0.5), shape).copy()
+    vy = np.broadcast_to(0.01 * np.sin(4 * np.pi * x) * (np.exp(-(y - 0.25) ** 2 / 0.005)
+                                                          + np.exp(-(y - 0.75) ** 2 / 0.005)), shape).copy()
+    vz = np.zeros(shape)
+    p = np.full(shape, 2.5)
+    if noise:
+        # noise indexed by interior cell (i, j, k) -> (i*ny + j)*nz + k
+        ii = np.arange(shape[0])[:, None, None] - 2
+        jj = np.arange(shape[1])[None, :, None] - 2
+        kk = np.arange(shape[2])[None, None, :] - 2
+        idx = ((np.mod(ii, n) * ny + np.mod(jj, ny)) * nz + np.mod(kk, nz)).astype(np.int64)
+        idx = np.broadcast_to(idx, shape)
+        for comp, v in enumerate((vx, vy, vz)):
+            v += noise * (2.0 * counter_uniform(seed, idx, comp) - 1.0)
+    return [rho, vx, vy, vz, p], ds, (PERIODIC,) * 6
+
+
+def sod(n: int = 64, ny: int | None = None, nz: int | None = None):
+    """rho=1, p=1 for x<0.5; rho=0.125, p=0.1 otherwise; v=0; outflow."""
+    ny = ny or n
+    nz = nz or n
+    ds = 1.0 / n
+    x = centres(n, ds)[:, None, None]
+    shape = (n + 4, ny + 4, nz + 4)
+    left = np.broadcast_to(x < 0.5, shape)
+    rho = np.where(left, 1.0, 0.125)
+    p = np.where(left, 1.0, 0.1)
+    z = np.zeros(shape)
+    return [rho, z.copy(), z.copy(), z.copy(), p], ds, (OUTFLOW,) * 6
+
+
+def isentropic_vortex(n: int = 64, beta: float = 5.0, gamma: float = 1.4, ny: int | None = None,
+                      nz: int | None = None, half_width: float = 5.0):
+    """Shu's isentropic vortex (tube along z) on [-L, L]^3, background
+    rho=1, p=1, v=(1, 1, 0), periodic."""
+    ny = ny or n
+    nz = nz or n
+    ds = 2.0 * half_width / n
+    x = centres(n, ds, -half_width)[:, None, None]
+    y = centres(ny, ds, -half_width)[None, :, None]
+    shape = (n + 4, ny + 4, nz + 4)
+    r2 = x * x + y * y
+    e = np.exp(0.5 * (1.0 - r2))
+    du = -beta / (2 * np.pi) * e * y
+    dv = beta / (2 * np.pi) * e * x
+    T = 1.0 - (gamma - 1.0) * beta * beta / (8.0 * gamma * np.pi * np.pi) * e * e
+    rho = np.broadcast_to(T ** (1.0 / (gamma - 1.0)), shape).copy()
+    p = rho ** gamma
+    vx = np.broadcast_to(1.0 + du, shape).copy()
+    vy = np.broadcast_to(1.0 + dv, shape).copy()
+    vz = np.zeros(shape)
+    return [rho, vx, vy, vz, p], ds, (PERIODIC,) * 6
+
+
+def riemann_random(shape, seed: int, bcs=(OUTFLOW,) * 6):
+    """Two constant states split by a plane through a random point with a
+    random unit normal; rho, p log-uniform in [0.1, 10], velocities uniform
+    in [-1, 1].  ``shape`` is the interior shape; the box is [0, shape*ds]
+    with ds = 1 / max(shape)."""
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = shape
+    ds = 1.0 / max(shape)
+    states = []
+    for _ in range(2):
+        rho = float(np.exp(rng.uniform(np.log(0.1), np.log(10.0))))
+        p = float(np.exp(rng.uniform(np.log(0.1), np.log(10.0))))
+        v = rng.uniform(-1.0, 1.0, 3)
+        states.append((rho, v, p))
+    point = rng.uniform(0.25, 0.75, 3) * np.array(shape) * ds
+    normal = rng.normal(size=3)
+    normal /= np.linalg.norm(normal)
+    x = centres(nx, ds)[:, None, None]
+    y = centres(ny, ds)[None, :, None]
+    z = centres(nz, ds)[None, None, :]
+    side = ((x - point[0]) * normal[0] + (y - point[1]) * normal[1] + (z - point[2]) * normal[2]) < 0
+    full = (nx + 4, ny + 4, nz + 4)
+    side = np.broadcast_to(side, full)
+    (r0, v0, p0), (r1, v1, p1) = states
+    prim = [np.where(side, r0, r1), np.where(side, v0[0], v1[0]), np.where(side, v0[1], v1[1]),
+            np.where(side, v0[2], v1[2]), np.where(side, p0, p1)]
+    return prim, ds, tuple(bcs)
+
+
+def conserved_from_primitives(prim, ds, gamma):
+    """calc_conserved (src/rs/src/physics.rs:143-175) in NumPy, any dtype."""
+    rho, vx, vy, vz, p = prim
+    T = rho.dtype.type
+    V = T(ds) * T(ds) * T(ds)
+    gm1 = T(gamma) - T(1.0)
+    return [rho * V, vx * rho * V, vy * rho * V, vz * rho * V,
+            V * (rho * (vx * vx + vy * vy + vz * vz) / T(2.0) + p / gm1)]

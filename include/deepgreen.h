@@ -1,0 +1,153 @@
+/*
+ * deepgreen.h -- C ABI of the B200 implementation of deep-green's 3D
+ * compressible Euler finite-volume step.
+ *
+ * The reference exposes its step as Rust free functions over a host-side
+ * grid (deep-green src/rs/src/physics.rs and grid.rs).  This header is the
+ * boundary a Rust `-sys` crate (or ctypes, cgo, ...) binds instead:
+ *
+ *   reference (src/rs/src/...)                     this ABI
+ *   ---------------------------------------------  -----------------------------
+ *   Simulation::new            grid.rs:44-76        dg_sim_info + dg_create
+ *   SimulationGrid::new        grid.rs:169-221      dg_create (device buffers)
+ *   calc_conserved             physics.rs:143-175   dg_set_primitives
+ *   grid.conserved.* (write)   grid.rs:87-93        dg_set_conserved
+ *   update_primitive_ghost_cells grid.rs:121-135    applied inside every call
+ *   compute_step               physics.rs:595-681   dg_compute_step
+ *   grid.conserved.* (read)    grid.rs:87-93        dg_get_conserved
+ *   grid.primitives.* (read)   grid.rs:95-101       dg_get_primitives
+ *
+ * Conventions (all functions):
+ *   - return int32_t: DG_OK (0) or a negative DG_ERR_* code; nothing throws
+ *     across the ABI; dg_last_error() gives a message for the last failure.
+ *   - host arrays are C-order (x slowest, z fastest) with the reference's
+ *     two ghost layers: (nx+4) x (ny+4) x (nz+4) elements, float or double
+ *     as dg_sim_info.precision says.  Conserved fields hold per-cell totals
+ *     (mass = rho * ds^3, ...), as the reference's Conserved does.
+ *   - one context = one device + one CUDA stream; do not call one context
+ *     from two host threads at once (the reference's SimulationGrid is not
+ *     shared either).  State stays on the device between calls.
+ *   - Every kernel runs on the GPU; there is no CPU path.  A call made
+ *     where the device or the kernels are unavailable returns an error.
+ */
+#ifndef DEEPGREEN_H
+#define DEEPGREEN_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DG_ABI_VERSION 1
+
+/* status codes */
+#define DG_OK 0
+#define DG_ERR_INVALID (-1)   /* bad argument or unsupported configuration */
+#define DG_ERR_CUDA (-2)      /* CUDA runtime/driver error */
+#define DG_ERR_NO_STATE (-3)  /* step or read before any state was set */
+#define DG_ERR_TIMEOUT (-4)   /* a bounded device-side wait gave up */
+#define DG_ERR_NO_DEVICE (-5) /* no usable sm_100 device */
+
+/* BoundaryType, grid.rs:23-28 (same order). Faces: x-, x+, y-, y+, z-, z+. */
+#define DG_BC_PERIODIC 0
+#define DG_BC_OUTFLOW 1
+#define DG_BC_WALL 2
+
+/* slope limiter: NONE = the reference's central slopes (physics.rs:198-215);
+ * MINMOD is an addition of this library */
+#define DG_LIMITER_NONE 0
+#define DG_LIMITER_MINMOD 1
+
+#define DG_F32 0
+#define DG_F64 1
+
+/* status flags (dg_status) */
+#define DG_STATUS_NONFINITE 0x1u  /* a NaN wave speed was seen; dt fell back to cfl*1.0
+                                     as calc_timestep does (physics.rs:191-195) */
+#define DG_STATUS_TIMEOUT 0x2u    /* a device-side wait ran out; results invalid */
+
+/* Runtime form of Simulation (grid.rs:30-41) plus the constants the
+ * reference keeps as statics (globals.rs:3-8). */
+typedef struct dg_sim_info {
+    int32_t nx, ny, nz;  /* interior cells per axis (>= 2), the arguments of
+                            Simulation::new before it adds the ghosts */
+    int32_t nghosts;     /* must be 2 (physics.rs:14) */
+    double ds;           /* uniform cell size */
+    double gamma;        /* globals::GAMMA */
+    double cfl;          /* globals::CFL */
+    double g;            /* globals::G, used when gravity != 0 */
+    int32_t bcs[6];      /* DG_BC_*, Simulation::bcs; periodic faces come in pairs */
+    int32_t gravity;     /* Simulation::gravity: z-sweep source, physics.rs:366-372 */
+    int32_t limiter;     /* DG_LIMITER_* */
+    int32_t precision;   /* DG_F32 or DG_F64 */
+    int32_t device;      /* CUDA device ordinal */
+} dg_sim_info;
+
+typedef struct dg_ctx dg_ctx;
+
+/* ABI version of the loaded library (DG_ABI_VERSION). */
+int32_t dg_abi_version(void);
+
+/* Simulation::new + SimulationGrid::new: validates info and allocates the
+ * device state.  *out is NULL on failure. */
+int32_t dg_create(const dg_sim_info *info, dg_ctx **out);
+int32_t dg_destroy(dg_ctx *ctx);
+
+/* Primitive fields (rho, vx, vy, vz, p) in; computes the conserved state on
+ * the device exactly as calc_conserved (physics.rs:143-175).  Ghost values
+ * of the input are ignored: ghosts are refilled by the boundary rules. */
+int32_t dg_set_primitives(dg_ctx *ctx, const void *const prim[5]);
+/* Conserved fields (mass, mom_x, mom_y, mom_z, energy) in. */
+int32_t dg_set_conserved(dg_ctx *ctx, const void *const cons[5]);
+
+/* compute_step (physics.rs:595-681) repeated nsteps times on the device.
+ * dt of every step (computed from the state at the start of that step, as
+ * calc_timestep does) is written to dts[0..nsteps-1] when dts is non-NULL.
+ * Blocks until the steps are done. */
+int32_t dg_compute_step(dg_ctx *ctx, int32_t nsteps, double *dts);
+
+/* Conserved state after the last step, ghosts filled by the boundary rules. */
+int32_t dg_get_conserved(dg_ctx *ctx, void *const cons[5]);
+/* Primitive fields as SimulationGrid::primitives holds them after
+ * compute_step returns: the state at the START of the last step (the
+ * reference converts before it updates), ghosts filled.  Before any step:
+ * the primitives of the current state. */
+int32_t dg_get_primitives(dg_ctx *ctx, void *const prim[5]);
+
+/* FP64 sums over interior cells of the five conserved fields of the current
+ * state (global mass, momentum and energy). */
+int32_t dg_conservation_sums(dg_ctx *ctx, double out[5]);
+
+/* Device-pointer variants of dg_set_conserved / dg_get_conserved for
+ * callers that keep the fields in their own CUDA allocations (same layout
+ * as the host arrays; ordered on the context's stream). */
+int32_t dg_set_conserved_device(dg_ctx *ctx, const void *const cons[5]);
+int32_t dg_get_conserved_device(dg_ctx *ctx, void *const cons[5]);
+
+/* Asynchronous stepping: enqueue nsteps steps on the context's stream and
+ * return at once.  dg_get_dts then reads the dt of the last nsteps steps
+ * (nsteps <= 4096) after synchronizing. */
+int32_t dg_enqueue_steps(dg_ctx *ctx, int32_t nsteps);
+int32_t dg_get_dts(dg_ctx *ctx, int32_t nsteps, double *dts);
+int32_t dg_synchronize(dg_ctx *ctx);
+/* The cudaStream_t the context launches on, as void*. */
+int32_t dg_get_stream(dg_ctx *ctx, void **stream);
+/* Number of kernel launches one step makes (1) and the grid of the step
+ * kernel (blocks, threads per block, x-planes per block). */
+int32_t dg_step_launch_shape(dg_ctx *ctx, int32_t *blocks, int32_t *threads, int32_t *chunk);
+/* Override the x-planes per block of the step kernel (0 = automatic). */
+int32_t dg_set_chunk(dg_ctx *ctx, int32_t chunk);
+
+/* Sticky DG_STATUS_* flags raised by the device since dg_create. */
+int32_t dg_status(dg_ctx *ctx, uint32_t *flags);
+
+/* Message of the last failed call on ctx (or of the last failed dg_create
+ * when ctx is NULL).  Never NULL. */
+const char *dg_last_error(const dg_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,91 @@
+/*
+ * dg_oracle.h -- CPU oracle for the deep-green Euler finite-volume step.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker for the CUDA
+ * implementation: only the test-suite, the smoke check and the CPU-baseline
+ * leg of the benchmark may load it.  The product path never links it.
+ *
+ * It restates, array by array and in the same operation order, the Rust
+ * reference path of deep-green:
+ *   src/rs/src/physics.rs   calc_primitives (109-141), calc_conserved (143-175),
+ *                           calc_timestep (177-196), calc_gradients (198-215),
+ *                           extrapolate_primitives_t (217-282),
+ *                           calc_flux_reconstruction (284-409), add_fluxes
+ *                           (539-593), compute_step (595-681)
+ *   src/rs/src/boundaries.rs apply_boundary_conditions (5-99),
+ *                           apply_boundary_conditions4 (101-195),
+ *                           handle_walls (197-407)
+ *   src/rs/src/grid.rs      Simulation::new (44-76), ghost-update methods
+ *                           (121-167), SimulationGrid::new (169-221)
+ * It keeps all 45 ghosted arrays of SimulationGrid (5 primitives, 5
+ * extrapolated primitives, 5 conserved, 5 gradients x 3, 5 fluxes x 3) and
+ * fills ghosts with whole-slice copies exactly as the reference does.
+ *
+ * Parameters that the reference hard-codes as statics (globals.rs:3-8:
+ * GAMMA, CFL, G) are runtime fields here.  Two additions that the reference
+ * does not have are switchable and off by default: a minmod slope limiter
+ * (limiter = 1) and nothing else; gravity follows physics.rs:366-372.
+ *
+ * PARITY UNPINNED: the reference ships no tests, golden vectors or stored
+ * outputs, and none of its implementations can be built or run in this
+ * environment (no Rust toolchain or crates, no gfortran, no warp, and the
+ * CUDA path needs HighFive/HDF5).  This oracle is cross-checked against an
+ * independent NumPy restatement (oracle/numpy_twin.py) and against physics
+ * invariants, not against reference outputs.
+ *
+ * Build: make -C oracle   (gcc, -O2 -fopenmp -ffp-contract=off)
+ */
+#ifndef DG_ORACLE_H
+#define DG_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* BoundaryType, grid.rs:23-28 (same order). */
+enum { DGO_PERIODIC = 0, DGO_OUTFLOW = 1, DGO_WALL = 2 };
+
+/* Array groups of SimulationGrid, grid.rs:111-118. */
+enum { DGO_PRIM = 0, DGO_XTR = 1, DGO_CONS = 2, DGO_GRAD = 3, DGO_FLUX = 4 };
+
+/* Threading of the restatement: serial; parallel only where the Rust code
+ * uses rayon Zip::par_for_each (calc_primitives, calc_conserved,
+ * calc_timestep, calc_gradients); or every phase parallel. */
+enum { DGO_SERIAL = 0, DGO_RUST_LIKE = 1, DGO_ALL_PARALLEL = 2 };
+
+typedef struct dgo_info {
+    int32_t nx, ny, nz;  /* interior cells; arrays are (n+4)^3 with 2 ghosts */
+    int32_t bcs[6];      /* x-, x+, y-, y+, z-, z+ */
+    int32_t gravity;     /* Simulation::gravity */
+    int32_t limiter;     /* 0: central slopes (reference); 1: minmod */
+    double ds, gamma, cfl, g;
+} dgo_info;
+
+typedef struct dgo_ctx dgo_ctx;
+
+/* precision: 8 (double) or 4 (float).  Returns NULL on bad arguments. */
+dgo_ctx *dgo_create(const dgo_info *info, int32_t precision);
+void dgo_destroy(dgo_ctx *ctx);
+void dgo_set_threads(dgo_ctx *ctx, int32_t mode);
+/* Pointer to an internal array: group DGO_PRIM/XTR/CONS: (n_x,n_y,n_z);
+ * DGO_GRAD/FLUX: (n_x,n_y,n_z,3).  field: 0 rho/mass, 1 vx/mom_x,
+ * 2 vy/mom_y, 3 vz/mom_z, 4 p/energy. */
+void *dgo_field(dgo_ctx *ctx, int32_t group, int32_t field);
+/* physics.rs:143 */
+void dgo_calc_conserved(dgo_ctx *ctx);
+/* physics.rs:109 */
+void dgo_calc_primitives(dgo_ctx *ctx);
+/* grid.rs:121 */
+void dgo_update_primitive_ghost_cells(dgo_ctx *ctx);
+/* physics.rs:177; returns dt in double. */
+double dgo_calc_timestep(dgo_ctx *ctx);
+/* physics.rs:595; runs nsteps steps, dt of each step written to dts[]
+ * (may be NULL).  Returns 0. */
+int32_t dgo_compute_step(dgo_ctx *ctx, int32_t nsteps, double *dts);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,200 @@
+"""GPU parity: the CUDA step (through the C ABI) against the CPU oracle.
+
+Tolerances (per conserved field, relative L1 = sum|a-b| / sum|b| over the
+interior, against the FP64 oracle):
+    FP64 kernel <= 1e-12,   FP32 kernel <= 1e-5.
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import pyoracle
+from conftest import INTERIOR, random_primitives, rel_l1
+from deepgreen import capi, setups
+
+pytestmark = pytest.mark.gpu
+
+P, O, W = 0, 1, 2
+TOL = {capi.F64: 1e-12, capi.F32: 1e-5}
+DT_TOL = {capi.F64: 1e-13, capi.F32: 1e-6}
+BC_SETS = [(P,) * 6, (O,) * 6, (W,) * 6, (W, W, P, P, O, O), (P, P, W, W, O, O), (O, W, W, O, P, P)]
+GOLD = Path(__file__).parent / "golden" / "oracle_cases.npz"
+
+
+def gpu_run(shape, ds, bcs, prim, steps, precision, limiter=1, gamma=1.4, cfl=0.4, gravity=False, chunk=0):
+    ctx = capi.Context(shape, ds, bcs, gamma=gamma, cfl=cfl, limiter=limiter, precision=precision,
+                       gravity=gravity)
+    if chunk:
+        ctx.set_chunk(chunk)
+    ctx.set_primitives([np.asarray(a, dtype=ctx.dtype) for a in prim])
+    dts = ctx.compute_step(steps)
+    cons = ctx.get_conserved()
+    return ctx, dts, cons
+
+
+def oracle_run(shape, ds, bcs, prim, steps, limiter=1, gamma=1.4, cfl=0.4, gravity=False):
+    o = pyoracle.Oracle(shape, ds, bcs, gamma=gamma, cfl=cfl, limiter=limiter, gravity=gravity,
+                        threads=pyoracle.ALL_PARALLEL)
+    o.set_primitives(prim)
+    dts = o.step(steps)
+    return o, dts, o.conserved()
+
+
+def assert_parity(cons, ref, dts, ref_dts, precision, label=""):
+    errs = [rel_l1(cons[f], ref[f]) for f in range(5)]
+    assert max(errs) <= TOL[precision], f"{label} rel-L1 per field {errs}"
+    np.testing.assert_allclose(dts, ref_dts, rtol=DT_TOL[precision], err_msg=label)
+    return errs
+
+
+@pytest.mark.parametrize("precision", [capi.F64, capi.F32])
+def test_golden_cases(precision):
+    import sys
+    sys.path.insert(0, str(GOLD.parent))
+    import make_golden
+    gold = np.load(GOLD)
+    for name, shape, bcs, lim, grav, steps, seed in make_golden.CASES:
+        prim = random_primitives(shape, seed)
+        _, dts, cons = gpu_run(shape, 0.1, bcs, prim, steps, precision, limiter=lim, gravity=bool(grav))
+        ref = [np.pad(gold[f"{name}/cons"][f], 2) for f in range(5)]
+        assert_parity(cons, ref, dts, gold[f"{name}/dts"], precision, name)
+
+
+@pytest.mark.parametrize("bcs", BC_SETS)
+@pytest.mark.parametrize("limiter", [0, 1])
+@pytest.mark.parametrize("precision", [capi.F64, capi.F32])
+def test_bc_matrix_ragged_tiles(bcs, limiter, precision):
+    # y not a multiple of the tile rows, z spans two ragged warp tiles,
+    # several x-chunks per column
+    shape = (13, 11, 45)
+    prim = random_primitives(shape, 100 + limiter)
+    _, ref_dts, ref = oracle_run(shape, 0.05, bcs, prim, 6, limiter=limiter)
+    _, dts, cons = gpu_run(shape, 0.05, bcs, prim, 6, precision, limiter=limiter, chunk=4)
+    assert_parity(cons, ref, dts, ref_dts, precision, str(bcs))
+
+
+@pytest.mark.parametrize("precision", [capi.F64, capi.F32])
+def test_kelvin_helmholtz_64_200_steps(precision):
+    """The CPU-runnable workload: 64^3 periodic KH, gamma 1.4, minmod,
+    CFL 0.4, 200 steps, compared with the FP64 oracle."""
+    prim, ds, bcs = setups.kelvin_helmholtz(64, seed=1)
+    _, ref_dts, ref = oracle_run((64,) * 3, ds, bcs, prim, 200)
+    _, dts, cons = gpu_run((64,) * 3, ds, bcs, prim, 200, precision)
+    errs = assert_parity(cons, ref, dts, ref_dts, precision, "kh64")
+    print("kh64 precision", precision, "rel-L1 per field", errs)
+
+
+@pytest.mark.parametrize("case", ["sod", "vortex"])
+@pytest.mark.parametrize("precision", [capi.F64, capi.F32])
+def test_sod_and_vortex_48(case, precision):
+    if case == "sod":
+        prim, ds, bcs = setups.sod(48)
+    else:
+        prim, ds, bcs = setups.isentropic_vortex(48)
+    _, ref_dts, ref = oracle_run((48,) * 3, ds, bcs, prim, 40)
+    _, dts, cons = gpu_run((48,) * 3, ds, bcs, prim, 40, precision)
+    assert_parity(cons, ref, dts, ref_dts, precision, case)
+
+
+def test_gravity_wall_case():
+    shape = (9, 10, 40)
+    prim = random_primitives(shape, 33)
+    bcs = (P, P, O, O, W, W)
+    _, ref_dts, ref = oracle_run(shape, 0.05, bcs, prim, 8, limiter=0, gravity=True)
+    _, dts, cons = gpu_run(shape, 0.05, bcs, prim, 8, capi.F64, limiter=0, gravity=True)
+    assert_parity(cons, ref, dts, ref_dts, capi.F64, "gravity")
+
+
+def test_tiling_does_not_change_results():
+    """Every cell is computed by the same arithmetic whatever the tiling:
+    results are bitwise identical across x-chunk sizes."""
+    shape = (24, 17, 40)
+    prim = random_primitives(shape, 44)
+    outs = []
+    for chunk in (0, 1, 5, 24):
+        _, dts, cons = gpu_run(shape, 0.05, BC_SETS[3], prim, 5, capi.F32, chunk=chunk)
+        outs.append((dts, cons))
+    for dts, cons in outs[1:]:
+        np.testing.assert_array_equal(dts, outs[0][0])
+        for f in range(5):
+            np.testing.assert_array_equal(cons[f][INTERIOR], outs[0][1][f][INTERIOR])
+
+
+def test_deterministic_sums_and_state():
+    shape = (20, 20, 20)
+    prim = random_primitives(shape, 55)
+    a = gpu_run(shape, 0.05, BC_SETS[0], prim, 4, capi.F64)
+    b = gpu_run(shape, 0.05, BC_SETS[0], prim, 4, capi.F64)
+    np.testing.assert_array_equal(a[0].conservation_sums(), b[0].conservation_sums())
+    for f in range(5):
+        np.testing.assert_array_equal(a[2][f], b[2][f])
+
+
+def test_conservation_sums_and_periodic_conservation():
+    prim, ds, bcs = setups.kelvin_helmholtz(32, seed=4)
+    ctx = capi.Context((32,) * 3, ds, bcs, gamma=1.4, cfl=0.4, limiter=1, precision=capi.F64)
+    ctx.set_primitives(prim)
+    s0 = ctx.conservation_sums()
+    c0 = ctx.get_conserved()
+    np.testing.assert_allclose(s0, [c[INTERIOR].sum() for c in c0], rtol=1e-13)
+    ctx.compute_step(50)
+    s1 = ctx.conservation_sums()
+    c1 = ctx.get_conserved()
+    np.testing.assert_allclose(s1, [c[INTERIOR].sum() for c in c1], rtol=1e-12, atol=1e-16)
+    for f in (0, 1, 4):
+        assert abs(s1[f] - s0[f]) <= 1e-12 * abs(s0[f])
+
+
+def test_ghost_cells_follow_boundary_rules():
+    """Downloaded ghosts are the images the reference's ghost fill makes."""
+    from fused_model import fill_ghosts
+    shape = (10, 9, 11)
+    prim = random_primitives(shape, 66)
+    for bcs in BC_SETS:
+        _, _, cons = gpu_run(shape, 0.05, bcs, prim, 2, capi.F64)
+        ref = fill_ghosts(cons, bcs)
+        for f in range(5):
+            np.testing.assert_array_equal(cons[f], ref[f])
+
+
+def test_primitives_are_pre_step_state_like_reference():
+    """After compute_step the reference's grid.primitives hold the state the
+    step started from, ghosts filled (physics.rs:597-598)."""
+    shape = (8, 9, 10)
+    prim = random_primitives(shape, 77)
+    bcs = BC_SETS[5]
+    o, _, _ = oracle_run(shape, 0.05, bcs, prim, 3)
+    ctx, _, _ = gpu_run(shape, 0.05, bcs, prim, 3, capi.F64)
+    got = ctx.get_primitives()
+    want = o.primitives()
+    for f in range(5):
+        np.testing.assert_allclose(got[f], want[f], rtol=1e-12, atol=1e-13)
+
+
+def test_nonfinite_state_flags_and_cfl_fallback():
+    shape = (8, 8, 8)
+    prim = random_primitives(shape, 88)
+    prim[4][5, 5, 5] = -1.0
+    ctx, dts, _ = gpu_run(shape, 0.1, BC_SETS[0], prim, 1, capi.F64, cfl=0.4)
+    assert dts[0] == pytest.approx(0.4)
+    assert ctx.status() & capi.STATUS_NONFINITE
+
+
+def test_reference_shaped_api():
+    """Simulation / SimulationGrid / calc_conserved / compute_step used the
+    way the reference's main.rs uses them."""
+    from deepgreen import BoundaryType as BT, Simulation, SimulationGrid, calc_conserved, compute_step
+    sim = Simulation.new(16, 12, 20, 1.0 / 16, (BT.OUTFLOW,) * 6, gamma=1.4, cfl=0.4, limiter=1,
+                         precision=capi.F64)
+    grid = SimulationGrid.new(sim)
+    prim, ds, _ = setups.sod(16, ny=12, nz=20)
+    for dst, src in zip(grid.primitives.fields(), prim):
+        dst[...] = src
+    calc_conserved(grid)
+    dt = compute_step(sim, grid)
+    o, ref_dts, ref = oracle_run((16, 12, 20), ds, (O,) * 6, prim, 1)
+    assert dt == pytest.approx(ref_dts[0], rel=1e-13)
+    got = grid.conserved.fields()
+    for f in range(5):
+        assert rel_l1(got[f], ref[f]) <= 1e-12
