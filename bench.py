@@ -1,0 +1,371 @@
+"""Benchmark of the fused Euler step on B200.
+
+Workload: 3D Sod shock tube on a 512^3 grid (plus 2 ghost layers), FP32
+conserved state (rho, rho*u, rho*v, rho*w, E) in HBM, gamma 1.4, minmod
+slopes, CFL 0.4, outflow boundaries.  One bench step = one call of the
+reference's compute_step = one launch of the fused kernel over all 512^3
+cells.  Data: synthetic (the workload's initial state, built on the GPU).
+
+Metric: GCUPS = 1e9 cell updates per second (whole job: all ranks).
+
+Keys beside the contract's ones:
+  roofline      the step kernel against measured HBM bandwidth:
+                achieved = 40 B per cell update (read + write 5 FP32 fields)
+                x cells / mean kernel time (CUDA events on the library's
+                stream); traffic = ncu DRAM bytes per launch from the
+                committed profile summary when present.
+  e2e           the same metric through the C ABI from pinned HOST buffers:
+                upload of the state, K steps reading dt back after each one
+                (as the reference's time loop does), download of the state.
+  cpu_baseline  the C oracle (a restatement of the reference's Rust step)
+                on the host cores, bounded sample of the same workload.
+  clocks        nvidia-smi samples during the timed region.
+
+--impl reference times the reference's CPU algorithm (the oracle port; the
+Rust crate cannot be built on this image) on the same workload and metric.
+Multi-GPU (torchrun): independent replicas, one 512^3 grid per rank
+(the step has no exchange in this configuration); timing is the max over
+ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "deep-green_b200" / "python"))
+
+METRIC = "GCUPS"
+UNIT = "1e9 cell-updates/s"
+GAMMA, CFL = 1.4, 0.4
+BYTES_PER_CELL = {"f32": 40, "f64": 80}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=512, help="interior cells per axis")
+    ap.add_argument("--case", default="sod", choices=["sod", "vortex"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def workload_name(case, n):
+    return f"{case}3d_{n}^3_fp32_minmod_cfl{CFL}"
+
+
+# --------------------------------------------------------------------------
+# GPU set-up of the initial state (conserved totals, ghosted, dense)
+# --------------------------------------------------------------------------
+def device_initial_state(case, n, device):
+    import torch
+    f64 = torch.float64
+    m = n + 4
+    if case == "sod":
+        ds = 1.0 / n
+        x = (torch.arange(m, dtype=f64, device=device) - 2 + 0.5) * ds
+        left = (x < 0.5).view(m, 1, 1).expand(m, m, m)
+        rho = torch.where(left, 1.0, 0.125).to(f64)
+        p = torch.where(left, 1.0, 0.1).to(f64)
+        vx = torch.zeros((m, m, m), dtype=f64, device=device)
+        vy = torch.zeros_like(vx)
+        vz = torch.zeros_like(vx)
+        bcs = (1,) * 6
+    else:
+        L, beta = 5.0, 5.0
+        ds = 2 * L / n
+        c = -L + (torch.arange(m, dtype=f64, device=device) - 2 + 0.5) * ds
+        x = c.view(m, 1, 1)
+        y = c.view(1, m, 1)
+        r2 = x * x + y * y
+        e = torch.exp(0.5 * (1 - r2))
+        T = 1 - (GAMMA - 1) * beta * beta / (8 * GAMMA * np.pi ** 2) * e * e
+        rho = (T ** (1 / (GAMMA - 1))).expand(m, m, m).contiguous()
+        p = rho ** GAMMA
+        vx = (1 - beta / (2 * np.pi) * e * y).expand(m, m, m).contiguous()
+        vy = (1 + beta / (2 * np.pi) * e * x).expand(m, m, m).contiguous()
+        vz = torch.zeros((m, m, m), dtype=f64, device=device)
+        bcs = (0,) * 6
+    V = ds * ds * ds
+    cons = [rho * V, vx * rho * V, vy * rho * V, vz * rho * V,
+            V * (rho * (vx * vx + vy * vy + vz * vz) / 2 + p / (GAMMA - 1))]
+    cons = [c.to(torch.float32).contiguous() for c in cons]
+    return cons, ds, bcs
+
+
+# --------------------------------------------------------------------------
+# clocks during the timed region
+# --------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            parts = [p.strip() for p in l.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------
+# CPU oracle timing (reference algorithm on the host cores)
+# --------------------------------------------------------------------------
+def cpu_oracle_gcups(case, n, nz_sample, steps, warmup=1):
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle
+    from deepgreen import setups
+    if case == "sod":
+        prim, ds, bcs = setups.sod(n, ny=n, nz=nz_sample)
+    else:
+        prim, ds, bcs = setups.isentropic_vortex(n, ny=n, nz=nz_sample)
+    o = pyoracle.Oracle((n, n, nz_sample), ds, bcs, gamma=GAMMA, cfl=CFL, limiter=1, dtype=np.float32,
+                        threads=pyoracle.ALL_PARALLEL)
+    o.set_primitives([a.astype(np.float32) for a in prim])
+    del prim
+    if warmup:
+        o.step(warmup)
+    times = []
+    for _ in range(steps):
+        t = time.perf_counter()
+        o.step(1)
+        times.append(time.perf_counter() - t)
+    o.close()
+    cells = n * n * nz_sample
+    return cells / statistics.mean(times) / 1e9, times
+
+
+def ncu_traffic_per_launch():
+    """DRAM bytes per launch of the step kernel from the committed ncu
+    summary (profiles/step_kernel_sod512.json), or None."""
+    p = ROOT / "profiles" / "step_kernel_sod512.json"
+    if not p.exists():
+        return None
+    try:
+        d = json.loads(p.read_text())
+        return float(d["dram_bytes_per_launch"])
+    except Exception:
+        return None
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# --------------------------------------------------------------------------
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    n = args.n
+    nz_sample = 64
+    cores = os.cpu_count()
+    gcups, times = cpu_oracle_gcups(args.case, n, nz_sample, args.steps, warmup=args.warmup)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": gcups, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": workload_name(args.case, n), "sample": f"{n}x{n}x{nz_sample} slab of the grid"},
+        "cpu_baseline": {"value": gcups, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} steps of a {n}x{n}x{nz_sample} slab, same physics, FP32, "
+                                   f"C restatement of the Rust step, OpenMP over {cores} threads"},
+        "e2e": {"value": gcups, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    from deepgreen import capi
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n = args.n
+    cons, ds, bcs = device_initial_state(args.case, n, dev)
+    ctx = capi.Context((n, n, n), ds, bcs, gamma=GAMMA, cfl=CFL, limiter=capi.LIMITER_MINMOD,
+                       precision=capi.F32, device=local)
+    ctx.set_conserved_device([c.data_ptr() for c in cons])
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    blocks, threads, chunk = ctx.launch_shape()
+
+    # warm-up
+    ctx.enqueue_steps(args.warmup)
+    ctx.synchronize()
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        start.record(stream)
+        ctx.enqueue_steps(args.steps)
+        end.record(stream)
+        end.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    ms = start.elapsed_time(end)
+    dts = ctx.get_dts(args.steps)
+    status = ctx.status()
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    cells = n ** 3
+    ms_step = ms / args.steps
+    value = world * cells * args.steps / (ms * 1e-3) / 1e9
+
+    # end to end through the C ABI from pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        host_in = [c.cpu().pin_memory() for c in cons]
+        host_out = [torch.empty_like(h).pin_memory() for h in host_in]
+        ptr_in = [h.data_ptr() for h in host_in]
+        ptr_out = [h.data_ptr() for h in host_out]
+        import ctypes
+        lib = ctx.lib
+        arr_in = (ctypes.c_void_p * 5)(*ptr_in)
+        arr_out = (ctypes.c_void_p * 5)(*ptr_out)
+        dtbuf = (ctypes.c_double * 1)()
+        barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx._check(lib.dg_set_conserved(ctx.h, arr_in))
+        for _ in range(args.steps):
+            ctx._check(lib.dg_compute_step(ctx.h, 1, dtbuf))
+        ctx._check(lib.dg_get_conserved(ctx.h, arr_out))
+        e1.record(stream)
+        e1.synchronize()
+        barrier()
+        e2e_ms = e0.elapsed_time(e1)
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([e2e_ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        state_bytes = 5 * (n + 4) ** 3 * 4
+        e2e = {"value": world * cells * args.steps / (e2e_ms * 1e-3) / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": state_bytes / args.steps,
+               "d2h_bytes_per_step": state_bytes / args.steps + 8,
+               "ms_total": e2e_ms, "path": "dg_set_conserved + K x dg_compute_step(1) + dg_get_conserved"}
+
+    if rank != 0:
+        return
+    peak, peak_kind = peaks()
+    achieved = BYTES_PER_CELL["f32"] * cells / (ms_step * 1e-3) / 1e9
+    traffic = ncu_traffic_per_launch()
+    cpu = None
+    if not args.no_cpu and world == 1:
+        nz_sample = 64
+        g, times = cpu_oracle_gcups(args.case, n, nz_sample, 5, warmup=1)
+        cpu = {"value": g, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+               "sample": f"5 steps of a {n}x{n}x{nz_sample} slab of the same workload (FP32, C restatement "
+                         f"of the Rust step, OpenMP over all host threads)"}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": workload_name(args.case, n), "grid": [n, n, n], "ghosts": 2,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single grid",
+                   "l2": "state (2.9 GB read + 2.9 GB written per step) is larger than L2",
+                   "launch": {"blocks": blocks, "threads": threads, "x_planes_per_block": chunk}},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": BYTES_PER_CELL["f32"] * cells},
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "clocks": clk.summary(),
+        "gpu_launches": args.steps,
+        "dt_first_last": [float(dts[0]), float(dts[-1])],
+        "status_flags": status,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -35,6 +35,7 @@ struct dg_ctx {
     CUtensorMap tmap[2];
     cudaStream_t stream;
     int chunk;                 // 0 = automatic
+    bool exact;                // reference-rounding policy
     std::string err;
 };
 
@@ -90,6 +91,7 @@ template <class T> GridArgs<T> grid_args(const dg_ctx *c, const void *src, void 
     a.k.gm1 = a.k.gamma - T(1);
     a.k.inv_gm1 = T(1) / a.k.gm1;
     a.k.half_ds = ds / T(2);
+    a.k.two_ds = T(2) * ds;
     a.k.inv_ds = T(1) / ds;
     a.k.inv_2ds = T(1) / (T(2) * ds);
     a.k.cfl = (T)c->info.cfl;
@@ -140,11 +142,13 @@ int finish_state(dg_ctx *c) {
     if (c->elem == 8) {
         auto a = grid_args<double>(c, c->buf[c->cur], c->buf[c->cur]);
         e = launch_fill_ghosts<double>(a, static_cast<double *>(c->buf[c->cur]), c->stream);
-        if (e == cudaSuccess) e = launch_reduce<double>(a, 1, c->stream);
+        if (e == cudaSuccess) e = launch_reduce_policy<double, true>(a, 1, c->stream);
     } else {
         auto a = grid_args<float>(c, c->buf[c->cur], c->buf[c->cur]);
         e = launch_fill_ghosts<float>(a, static_cast<float *>(c->buf[c->cur]), c->stream);
-        if (e == cudaSuccess) e = launch_reduce<float>(a, 1, c->stream);
+        if (e == cudaSuccess)
+            e = c->exact ? launch_reduce_policy<float, true>(a, 1, c->stream)
+                         : launch_reduce_policy<float, false>(a, 1, c->stream);
     }
     if (e != cudaSuccess) return cuda_fail(c, e, "state set-up kernels");
     c->has_state = true;
@@ -198,10 +202,11 @@ int enqueue(dg_ctx *c, int nsteps) {
         cudaError_t e;
         if (c->elem == 8) {
             auto a = grid_args<double>(c, c->buf[src], c->buf[dst]);
-            e = launch_step<double>(a, &c->tmap[src], c->info.limiter, chunk, c->stream);
+            e = launch_step_policy<double, true>(a, &c->tmap[src], c->info.limiter, chunk, c->stream);
         } else {
             auto a = grid_args<float>(c, c->buf[src], c->buf[dst]);
-            e = launch_step<float>(a, &c->tmap[src], c->info.limiter, chunk, c->stream);
+            e = c->exact ? launch_step_policy<float, true>(a, &c->tmap[src], c->info.limiter, chunk, c->stream)
+                         : launch_step_policy<float, false>(a, &c->tmap[src], c->info.limiter, chunk, c->stream);
         }
         if (e != cudaSuccess) return cuda_fail(c, e, "step kernel launch");
         c->cur = dst;
@@ -245,6 +250,7 @@ int32_t dg_create(const dg_sim_info *info, dg_ctx **out) {
     if (!(info->ds > 0) || !(info->gamma > 1) || !(info->cfl > 0)) { set_err("ds > 0, gamma > 1, cfl > 0 required"); return DG_ERR_INVALID; }
     if (info->precision != DG_F32 && info->precision != DG_F64) { set_err("precision must be DG_F32 or DG_F64"); return DG_ERR_INVALID; }
     if (info->limiter != DG_LIMITER_NONE && info->limiter != DG_LIMITER_MINMOD) { set_err("unknown limiter"); return DG_ERR_INVALID; }
+    if (info->rounding != DG_ROUNDING_DEFAULT && info->rounding != DG_ROUNDING_REFERENCE) { set_err("unknown rounding policy"); return DG_ERR_INVALID; }
     for (int a = 0; a < 3; ++a) {
         const int lo = info->bcs[2 * a], hi = info->bcs[2 * a + 1];
         if (lo < 0 || lo > 2 || hi < 0 || hi > 2) { set_err("unknown boundary type"); return DG_ERR_INVALID; }
@@ -265,6 +271,7 @@ int32_t dg_create(const dg_sim_info *info, dg_ctx **out) {
     if (!c) { set_err("out of host memory"); return DG_ERR_INVALID; }
     c->info = *info;
     c->elem = info->precision == DG_F64 ? 8 : 4;
+    c->exact = c->elem == 8 || info->rounding == DG_ROUNDING_REFERENCE;
     c->nx = info->nx + 4;
     c->ny = info->ny + 4;
     c->nz = info->nz + 4;
@@ -284,7 +291,7 @@ int32_t dg_create(const dg_sim_info *info, dg_ctx **out) {
         const int ty = step_tile_rows(c->elem == 8);
         long long tiles = (long long)((c->ny - 4 + ty - 1) / ty) * ((c->nz - 4 + kTZ - 1) / kTZ);
         long long cap = tiles * (c->nx - 4);   // chunk >= 1
-        if (cap < 148 * 8) cap = 148 * 8;      // reduce kernel
+        if (cap < kReduceBlocks) cap = kReduceBlocks;
         c->part_cap = (int)cap;
         e = cudaMalloc(&c->part, (size_t)cap * sizeof(Partial));
     }
@@ -430,12 +437,16 @@ int32_t dg_get_primitives(dg_ctx *c, void *const prim[5]) {
     cudaError_t e;
     if (c->elem == 8) {
         auto a = grid_args<double>(c, src, nullptr);
-        e = launch_cons_to_prim<double>(a, static_cast<const double *>(src), static_cast<double *>(c->prim_scratch),
-                                        c->fstride, c->pitch, c->stream);
+        e = launch_cons_to_prim_policy<double, true>(a, static_cast<const double *>(src),
+                                                     static_cast<double *>(c->prim_scratch), c->fstride, c->pitch,
+                                                     c->stream);
     } else {
         auto a = grid_args<float>(c, src, nullptr);
-        e = launch_cons_to_prim<float>(a, static_cast<const float *>(src), static_cast<float *>(c->prim_scratch),
-                                       c->fstride, c->pitch, c->stream);
+        auto *dstp = static_cast<float *>(c->prim_scratch);
+        e = c->exact ? launch_cons_to_prim_policy<float, true>(a, static_cast<const float *>(src), dstp, c->fstride,
+                                                               c->pitch, c->stream)
+                     : launch_cons_to_prim_policy<float, false>(a, static_cast<const float *>(src), dstp, c->fstride,
+                                                                c->pitch, c->stream);
     }
     if (e != cudaSuccess) return cuda_fail(c, e, "cons_to_prim");
     if ((r = copy_out(c, prim, c->prim_scratch, cudaMemcpyDeviceToHost)) != DG_OK) return r;
@@ -462,9 +473,7 @@ int32_t dg_get_stream(dg_ctx *c, void **stream) {
 int32_t dg_step_launch_shape(dg_ctx *c, int32_t *blocks, int32_t *threads, int32_t *chunk) {
     if (!c) return DG_ERR_INVALID;
     const int ch = auto_chunk(c);
-    int b;
-    if (c->elem == 8) b = step_grid_blocks<double>(grid_args<double>(c, nullptr, nullptr), ch);
-    else b = step_grid_blocks<float>(grid_args<float>(c, nullptr, nullptr), ch);
+    const int b = step_grid_blocks(c->nx, c->ny, c->nz, c->elem == 8, ch);
     if (blocks) *blocks = b;
     if (threads) *threads = kTZ * step_tile_rows(c->elem == 8);
     if (chunk) *chunk = ch;

@@ -52,20 +52,38 @@ template <class T> struct GridArgs {
     Partial *part;
 };
 
-// Launch helpers implemented in dg_step.cu.
-template <class T>
-cudaError_t launch_step(const GridArgs<T> &a, const CUtensorMap *tmap_src, int limiter, int chunk,
-                        cudaStream_t st);
-template <class T>
-cudaError_t launch_reduce(const GridArgs<T> &a, int set_dt, cudaStream_t st);
+constexpr int kReduceBlocks = 148 * 8;   // grid of the state-reduction kernel
+
+// Tile rows of the step kernel: 32 (z) x 8 (y) threads for float, 32 x 4
+// for double.
+inline int step_tile_rows(bool is_double) { return is_double ? 4 : 8; }
+
+// Blocks of one step launch: (y tiles) x (z tiles) x (x chunks of `chunk`
+// planes).
+inline int step_grid_blocks(int nx, int ny, int nz, bool is_double, int chunk) {
+    const int ty = step_tile_rows(is_double);
+    const int tiles_z = (nz - 4 + kTZ - 1) / kTZ;
+    const int tiles_y = (ny - 4 + ty - 1) / ty;
+    const int chunks = (nx - 4 + chunk - 1) / chunk;
+    return tiles_z * tiles_y * chunks;
+}
+template <class T> int step_grid_blocks(const GridArgs<T> &a, int chunk) {
+    return step_grid_blocks(a.nx, a.ny, a.nz, sizeof(T) == 8, chunk);
+}
+
+// Launch helpers.  EXACT selects the reference-rounding policy
+// (dg_step_ref.cu, built with --fmad=false) or the fast one
+// (dg_step_fast.cu); float/fast, float/exact and double/exact exist.
+template <class T, bool EXACT>
+cudaError_t launch_step_policy(const GridArgs<T> &a, const CUtensorMap *tmap_src, int limiter, int chunk,
+                               cudaStream_t st);
+template <class T, bool EXACT> cudaError_t launch_reduce_policy(const GridArgs<T> &a, int set_dt, cudaStream_t st);
+template <class T, bool EXACT>
+cudaError_t launch_cons_to_prim_policy(const GridArgs<T> &a, const T *cons, T *prim, long long prim_fstride,
+                                       int prim_pitch, cudaStream_t st);
 template <class T> cudaError_t launch_fill_ghosts(const GridArgs<T> &a, T *buf, cudaStream_t st);
 template <class T>
-cudaError_t launch_prim_to_cons(const GridArgs<T> &a, const T *prim, long long prim_fstride,
-                                int prim_pitch, T *cons, cudaStream_t st);
-template <class T>
-cudaError_t launch_cons_to_prim(const GridArgs<T> &a, const T *cons, T *prim, long long prim_fstride,
-                                int prim_pitch, cudaStream_t st);
-template <class T> int step_grid_blocks(const GridArgs<T> &a, int chunk);
-int step_tile_rows(bool is_double);
+cudaError_t launch_prim_to_cons(const GridArgs<T> &a, const T *prim, long long prim_fstride, int prim_pitch, T *cons,
+                                cudaStream_t st);
 
 }  // namespace dg

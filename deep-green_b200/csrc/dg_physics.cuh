@@ -1,14 +1,20 @@
 // dg_physics.cuh -- per-cell and per-face arithmetic of deep-green's Euler
 // step, shared by every kernel of this library.
 //
-// The formulas are those of the reference's Rust path (deep-green
-// src/rs/src/physics.rs); each function cites the lines it follows.  The
-// operation order is re-associated where that saves instructions (one
-// reciprocal per state instead of several divides; the ds and dt factors of
-// the update folded into one scale): results differ from the reference's
-// rounding at the level of the unit roundoff of T, which is what the
-// tolerances of the parity tests (1e-12 relative for double, 1e-5 for float
-// against the double oracle) allow.
+// Two arithmetic policies implement the same formulas (deep-green
+// src/rs/src/physics.rs; each function cites the lines it follows):
+//
+//   Phys<T, true>   "reference rounding": the reference's operation order and
+//                   association, IEEE division and square root.  Compiled
+//                   without fused multiply-add contraction (--fmad=false) it
+//                   rounds exactly like the reference's scalar code, so the
+//                   GPU result equals the CPU restatement bit for bit.  Used
+//                   for FP64 and, on request, for FP32.
+//   Phys<T, false>  "fast": one reciprocal per state instead of several
+//                   divides, the ds and dt factors folded into one update
+//                   scale, fused multiply-adds.  Differs from the reference's
+//                   rounding at the level of the unit roundoff.  The FP32
+//                   production path.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -18,65 +24,222 @@ namespace dg {
 
 enum Bc : int { kPeriodic = 0, kOutflow = 1, kWall = 2 };
 
-template <class T> struct Num;
-
-template <> struct Num<float> {
-    // Reciprocal to ~1 ulp: MUFU.RCP refined by one Newton step would be
-    // exact-ish; the hardware approximation alone is within 2^-22.
-    static __device__ __forceinline__ float rcp(float x) { return __fdividef(1.0f, x); }
-    static __device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
-};
-
-template <> struct Num<double> {
-    static __device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
-    static __device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
-};
-
-// Runtime constants of one grid, derived once on the host.
+// Runtime constants of one grid, derived once on the host in precision T.
 template <class T> struct Consts {
     T ds;        // cell size
-    T inv_vol;   // 1 / ds^3
-    T vol;       // ds^3
-    T gamma;     // ratio of specific heats
+    T vol;       // ds*ds*ds (physics.rs:110, powi(3))
+    T inv_vol;   // 1 / vol
+    T gamma;     // ratio of specific heats (globals.rs:3)
     T gm1;       // gamma - 1
     T inv_gm1;   // 1 / (gamma - 1)
     T half_ds;   // ds / 2 : face reconstruction offset (physics.rs:313-336)
+    T two_ds;    // 2 * ds : central-difference denominator (physics.rs:206)
     T inv_ds;    // 1 / ds
-    T inv_2ds;   // 1 / (2 ds) : central gradient (physics.rs:206-208)
-    T cfl;
+    T inv_2ds;   // 1 / (2 ds)
+    T cfl;       // globals.rs:4
     T g;         // gravity acceleration (globals.rs:7)
 };
 
+template <class T> __device__ __forceinline__ T fast_rcp(T x);
+template <> __device__ __forceinline__ float fast_rcp<float>(float x) { return __fdividef(1.0f, x); }
+template <> __device__ __forceinline__ double fast_rcp<double>(double x) { return 1.0 / x; }
+
 // minmod slope limiter (an addition of this library; the reference uses
-// unlimited central slopes).  Zero when the one-sided slopes differ in sign
-// or one of them is zero, else the one of smaller magnitude.
+// unlimited central slopes): zero when the one-sided slopes differ in sign
+// or one is zero, else the one of smaller magnitude.
 template <class T> __device__ __forceinline__ T minmod(T a, T b) {
-    const T pick = fabs(a) < fabs(b) ? a : b;
-    return (a * b > T(0)) ? pick : T(0);
+    if (!(a * b > T(0))) return T(0);
+    return fabs(a) < fabs(b) ? a : b;
 }
 
-// Slope of q at a cell from its two neighbours along one axis: the
-// reference's central difference (physics.rs:206-208) or minmod.
-template <class T, int LIM>
-__device__ __forceinline__ T slope(T qm, T q0, T qp, const Consts<T> &k) {
-    if (LIM == 0) return (qp - qm) * k.inv_2ds;
-    return minmod((q0 - qm) * k.inv_ds, (qp - q0) * k.inv_ds);
-}
+template <class T, bool EXACT> struct Phys;
 
-// Conserved totals -> primitives (calc_primitives, physics.rs:109-141).
-template <class T>
-__device__ __forceinline__ void cons_to_prim(const T u[5], T w[5], const Consts<T> &k) {
-    const T rho = u[0] * k.inv_vol;
-    const T ir = Num<T>::rcp(u[0]);  // 1 / (rho * V)
-    const T vx = u[1] * ir, vy = u[2] * ir, vz = u[3] * ir;
-    w[0] = rho;
-    w[1] = vx;
-    w[2] = vy;
-    w[3] = vz;
-    w[4] = (u[4] * k.inv_vol - T(0.5) * rho * (vx * vx + vy * vy + vz * vz)) * k.gm1;
-}
+// ---------------------------------------------------------------------------
+// Reference rounding
+// ---------------------------------------------------------------------------
+template <class T> struct Phys<T, true> {
+    // calc_primitives, physics.rs:112-140
+    static __device__ __forceinline__ void prim(const T u[5], T w[5], const Consts<T> &k) {
+        const T r = u[0] / k.vol;
+        const T vx = u[1] / (r * k.vol);
+        const T vy = u[2] / (r * k.vol);
+        const T vz = u[3] / (r * k.vol);
+        w[0] = r;
+        w[1] = vx;
+        w[2] = vy;
+        w[3] = vz;
+        w[4] = (u[4] / k.vol - T(0.5) * r * (vx * vx + vy * vy + vz * vz)) * k.gm1;
+    }
 
-// Primitives -> conserved totals (calc_conserved, physics.rs:143-175).
+    // calc_timestep body, physics.rs:187-189
+    static __device__ __forceinline__ T wave_dt(const T w[5], const Consts<T> &k) {
+        return k.ds / (sqrt(k.gamma * w[4] / w[0]) + sqrt(w[1] * w[1] + w[2] * w[2] + w[3] * w[3]));
+    }
+
+    // calc_gradients, physics.rs:206-208 (LIM 0); minmod of the one-sided
+    // differences (LIM 1)
+    template <int LIM> static __device__ __forceinline__ T slope(T qm, T q0, T qp, const Consts<T> &k) {
+        if (LIM == 0) return (qp - qm) / k.two_ds;
+        return minmod((q0 - qm) / k.ds, (qp - q0) / k.ds);
+    }
+
+    // extrapolate_primitives_t, physics.rs:251-278; gx/gy/gz are d/dx, d/dy,
+    // d/dz of (rho, vx, vy, vz, p)
+    static __device__ __forceinline__ void predict(const T w[5], const T gx[5], const T gy[5], const T gz[5], T dt,
+                                                   const Consts<T> &k, T out[5]) {
+        const T rho = w[0], vx = w[1], vy = w[2], vz = w[3], p = w[4];
+        const T h = T(0.5) * dt;
+        out[0] = rho - h * (vx * gx[0] + rho * gx[1] + vy * gy[0] + rho * gy[2] + vz * gz[0] + rho * gz[3]);
+        out[1] = vx - h * (vx * gx[1] + vy * gy[1] + vz * gz[1] + (T(1.0) / rho) * gx[4]);
+        out[2] = vy - h * (vx * gx[2] + vy * gy[2] + vz * gz[2] + (T(1.0) / rho) * gy[4]);
+        out[3] = vz - h * (vx * gx[3] + vy * gy[3] + vz * gz[3] + (T(1.0) / rho) * gz[4]);
+        out[4] = p - h * (k.gamma * p * (gx[1] + gy[2] + gz[3]) + vx * gx[4] + vy * gy[4] + vz * gz[4]);
+    }
+
+    // calc_flux_reconstruction, physics.rs:313-405, for the face between the
+    // lower cell (xl, gl = predicted state, slope along the face normal) and
+    // the upper cell (xu, gu).  n = 1, 2, 3: index of the normal velocity.
+    // The result includes the final *ds (physics.rs:401-405).  klow: z index
+    // of the lower cell, for the gravity term (z faces only, grav != 0).
+    static __device__ __forceinline__ void face(const T xl[5], const T gl[5], const T xu[5], const T gu[5], int n,
+                                                int grav, int klow, int nz, const Consts<T> &k, T F[5]) {
+        const int t1 = n == 1 ? 2 : 1, t2 = n == 3 ? 2 : 3;
+        const T half = k.half_ds;
+        const T rl = xu[0] - gu[0] * half;
+        const T rr = xl[0] + gl[0] * half;
+        const T vxl = xu[n] - gu[n] * half;
+        const T vxr = xl[n] + gl[n] * half;
+        const T vyl = xu[t1] - gu[t1] * half;
+        const T vyr = xl[t1] + gl[t1] * half;
+        const T vzl = xu[t2] - gu[t2] * half;
+        const T vzr = xl[t2] + gl[t2] * half;
+        const T pl = xu[4] - gu[4] * half;
+        const T pr = xl[4] + gl[4] * half;
+        const T en_left = T(0.5) * (rl * (vxl * vxl + vyl * vyl + vzl * vzl)) + (pl / k.gm1);
+        const T en_right = T(0.5) * (rr * (vxr * vxr + vyr * vyr + vzr * vzr)) + (pr / k.gm1);
+        const T rho_star = (rl + rr) / T(2.0);
+        const T mx = (rl * vxl + rr * vxr) / T(2.0);
+        const T my = (rl * vyl + rr * vyr) / T(2.0);
+        const T mz = (rl * vzl + rr * vzr) / T(2.0);
+        const T en_star = T(0.5) * (en_left + en_right);
+        const T p_star = k.gm1 * (en_star - T(0.5) * (mx * mx + my * my + mz * mz) / rho_star);
+        T f0 = mx;
+        T f1 = (mx * mx / rho_star) + p_star;
+        T f2 = mx * my / rho_star;
+        T f3 = mx * mz / rho_star;
+        T f4 = (en_star + p_star) * (mx / rho_star);
+        if (grav) {
+            const T h = (T(nz) - T(2.0) * T(2)) * k.ds - (T(klow) - T(2.0)) * k.ds;
+            f1 += T(1.0) * rho_star * k.g * h;
+            f4 += T(0.5) * rho_star * (vxl + vxr) * k.g * h;
+        }
+        const T c_l = sqrt(k.gamma * pl / rl) + fabs(vxl);
+        const T c_r = sqrt(k.gamma * pr / rr) + fabs(vxr);
+        const T c_star = fmax(c_l, c_r);
+        f0 = mx - T(0.5) * c_star * (rl - rr);
+        f1 -= c_star * (rl * vxl - rr * vxr) / T(2.0);
+        f2 -= c_star * (rl * vyl - rr * vyr) / T(2.0);
+        f3 -= c_star * (rl * vzl - rr * vzr) / T(2.0);
+        f4 -= c_star * (en_left - en_right) / T(2.0);
+        F[0] = f0 * k.ds;
+        F[n] = f1 * k.ds;
+        F[t1] = f2 * k.ds;
+        F[t2] = f3 * k.ds;
+        F[4] = f4 * k.ds;
+    }
+
+    // add_fluxes, physics.rs:548-554, same summation order
+    static __device__ __forceinline__ T update(T u, T fxh, T fxl, T fyh, T fyl, T fzh, T fzl, T dt,
+                                               const Consts<T> &k) {
+        return u - dt * k.ds * (fxh - fxl + fyh - fyl + fzh - fzl);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Fast
+// ---------------------------------------------------------------------------
+template <class T> struct Phys<T, false> {
+    static __device__ __forceinline__ void prim(const T u[5], T w[5], const Consts<T> &k) {
+        const T ir = fast_rcp(u[0]);   // 1 / (rho V)
+        const T rho = u[0] * k.inv_vol;
+        const T vx = u[1] * ir, vy = u[2] * ir, vz = u[3] * ir;
+        w[0] = rho;
+        w[1] = vx;
+        w[2] = vy;
+        w[3] = vz;
+        w[4] = (u[4] * k.inv_vol - T(0.5) * rho * (vx * vx + vy * vy + vz * vz)) * k.gm1;
+    }
+
+    static __device__ __forceinline__ T wave_dt(const T w[5], const Consts<T> &k) {
+        const T cs = sqrt(k.gamma * w[4] * fast_rcp(w[0]));
+        const T vm = sqrt(w[1] * w[1] + w[2] * w[2] + w[3] * w[3]);
+        return k.ds * fast_rcp(cs + vm);
+    }
+
+    template <int LIM> static __device__ __forceinline__ T slope(T qm, T q0, T qp, const Consts<T> &k) {
+        if (LIM == 0) return (qp - qm) * k.inv_2ds;
+        return minmod((q0 - qm) * k.inv_ds, (qp - q0) * k.inv_ds);
+    }
+
+    static __device__ __forceinline__ void predict(const T w[5], const T gx[5], const T gy[5], const T gz[5], T dt,
+                                                   const Consts<T> &k, T out[5]) {
+        const T rho = w[0], vx = w[1], vy = w[2], vz = w[3], p = w[4];
+        const T h = T(0.5) * dt;
+        const T ir = fast_rcp(rho);
+        const T div = gx[1] + gy[2] + gz[3];
+        out[0] = rho - h * (vx * gx[0] + vy * gy[0] + vz * gz[0] + rho * div);
+        out[1] = vx - h * (vx * gx[1] + vy * gy[1] + vz * gz[1] + ir * gx[4]);
+        out[2] = vy - h * (vx * gx[2] + vy * gy[2] + vz * gz[2] + ir * gy[4]);
+        out[3] = vz - h * (vx * gx[3] + vy * gy[3] + vz * gz[3] + ir * gz[4]);
+        out[4] = p - h * (k.gamma * p * div + vx * gx[4] + vy * gy[4] + vz * gz[4]);
+    }
+
+    // Same flux as the reference policy, re-associated; WITHOUT the final
+    // *ds (folded into the update scale dt*ds*ds).
+    static __device__ __forceinline__ void face(const T xl[5], const T gl[5], const T xu[5], const T gu[5], int n,
+                                                int grav, int klow, int nz, const Consts<T> &k, T F[5]) {
+        const int t1 = n == 1 ? 2 : 1, t2 = n == 3 ? 2 : 3;
+        const T half = k.half_ds;
+        // a: lower side of the face, b: upper side
+        const T ra = xl[0] + gl[0] * half, rb = xu[0] - gu[0] * half;
+        const T ua = xl[n] + gl[n] * half, ub = xu[n] - gu[n] * half;
+        const T va = xl[t1] + gl[t1] * half, vb = xu[t1] - gu[t1] * half;
+        const T wa = xl[t2] + gl[t2] * half, wb = xu[t2] - gu[t2] * half;
+        const T pa = xl[4] + gl[4] * half, pb = xu[4] - gu[4] * half;
+        const T ea = T(0.5) * ra * (ua * ua + va * va + wa * wa) + pa * k.inv_gm1;
+        const T eb = T(0.5) * rb * (ub * ub + vb * vb + wb * wb) + pb * k.inv_gm1;
+        const T mua = ra * ua, mva = ra * va, mwa = ra * wa;
+        const T mub = rb * ub, mvb = rb * vb, mwb = rb * wb;
+        const T rs = T(0.5) * (ra + rb);
+        const T mu = T(0.5) * (mua + mub), mv = T(0.5) * (mva + mvb), mw = T(0.5) * (mwa + mwb);
+        const T es = T(0.5) * (ea + eb);
+        const T irs = fast_rcp(rs);
+        const T us = mu * irs;
+        const T ps = k.gm1 * (es - T(0.5) * (mu * mu + mv * mv + mw * mw) * irs);
+        const T ca = sqrt(k.gamma * pa * fast_rcp(ra)) + fabs(ua);
+        const T cb = sqrt(k.gamma * pb * fast_rcp(rb)) + fabs(ub);
+        const T hc = T(0.5) * fmax(ca, cb);
+        T fu = mu * us + ps, fe = (es + ps) * us;
+        if (grav) {
+            const T gh = k.g * (T(nz - 4) * k.ds - T(klow - 2) * k.ds);
+            fu += rs * gh;
+            fe += T(0.5) * rs * (ua + ub) * gh;
+        }
+        F[0] = mu - hc * (rb - ra);
+        F[n] = fu - hc * (mub - mua);
+        F[t1] = mv * us - hc * (mvb - mva);
+        F[t2] = mw * us - hc * (mwb - mwa);
+        F[4] = fe - hc * (eb - ea);
+    }
+
+    static __device__ __forceinline__ T update(T u, T fxh, T fxl, T fyh, T fyl, T fzh, T fzl, T dt,
+                                               const Consts<T> &k) {
+        return u - (dt * k.ds * k.ds) * ((fxh - fxl) + (fyh - fyl) + (fzh - fzl));
+    }
+};
+
+// Primitives -> conserved totals (calc_conserved, physics.rs:146-174);
+// reference order.
 template <class T>
 __host__ __device__ __forceinline__ void prim_to_cons(const T w[5], T u[5], T vol, T gm1) {
     const T rho = w[0], vx = w[1], vy = w[2], vz = w[3], p = w[4];
@@ -84,73 +247,7 @@ __host__ __device__ __forceinline__ void prim_to_cons(const T w[5], T u[5], T vo
     u[1] = vx * rho * vol;
     u[2] = vy * rho * vol;
     u[3] = vz * rho * vol;
-    u[4] = vol * (rho * (vx * vx + vy * vy + vz * vz) / T(2) + p / gm1);
-}
-
-// ds / (c_s + |v|) of one cell (the quantity minimised by calc_timestep,
-// physics.rs:186-190).  NaN propagates so the caller can flag it.
-template <class T>
-__device__ __forceinline__ T wave_dt(const T w[5], const Consts<T> &k) {
-    const T cs = Num<T>::sqrt_(k.gamma * w[4] * Num<T>::rcp(w[0]));
-    const T vm = Num<T>::sqrt_(w[1] * w[1] + w[2] * w[2] + w[3] * w[3]);
-    return k.ds * Num<T>::rcp(cs + vm);
-}
-
-// Half-step predictor (extrapolate_primitives_t, physics.rs:251-278).
-// gx/gy/gz hold d/dx, d/dy, d/dz of (rho, vx, vy, vz, p); hdt = dt / 2.
-template <class T>
-__device__ __forceinline__ void predict(const T w[5], const T gx[5], const T gy[5], const T gz[5],
-                                        T hdt, const Consts<T> &k, T out[5]) {
-    const T rho = w[0], vx = w[1], vy = w[2], vz = w[3], p = w[4];
-    const T ir = Num<T>::rcp(rho);
-    const T div = gx[1] + gy[2] + gz[3];
-    out[0] = rho - hdt * (vx * gx[0] + vy * gy[0] + vz * gz[0] + rho * div);
-    out[1] = vx - hdt * (vx * gx[1] + vy * gy[1] + vz * gz[1] + ir * gx[4]);
-    out[2] = vy - hdt * (vx * gx[2] + vy * gy[2] + vz * gz[2] + ir * gy[4]);
-    out[3] = vz - hdt * (vx * gx[3] + vy * gy[3] + vz * gz[3] + ir * gz[4]);
-    out[4] = p - hdt * (k.gamma * p * div + vx * gx[4] + vy * gy[4] + vz * gz[4]);
-}
-
-// Rusanov / local Lax-Friedrichs flux through one face
-// (calc_flux_reconstruction, physics.rs:338-405) WITHOUT the final *ds
-// (the caller folds it into the update scale).
-//   a: reconstructed primitive state on the lower side of the face
-//      (the reference's "r" values: lower cell + slope*ds/2),
-//   b: the upper side (the reference's "l" values: upper cell - slope*ds/2),
-//   n: index 1..3 of the velocity component normal to the face.
-// grav_h: G*h of the gravity term (physics.rs:366-372) or 0.
-template <class T>
-__device__ __forceinline__ void face_flux(const T a[5], const T b[5], int n, T grav_h,
-                                          const Consts<T> &k, T F[5]) {
-    const int t1 = n == 1 ? 2 : 1;
-    const int t2 = n == 3 ? 2 : 3;
-    const T ra = a[0], ua = a[n], va = a[t1], wa = a[t2], pa = a[4];
-    const T rb = b[0], ub = b[n], vb = b[t1], wb = b[t2], pb = b[4];
-    const T ea = T(0.5) * ra * (ua * ua + va * va + wa * wa) + pa * k.inv_gm1;
-    const T eb = T(0.5) * rb * (ub * ub + vb * vb + wb * wb) + pb * k.inv_gm1;
-    const T mua = ra * ua, mva = ra * va, mwa = ra * wa;
-    const T mub = rb * ub, mvb = rb * vb, mwb = rb * wb;
-    const T rs = T(0.5) * (ra + rb);
-    const T mu = T(0.5) * (mua + mub), mv = T(0.5) * (mva + mvb), mw = T(0.5) * (mwa + mwb);
-    const T es = T(0.5) * (ea + eb);
-    const T irs = Num<T>::rcp(rs);
-    const T us = mu * irs;
-    const T ps = k.gm1 * (es - T(0.5) * (mu * mu + mv * mv + mw * mw) * irs);
-    const T ca = Num<T>::sqrt_(k.gamma * pa * Num<T>::rcp(ra)) + fabs(ua);
-    const T cb = Num<T>::sqrt_(k.gamma * pb * Num<T>::rcp(rb)) + fabs(ub);
-    const T c = fmax(ca, cb);
-    const T hc = T(0.5) * c;
-    T fr = mu, fu = mu * us + ps, fv = mv * us, fw = mw * us, fe = (es + ps) * us;
-    if (grav_h != T(0)) {
-        fu += rs * grav_h;
-        fe += T(0.5) * rs * (ua + ub) * grav_h;
-    }
-    // F -= c/2 (U_upper - U_lower)
-    F[0] = fr - hc * (rb - ra);
-    F[n] = fu - hc * (mub - mua);
-    F[t1] = fv - hc * (mvb - mva);
-    F[t2] = fw - hc * (mwb - mwa);
-    F[4] = fe - hc * (eb - ea);
+    u[4] = vol * (rho * (vx * vx + vy * vy + vz * vz) / T(2.0) + p / gm1);
 }
 
 }  // namespace dg

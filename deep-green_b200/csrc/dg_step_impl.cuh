@@ -1,4 +1,7 @@
-// dg_step.cu -- the fused Euler step for sm_100a and its helper kernels.
+// dg_step_impl.cuh -- the fused Euler step for sm_100a and its helper
+// kernels, templated on precision and arithmetic policy (dg_physics.cuh).
+// Instantiated by dg_step_fast.cu (fused multiply-add allowed) and
+// dg_step_ref.cu (compiled with --fmad=false: reference rounding).
 //
 // One launch = one compute_step of the reference (deep-green
 // src/rs/src/physics.rs:595-681).  The reference runs ten passes over 45
@@ -31,6 +34,7 @@
 // Ghost layers of the state itself are kept up to date in memory (every
 // updated cell also writes its periodic/outflow/wall images), so the TMA
 // boxes need no fix-up.
+#pragma once
 #include <cstdio>
 
 #include "dg_kernels.cuh"
@@ -158,17 +162,18 @@ template <class T, int TY, int R> struct StepSmem {
     T xt[5 * kRect];             // predicted primitives
     T gy[5 * kRect];             // y-slopes
     T gz[5 * kRect];             // z-slopes
-    T fy[5 * (TY + 1) * kTZ];    // y-face fluxes of the plane
-    T fz[5 * TY * (kTZ + 1)];    // z-face fluxes of the plane
+    T fy[2][5 * (TY + 1) * kTZ]; // y-face fluxes, double-buffered by plane parity
+    T fz[2][5 * TY * (kTZ + 1)]; // z-face fluxes, double-buffered by plane parity
     uint64_t bar[R];
     double red[(TY * kTZ / 32) * 7];
     int abort_flag;
     int is_last;
 };
 
-template <class T, int TY, int LIM, int R>
+template <class T, int TY, int LIM, int R, bool EXACT>
 struct StepKernel {
     using S = StepSmem<T, TY, R>;
+    using Ph = Phys<T, EXACT>;
     static constexpr int NT = TY * kTZ;
 
     // primitive f of region cell (ry, rz) in ring slot `slot`
@@ -185,9 +190,9 @@ struct StepKernel {
         for (int f = 0; f < 5; ++f) {
             const T c = P(s, s0, f, ry, rz);
             w[f] = c;
-            gx[f] = slope<T, LIM>(P(s, sm, f, ry, rz), c, P(s, sp, f, ry, rz), k);
-            gy[f] = slope<T, LIM>(P(s, s0, f, ry - 1, rz), c, P(s, s0, f, ry + 1, rz), k);
-            gz[f] = slope<T, LIM>(P(s, s0, f, ry, rz - 1), c, P(s, s0, f, ry, rz + 1), k);
+            gx[f] = Ph::template slope<LIM>(P(s, sm, f, ry, rz), c, P(s, sp, f, ry, rz), k);
+            gy[f] = Ph::template slope<LIM>(P(s, s0, f, ry - 1, rz), c, P(s, s0, f, ry + 1, rz), k);
+            gz[f] = Ph::template slope<LIM>(P(s, s0, f, ry, rz - 1), c, P(s, s0, f, ry, rz + 1), k);
         }
     }
 
@@ -195,7 +200,7 @@ struct StepKernel {
     // the ghost-layer-1 rules of the y and z boundaries.  Returns the
     // x-slopes and prediction of the stored cell in gx_out / xt_out.
     static __device__ __forceinline__ void cell_state(S &s, const GridArgs<T> &a, int sm, int s0, int sp,
-                                                      int ry, int rz, int gyc, int gzc, T hdt, T gx_out[5],
+                                                      int ry, int rz, int gyc, int gzc, T dt, T gx_out[5],
                                                       T xt_out[5]) {
         const Consts<T> &k = a.k;
         T w[5], gx[5], gy[5], gz[5];
@@ -209,16 +214,18 @@ struct StepKernel {
         if (rule == kOutflow) {
             // ghost takes slopes and prediction of the interior neighbour
             slopes(s, sm, s0, sp, nry, nrz, k, w, gx, gy, gz);
-            predict(w, gx, gy, gz, hdt, k, xt_out);
+            Ph::predict(w, gx, gy, gz, dt, k, xt_out);
         } else {
             slopes(s, sm, s0, sp, ry, rz, k, w, gx, gy, gz);
             if (rule == kWall) {
+                // slopes from the mirrored ghost primitives; prediction =
+                // mirror of the interior neighbour's (normal velocity negated)
                 T w2[5], gx2[5], gy2[5], gz2[5];
                 slopes(s, sm, s0, sp, nry, nrz, k, w2, gx2, gy2, gz2);
-                predict(w2, gx2, gy2, gz2, hdt, k, xt_out);
-                xt_out[axis - 1] = -xt_out[axis - 1];
+                Ph::predict(w2, gx2, gy2, gz2, dt, k, xt_out);
+                xt_out[axis] = -xt_out[axis];
             } else {
-                predict(w, gx, gy, gz, hdt, k, xt_out);
+                Ph::predict(w, gx, gy, gz, dt, k, xt_out);
             }
         }
         const int r = ridx(ry - 1, rz - 1);
@@ -233,32 +240,31 @@ struct StepKernel {
 
     // y-face flux between rectangle cells (sy-1, sz) [lower] and (sy, sz).
     static __device__ __forceinline__ void yface(S &s, int sy, int sz, const Consts<T> &k, T F[5]) {
-        T lo[5], up[5];
+        T xl[5], gl[5], xu[5], gu[5];
         const int rl = ridx(sy - 1, sz), ru = ridx(sy, sz);
 #pragma unroll
         for (int f = 0; f < 5; ++f) {
-            lo[f] = s.xt[f * S::kRect + rl] + s.gy[f * S::kRect + rl] * k.half_ds;
-            up[f] = s.xt[f * S::kRect + ru] - s.gy[f * S::kRect + ru] * k.half_ds;
+            xl[f] = s.xt[f * S::kRect + rl];
+            gl[f] = s.gy[f * S::kRect + rl];
+            xu[f] = s.xt[f * S::kRect + ru];
+            gu[f] = s.gy[f * S::kRect + ru];
         }
-        face_flux(lo, up, 2, T(0), k, F);
+        Ph::face(xl, gl, xu, gu, 2, 0, 0, 0, k, F);
     }
 
-    // z-face flux between rectangle cells (sy, sz-1) and (sy, sz).
-    static __device__ __forceinline__ void zface(S &s, int sy, int sz, T grav_h, const Consts<T> &k, T F[5]) {
-        T lo[5], up[5];
+    // z-face flux between rectangle cells (sy, sz-1) and (sy, sz); klow is
+    // the ghosted z index of the lower cell (gravity height).
+    static __device__ __forceinline__ void zface(S &s, int sy, int sz, const GridArgs<T> &a, int klow, T F[5]) {
+        T xl[5], gl[5], xu[5], gu[5];
         const int rl = ridx(sy, sz - 1), ru = ridx(sy, sz);
 #pragma unroll
         for (int f = 0; f < 5; ++f) {
-            lo[f] = s.xt[f * S::kRect + rl] + s.gz[f * S::kRect + rl] * k.half_ds;
-            up[f] = s.xt[f * S::kRect + ru] - s.gz[f * S::kRect + ru] * k.half_ds;
+            xl[f] = s.xt[f * S::kRect + rl];
+            gl[f] = s.gz[f * S::kRect + rl];
+            xu[f] = s.xt[f * S::kRect + ru];
+            gu[f] = s.gz[f * S::kRect + ru];
         }
-        face_flux(lo, up, 3, grav_h, k, F);
-    }
-
-    static __device__ __forceinline__ T grav_h(const GridArgs<T> &a, int klow) {
-        if (!a.gravity) return T(0);
-        // h = (nz - 2*nghosts)*ds - (k - 2)*ds  (physics.rs:368)
-        return a.k.g * (T(a.nz - 4) * a.k.ds - T(klow - 2) * a.k.ds);
+        Ph::face(xl, gl, xu, gu, 3, a.gravity, klow, a.nz, a.k, F);
     }
 
     static __device__ void run(const GridArgs<T> &a, const CUtensorMap *tmap, int chunk, unsigned char *raw) {
@@ -284,8 +290,6 @@ struct StepKernel {
         if (*(volatile unsigned *)&a.ctl->flags & kStatusTimeout) return;
         const unsigned step = (unsigned)a.ctl->step;
         const T dt = (T)a.ctl->dt[step & 1];
-        const T hdt = T(0.5) * dt;
-        const T scale = dt * k.ds * k.ds;
 
         if (tid == 0) {
             s.abort_flag = 0;
@@ -306,9 +310,9 @@ struct StepKernel {
         const int nzi = own_valid ? axis_images(gzo, a.nz, a.bc[4], a.bc[5], zimg, zflp) : 0;
 
         T cA[5], cB[5], cC[5];
-        T xt_prev[5], gx_prev[5], fx_lo[5], div_prev[5];
+        T xt_prev[5], gx_prev[5], fx_lo[5];
 #pragma unroll
-        for (int f = 0; f < 5; ++f) { cA[f] = cB[f] = cC[f] = xt_prev[f] = gx_prev[f] = fx_lo[f] = div_prev[f] = T(0); }
+        for (int f = 0; f < 5; ++f) { cA[f] = cB[f] = cC[f] = xt_prev[f] = gx_prev[f] = fx_lo[f] = T(0); }
         double sum[5] = {0, 0, 0, 0, 0};
         T wmin = T(INFINITY);
         unsigned nanf = 0;
@@ -326,7 +330,7 @@ struct StepKernel {
                 T u[5], w[5];
 #pragma unroll
                 for (int f = 0; f < 5; ++f) u[f] = P(s, slot, f, ry, rz);
-                cons_to_prim(u, w, k);
+                Ph::prim(u, w, k);
 #pragma unroll
                 for (int f = 0; f < 5; ++f) { P(s, slot, f, ry, rz) = w[f]; keep[f] = u[f]; }
             }
@@ -344,7 +348,7 @@ struct StepKernel {
                 T u[5], w[5];
 #pragma unroll
                 for (int f = 0; f < 5; ++f) u[f] = P(s, slot, f, ry, rz);
-                cons_to_prim(u, w, k);
+                Ph::prim(u, w, k);
 #pragma unroll
                 for (int f = 0; f < 5; ++f) P(s, slot, f, ry, rz) = w[f];
             }
@@ -369,7 +373,7 @@ struct StepKernel {
 
             // (b) own cell: slopes + prediction
             T xt_cur[5], gx_cur[5];
-            cell_state(s, a, sm, s0, sp, ly + 2, lz + 2, gyo, gzo, hdt, gx_cur, xt_cur);
+            cell_state(s, a, sm, s0, sp, ly + 2, lz + 2, gyo, gzo, dt, gx_cur, xt_cur);
             if (plane_upd) {
                 for (int h = tid; h < HC; h += NT) {
                     int yl, zl;
@@ -378,7 +382,7 @@ struct StepKernel {
                     else if (h < 2 * kTZ + TY) { yl = h - 2 * kTZ; zl = -1; }
                     else { yl = h - 2 * kTZ - TY; zl = kTZ; }
                     T gxh[5], xth[5];
-                    cell_state(s, a, sm, s0, sp, yl + 2, zl + 2, y0 + yl, z0 + zl, hdt, gxh, xth);
+                    cell_state(s, a, sm, s0, sp, yl + 2, zl + 2, y0 + yl, z0 + zl, dt, gxh, xth);
                 }
             }
 
@@ -400,13 +404,7 @@ struct StepKernel {
                         xt_cur[1] = -xt_cur[1];
                     }
                 }
-                T lo[5], up[5];
-#pragma unroll
-                for (int f = 0; f < 5; ++f) {
-                    lo[f] = xt_prev[f] + gx_prev[f] * k.half_ds;
-                    up[f] = xt_cur[f] - gx_cur[f] * k.half_ds;
-                }
-                face_flux(lo, up, 1, T(0), k, fx_hi);
+                Ph::face(xt_prev, gx_prev, xt_cur, gx_cur, 1, 0, 0, 0, k, fx_hi);
             }
             __syncthreads();               // S2: predicted rectangle ready; slot of plane m-1 free
 
@@ -420,56 +418,52 @@ struct StepKernel {
                 ++issued;
             }
 
-            // (d) y- and z-face fluxes of plane m
-            T div_cur[5] = {T(0), T(0), T(0), T(0), T(0)};
+            // (d) y- and z-face fluxes of plane m, into buffer m & 1
             if (plane_upd) {
+                T *fyb = s.fy[m & 1], *fzb = s.fz[m & 1];
                 T F[5];
                 yface(s, ly + 1, lz + 1, k, F);
 #pragma unroll
-                for (int f = 0; f < 5; ++f) s.fy[(f * (TY + 1) + ly) * kTZ + lz] = F[f];
-                zface(s, ly + 1, lz + 1, grav_h(a, gzo - 1), k, F);
+                for (int f = 0; f < 5; ++f) fyb[(f * (TY + 1) + ly) * kTZ + lz] = F[f];
+                zface(s, ly + 1, lz + 1, a, gzo - 1, F);
 #pragma unroll
-                for (int f = 0; f < 5; ++f) s.fz[(f * TY + ly) * (kTZ + 1) + lz] = F[f];
+                for (int f = 0; f < 5; ++f) fzb[(f * TY + ly) * (kTZ + 1) + lz] = F[f];
                 if (ly == 0) {
                     yface(s, TY + 1, lz + 1, k, F);
 #pragma unroll
-                    for (int f = 0; f < 5; ++f) s.fy[(f * (TY + 1) + TY) * kTZ + lz] = F[f];
+                    for (int f = 0; f < 5; ++f) fyb[(f * (TY + 1) + TY) * kTZ + lz] = F[f];
                 } else if (ly == 1 && lz < TY) {
-                    zface(s, lz + 1, kTZ + 1, grav_h(a, z0 + kTZ - 1), k, F);
+                    zface(s, lz + 1, kTZ + 1, a, z0 + kTZ - 1, F);
 #pragma unroll
-                    for (int f = 0; f < 5; ++f) s.fz[(f * TY + lz) * (kTZ + 1) + kTZ] = F[f];
+                    for (int f = 0; f < 5; ++f) fzb[(f * TY + lz) * (kTZ + 1) + kTZ] = F[f];
                 }
             }
             __syncthreads();               // S3: face fluxes of plane m ready
 
-            if (plane_upd) {
-                const bool y_out = gyo == 2 && a.bc[2] == kOutflow;
-                const bool z_out = gzo == 2 && a.bc[4] == kOutflow;
-#pragma unroll
-                for (int f = 0; f < 5; ++f) {
-                    const T fyh = s.fy[(f * (TY + 1) + ly + 1) * kTZ + lz];
-                    const T fyl = y_out ? fyh : s.fy[(f * (TY + 1) + ly) * kTZ + lz];
-                    const T fzh = s.fz[(f * TY + ly) * (kTZ + 1) + lz + 1];
-                    const T fzl = z_out ? fzh : s.fz[(f * TY + ly) * (kTZ + 1) + lz];
-                    div_cur[f] = (fyh - fyl) + (fzh - fzl);
-                }
-            }
-
-            // (e) update plane m-1
+            // (e) update plane m-1 with its y/z fluxes (buffer (m-1) & 1)
             const int xu = m - 1;
             if (xu >= xs && xu < xe && own_valid) {
+                const T *fyb = s.fy[xu & 1], *fzb = s.fz[xu & 1];
                 const bool x_out = xu == 2 && a.bc[0] == kOutflow;
+                const bool y_out = gyo == 2 && a.bc[2] == kOutflow;
+                const bool z_out = gzo == 2 && a.bc[4] == kOutflow;
                 T u[5];
 #pragma unroll
                 for (int f = 0; f < 5; ++f) {
-                    const T fl = x_out ? fx_hi[f] : fx_lo[f];
-                    u[f] = cA[f] - scale * ((fx_hi[f] - fl) + div_prev[f]);
+                    // lower outflow faces repeat the next face's flux
+                    // (boundaries.rs:107-111 applied to the fluxes)
+                    const T fyh = fyb[(f * (TY + 1) + ly + 1) * kTZ + lz];
+                    const T fyl = y_out ? fyh : fyb[(f * (TY + 1) + ly) * kTZ + lz];
+                    const T fzh = fzb[(f * TY + ly) * (kTZ + 1) + lz + 1];
+                    const T fzl = z_out ? fzh : fzb[(f * TY + ly) * (kTZ + 1) + lz];
+                    const T fxl = x_out ? fx_hi[f] : fx_lo[f];
+                    u[f] = Ph::update(cA[f], fx_hi[f], fxl, fyh, fyl, fzh, fzl, dt, k);
                 }
                 // (f) epilogue: next-dt wave speed and FP64 sums of the new state
                 {
                     T w[5];
-                    cons_to_prim(u, w, k);
-                    const T wd = wave_dt(w, k);
+                    Ph::prim(u, w, k);
+                    const T wd = Ph::wave_dt(w, k);
                     if (wd != wd) nanf = 1;
                     else wmin = fmin(wmin, wd);
 #pragma unroll
@@ -495,7 +489,6 @@ struct StepKernel {
                 if (m >= xs) fx_lo[f] = fx_hi[f];
                 xt_prev[f] = xt_cur[f];
                 gx_prev[f] = gx_cur[f];
-                if (plane_upd) div_prev[f] = div_cur[f];
                 cA[f] = cB[f];
                 cB[f] = cC[f];
             }
@@ -616,11 +609,11 @@ __device__ void final_reduce(const GridArgs<T> &a, int tid, int nt, double *red,
     }
 }
 
-template <class T, int TY, int LIM, int R>
+template <class T, int TY, int LIM, int R, bool EXACT>
 __global__ void __launch_bounds__(TY * kTZ)
     step_kernel(const GridArgs<T> a, const __grid_constant__ CUtensorMap tmap, int chunk) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    StepKernel<T, TY, LIM, R>::run(a, &tmap, chunk, smem_raw);
+    StepKernel<T, TY, LIM, R, EXACT>::run(a, &tmap, chunk, smem_raw);
 }
 
 // ---------------------------------------------------------------------------
@@ -628,7 +621,8 @@ __global__ void __launch_bounds__(TY * kTZ)
 // ---------------------------------------------------------------------------
 
 // Reduction of the current state (dt of the first step, conservation sums).
-template <class T> __global__ void __launch_bounds__(256) reduce_kernel(const GridArgs<T> a, int set_dt) {
+template <class T, bool EXACT>
+__global__ void __launch_bounds__(256) reduce_kernel(const GridArgs<T> a, int set_dt) {
     __shared__ double red[8 * 7];
     __shared__ int is_last;
     const int tid = threadIdx.x;
@@ -642,8 +636,8 @@ template <class T> __global__ void __launch_bounds__(256) reduce_kernel(const Gr
         const long long o = (x * a.ny + y) * a.pitch + z;
         T u[5], w[5];
         for (int f = 0; f < 5; ++f) u[f] = a.src[f * a.fstride + o];
-        cons_to_prim(u, w, a.k);
-        const T wd = wave_dt(w, a.k);
+        Phys<T, EXACT>::prim(u, w, a.k);
+        const T wd = Phys<T, EXACT>::wave_dt(w, a.k);
         if (wd != wd) nanf = 1;
         else wm = fmin(wm, (double)wd);
         for (int f = 0; f < 5; ++f) sum[f] += (double)u[f];
@@ -722,7 +716,7 @@ __global__ void prim_to_cons_kernel(const GridArgs<T> a, const T *prim, long lon
 }
 
 // calc_primitives over every cell (ghosts included).
-template <class T>
+template <class T, bool EXACT>
 __global__ void cons_to_prim_kernel(const GridArgs<T> a, const T *cons, T *prim, long long pfs, int ppitch) {
     const long long total = (long long)a.nx * a.ny * a.nz;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < total;
@@ -732,32 +726,22 @@ __global__ void cons_to_prim_kernel(const GridArgs<T> a, const T *cons, T *prim,
         const long long po = xy * ppitch + z, co = xy * a.pitch + z;
         T u[5], w[5];
         for (int f = 0; f < 5; ++f) u[f] = cons[f * a.fstride + co];
-        cons_to_prim(u, w, a.k);
+        Phys<T, EXACT>::prim(u, w, a.k);
         for (int f = 0; f < 5; ++f) prim[f * pfs + po] = w[f];
     }
 }
 
 // ---------------------------------------------------------------------------
-// Launch wrappers
+// Launch wrappers (instantiated per policy by the two translation units)
 // ---------------------------------------------------------------------------
-int step_tile_rows(bool is_double) { return is_double ? 4 : 8; }
-
 template <class T> constexpr int tile_rows() { return sizeof(T) == 8 ? 4 : 8; }
 constexpr int kRing = 4;
 
-template <class T> int step_grid_blocks(const GridArgs<T> &a, int chunk) {
-    constexpr int TY = tile_rows<T>();
-    const int tiles_z = (a.nz - 4 + kTZ - 1) / kTZ;
-    const int tiles_y = (a.ny - 4 + TY - 1) / TY;
-    const int chunks = (a.nx - 4 + chunk - 1) / chunk;
-    return tiles_z * tiles_y * chunks;
-}
-
-template <class T, int LIM>
+template <class T, bool EXACT, int LIM>
 static cudaError_t launch_step_t(const GridArgs<T> &a, const CUtensorMap *tmap, int chunk, cudaStream_t st) {
     constexpr int TY = tile_rows<T>();
     using S = StepSmem<T, TY, kRing>;
-    auto kern = step_kernel<T, TY, LIM, kRing>;
+    auto kern = step_kernel<T, TY, LIM, kRing, EXACT>;
     const int smem = (int)sizeof(S) + 1024;
     static unsigned long long attr_set = 0;  // per instantiation, one bit per device
     int dev = 0;
@@ -773,56 +757,33 @@ static cudaError_t launch_step_t(const GridArgs<T> &a, const CUtensorMap *tmap, 
     return cudaGetLastError();
 }
 
-template <class T>
-cudaError_t launch_step(const GridArgs<T> &a, const CUtensorMap *tmap, int limiter, int chunk, cudaStream_t st) {
-    return limiter ? launch_step_t<T, 1>(a, tmap, chunk, st) : launch_step_t<T, 0>(a, tmap, chunk, st);
+template <class T, bool EXACT>
+cudaError_t launch_step_policy(const GridArgs<T> &a, const CUtensorMap *tmap, int limiter, int chunk,
+                               cudaStream_t st) {
+    return limiter ? launch_step_t<T, EXACT, 1>(a, tmap, chunk, st) : launch_step_t<T, EXACT, 0>(a, tmap, chunk, st);
 }
 
-template <class T> cudaError_t launch_reduce(const GridArgs<T> &a, int set_dt, cudaStream_t st) {
+template <class T, bool EXACT> cudaError_t launch_reduce_policy(const GridArgs<T> &a, int set_dt, cudaStream_t st) {
     const long long total = (long long)(a.nx - 4) * (a.ny - 4) * (a.nz - 4);
     long long blocks = (total + 255) / 256;
-    if (blocks > 148 * 8) blocks = 148 * 8;
-    reduce_kernel<T><<<(int)blocks, 256, 0, st>>>(a, set_dt);
+    if (blocks > kReduceBlocks) blocks = kReduceBlocks;
+    reduce_kernel<T, EXACT><<<(int)blocks, 256, 0, st>>>(a, set_dt);
     return cudaGetLastError();
 }
 
-static int flat_blocks(long long total) {
+inline int flat_blocks(long long total) {
     long long b = (total + 255) / 256;
     if (b > 148 * 16) b = 148 * 16;
     if (b < 1) b = 1;
     return (int)b;
 }
 
-template <class T> cudaError_t launch_fill_ghosts(const GridArgs<T> &a, T *buf, cudaStream_t st) {
-    fill_ghosts_kernel<T><<<flat_blocks((long long)a.nx * a.ny * a.nz), 256, 0, st>>>(a, buf);
+template <class T, bool EXACT>
+cudaError_t launch_cons_to_prim_policy(const GridArgs<T> &a, const T *cons, T *prim, long long pfs, int ppitch,
+                                       cudaStream_t st) {
+    cons_to_prim_kernel<T, EXACT><<<flat_blocks((long long)a.nx * a.ny * a.nz), 256, 0, st>>>(a, cons, prim, pfs,
+                                                                                             ppitch);
     return cudaGetLastError();
 }
-
-template <class T>
-cudaError_t launch_prim_to_cons(const GridArgs<T> &a, const T *prim, long long pfs, int ppitch, T *cons,
-                                cudaStream_t st) {
-    prim_to_cons_kernel<T><<<flat_blocks((long long)a.nx * a.ny * a.nz), 256, 0, st>>>(a, prim, pfs, ppitch, cons);
-    return cudaGetLastError();
-}
-
-template <class T>
-cudaError_t launch_cons_to_prim(const GridArgs<T> &a, const T *cons, T *prim, long long pfs, int ppitch,
-                                cudaStream_t st) {
-    cons_to_prim_kernel<T><<<flat_blocks((long long)a.nx * a.ny * a.nz), 256, 0, st>>>(a, cons, prim, pfs, ppitch);
-    return cudaGetLastError();
-}
-
-#define DG_INSTANTIATE(T)                                                                                   \
-    template cudaError_t launch_step<T>(const GridArgs<T> &, const CUtensorMap *, int, int, cudaStream_t); \
-    template cudaError_t launch_reduce<T>(const GridArgs<T> &, int, cudaStream_t);                          \
-    template cudaError_t launch_fill_ghosts<T>(const GridArgs<T> &, T *, cudaStream_t);                     \
-    template cudaError_t launch_prim_to_cons<T>(const GridArgs<T> &, const T *, long long, int, T *,        \
-                                                cudaStream_t);                                              \
-    template cudaError_t launch_cons_to_prim<T>(const GridArgs<T> &, const T *, T *, long long, int,        \
-                                                cudaStream_t);                                              \
-    template int step_grid_blocks<T>(const GridArgs<T> &, int);
-
-DG_INSTANTIATE(float)
-DG_INSTANTIATE(double)
 
 }  // namespace dg

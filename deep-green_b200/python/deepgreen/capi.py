@@ -25,6 +25,7 @@ DG_ERR_NO_DEVICE = -5
 PERIODIC, OUTFLOW, WALL = 0, 1, 2
 LIMITER_NONE, LIMITER_MINMOD = 0, 1
 F32, F64 = 0, 1
+ROUNDING_DEFAULT, ROUNDING_REFERENCE = 0, 1
 STATUS_NONFINITE = 0x1
 STATUS_TIMEOUT = 0x2
 
@@ -38,6 +39,7 @@ class SimInfo(ctypes.Structure):
         ("bcs", ctypes.c_int32 * 6),
         ("gravity", ctypes.c_int32), ("limiter", ctypes.c_int32),
         ("precision", ctypes.c_int32), ("device", ctypes.c_int32),
+        ("rounding", ctypes.c_int32),
     ]
 
 
@@ -101,7 +103,7 @@ class Context:
     """Owner of one dg_ctx (one grid on one device)."""
 
     def __init__(self, shape, ds, bcs, gamma=5.0 / 3.0, cfl=0.2, g=-0.1, gravity=False,
-                 limiter=LIMITER_NONE, precision=F32, device=0):
+                 limiter=LIMITER_NONE, precision=F32, device=0, rounding=ROUNDING_DEFAULT):
         self.lib = load()
         self.shape = tuple(int(s) for s in shape)
         self.n = tuple(s + 4 for s in self.shape)
@@ -116,6 +118,7 @@ class Context:
         info.limiter = int(limiter)
         info.precision = int(precision)
         info.device = int(device)
+        info.rounding = int(rounding)
         self.info = info
         h = ctypes.c_void_p()
         rc = self.lib.dg_create(ctypes.byref(info), ctypes.byref(h))

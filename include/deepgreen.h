@@ -63,6 +63,13 @@ extern "C" {
 #define DG_F32 0
 #define DG_F64 1
 
+/* arithmetic policy: DEFAULT = fast fused arithmetic for DG_F32 and the
+ * reference's rounding for DG_F64; REFERENCE = the reference's operation
+ * order without fused multiply-add, IEEE divide/sqrt (bitwise reproducible
+ * against a scalar restatement of the Rust code) for either precision */
+#define DG_ROUNDING_DEFAULT 0
+#define DG_ROUNDING_REFERENCE 1
+
 /* status flags (dg_status) */
 #define DG_STATUS_NONFINITE 0x1u  /* a NaN wave speed was seen; dt fell back to cfl*1.0
                                      as calc_timestep does (physics.rs:191-195) */
@@ -83,6 +90,7 @@ typedef struct dg_sim_info {
     int32_t limiter;     /* DG_LIMITER_* */
     int32_t precision;   /* DG_F32 or DG_F64 */
     int32_t device;      /* CUDA device ordinal */
+    int32_t rounding;    /* DG_ROUNDING_* */
 } dg_sim_info;
 
 typedef struct dg_ctx dg_ctx;
@@ -140,7 +148,8 @@ int32_t dg_step_launch_shape(dg_ctx *ctx, int32_t *blocks, int32_t *threads, int
 /* Override the x-planes per block of the step kernel (0 = automatic). */
 int32_t dg_set_chunk(dg_ctx *ctx, int32_t chunk);
 
-/* Sticky DG_STATUS_* flags raised by the device since dg_create. */
+/* Sticky DG_STATUS_* flags raised by the device since the state was last
+ * set (dg_set_*). */
 int32_t dg_status(dg_ctx *ctx, uint32_t *flags);
 
 /* Message of the last failed call on ctx (or of the last failed dg_create
