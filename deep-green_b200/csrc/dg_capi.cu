@@ -36,6 +36,7 @@ struct dg_ctx {
     cudaStream_t stream;
     int chunk;                 // 0 = automatic
     bool exact;                // reference-rounding policy
+    int kind;                  // KernelKind of the step kernel
     std::string err;
 };
 
@@ -83,6 +84,7 @@ template <class T> GridArgs<T> grid_args(const dg_ctx *c, const void *src, void 
     a.fstride = c->fstride;
     for (int i = 0; i < 6; ++i) a.bc[i] = c->info.bcs[i];
     a.gravity = c->info.gravity;
+    a.limiter = c->info.limiter;
     const T ds = (T)c->info.ds;
     a.k.ds = ds;
     a.k.vol = ds * ds * ds;
@@ -103,10 +105,10 @@ template <class T> GridArgs<T> grid_args(const dg_ctx *c, const void *src, void 
 
 int auto_chunk(const dg_ctx *c) {
     if (c->chunk > 0) return c->chunk;
-    const int ty = step_tile_rows(c->elem == 8);
+    const int ty = step_tile_rows(c->kind);
     const long long tiles = (long long)((c->ny - 4 + ty - 1) / ty) * ((c->nz - 4 + kTZ - 1) / kTZ);
     const int nxi = c->nx - 4;
-    const long long target = 148LL * (c->elem == 8 ? 2 : 3) * 4;   // ~4 waves of resident CTAs
+    const long long target = 148LL * 2 * 4;   // ~4 waves of resident CTAs (2 per SM)
     long long chunks = (target + tiles - 1) / tiles;
     long long maxc = nxi / 8 > 0 ? nxi / 8 : 1;
     if (chunks > maxc) chunks = maxc;
@@ -117,7 +119,7 @@ int auto_chunk(const dg_ctx *c) {
 int encode_map(dg_ctx *c, int i) {
     auto fn = get_encode_fn();
     if (!fn) return fail(c, DG_ERR_CUDA, "cuTensorMapEncodeTiled not available from the driver");
-    const int ty = step_tile_rows(c->elem == 8);
+    const int ty = step_tile_rows(c->kind);
     cuuint64_t dims[4] = {(cuuint64_t)c->nz, (cuuint64_t)c->ny, (cuuint64_t)c->nx, 5};
     cuuint64_t strides[3] = {(cuuint64_t)c->pitch * c->elem, (cuuint64_t)c->pitch * c->ny * c->elem,
                              (cuuint64_t)c->fstride * c->elem};
@@ -206,7 +208,7 @@ int enqueue(dg_ctx *c, int nsteps) {
         } else {
             auto a = grid_args<float>(c, c->buf[src], c->buf[dst]);
             e = c->exact ? launch_step_policy<float, true>(a, &c->tmap[src], c->info.limiter, chunk, c->stream)
-                         : launch_step_policy<float, false>(a, &c->tmap[src], c->info.limiter, chunk, c->stream);
+                         : launch_fast_step(a, &c->tmap[src], chunk, c->stream);
         }
         if (e != cudaSuccess) return cuda_fail(c, e, "step kernel launch");
         c->cur = dst;
@@ -272,6 +274,7 @@ int32_t dg_create(const dg_sim_info *info, dg_ctx **out) {
     c->info = *info;
     c->elem = info->precision == DG_F64 ? 8 : 4;
     c->exact = c->elem == 8 || info->rounding == DG_ROUNDING_REFERENCE;
+    c->kind = c->elem == 8 ? kRefF64 : (c->exact ? kRefF32 : kFastF32);
     c->nx = info->nx + 4;
     c->ny = info->ny + 4;
     c->nz = info->nz + 4;
@@ -288,7 +291,7 @@ int32_t dg_create(const dg_sim_info *info, dg_ctx **out) {
     for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaMalloc(&c->buf[i], c->state_bytes);
     if (e == cudaSuccess) e = cudaMalloc(&c->ctl, sizeof(DevCtl));
     if (e == cudaSuccess) {
-        const int ty = step_tile_rows(c->elem == 8);
+        const int ty = step_tile_rows(c->kind);
         long long tiles = (long long)((c->ny - 4 + ty - 1) / ty) * ((c->nz - 4 + kTZ - 1) / kTZ);
         long long cap = tiles * (c->nx - 4);   // chunk >= 1
         if (cap < kReduceBlocks) cap = kReduceBlocks;
@@ -473,9 +476,9 @@ int32_t dg_get_stream(dg_ctx *c, void **stream) {
 int32_t dg_step_launch_shape(dg_ctx *c, int32_t *blocks, int32_t *threads, int32_t *chunk) {
     if (!c) return DG_ERR_INVALID;
     const int ch = auto_chunk(c);
-    const int b = step_grid_blocks(c->nx, c->ny, c->nz, c->elem == 8, ch);
+    const int b = step_grid_blocks(c->nx, c->ny, c->nz, c->kind, ch);
     if (blocks) *blocks = b;
-    if (threads) *threads = kTZ * step_tile_rows(c->elem == 8);
+    if (threads) *threads = step_threads(c->kind);
     if (chunk) *chunk = ch;
     return DG_OK;
 }

@@ -47,6 +47,7 @@ template <class T> struct GridArgs {
     long long fstride;         // elements between fields
     int bc[6];
     int gravity;
+    int limiter;               // 0 central slopes, 1 minmod
     Consts<T> k;
     DevCtl *ctl;
     Partial *part;
@@ -54,21 +55,25 @@ template <class T> struct GridArgs {
 
 constexpr int kReduceBlocks = 148 * 8;   // grid of the state-reduction kernel
 
-// Tile rows of the step kernel: 32 (z) x 8 (y) threads for float, 32 x 4
-// for double.
-inline int step_tile_rows(bool is_double) { return is_double ? 4 : 8; }
+// The three step kernels: reference rounding in double and in float
+// (dg_step_impl.cuh) and the fast float kernel (dg_fast_impl.cuh).
+enum KernelKind : int { kRefF64 = 0, kRefF32 = 1, kFastF32 = 2 };
+
+// Tile rows (y) of each kernel; every tile is 32 cells wide in z.
+inline int step_tile_rows(int kind) { return kind == kRefF64 ? 4 : (kind == kRefF32 ? 8 : 16); }
+inline int step_threads(int kind) { return kind == kFastF32 ? 32 * 8 : 32 * step_tile_rows(kind); }
 
 // Blocks of one step launch: (y tiles) x (z tiles) x (x chunks of `chunk`
 // planes).
-inline int step_grid_blocks(int nx, int ny, int nz, bool is_double, int chunk) {
-    const int ty = step_tile_rows(is_double);
+inline int step_grid_blocks(int nx, int ny, int nz, int kind, int chunk) {
+    const int ty = step_tile_rows(kind);
     const int tiles_z = (nz - 4 + kTZ - 1) / kTZ;
     const int tiles_y = (ny - 4 + ty - 1) / ty;
     const int chunks = (nx - 4 + chunk - 1) / chunk;
     return tiles_z * tiles_y * chunks;
 }
 template <class T> int step_grid_blocks(const GridArgs<T> &a, int chunk) {
-    return step_grid_blocks(a.nx, a.ny, a.nz, sizeof(T) == 8, chunk);
+    return step_grid_blocks(a.nx, a.ny, a.nz, sizeof(T) == 8 ? kRefF64 : kRefF32, chunk);
 }
 
 // Launch helpers.  EXACT selects the reference-rounding policy
@@ -81,6 +86,7 @@ template <class T, bool EXACT> cudaError_t launch_reduce_policy(const GridArgs<T
 template <class T, bool EXACT>
 cudaError_t launch_cons_to_prim_policy(const GridArgs<T> &a, const T *cons, T *prim, long long prim_fstride,
                                        int prim_pitch, cudaStream_t st);
+cudaError_t launch_fast_step(const GridArgs<float> &a, const CUtensorMap *tmap_src, int chunk, cudaStream_t st);
 template <class T> cudaError_t launch_fill_ghosts(const GridArgs<T> &a, T *buf, cudaStream_t st);
 template <class T>
 cudaError_t launch_prim_to_cons(const GridArgs<T> &a, const T *prim, long long prim_fstride, int prim_pitch, T *cons,

@@ -1,10 +1,28 @@
 // dg_step_fast.cu -- FP32 step with the fast arithmetic policy (fused
 // multiply-add contraction allowed).  Kernels: dg_step_impl.cuh.
+#include "dg_fast_impl.cuh"
 #include "dg_step_impl.cuh"
 
 namespace dg {
-template cudaError_t launch_step_policy<float, false>(const GridArgs<float> &, const CUtensorMap *, int, int,
-                                                      cudaStream_t);
+
+cudaError_t launch_fast_step(const GridArgs<float> &a, const CUtensorMap *tmap, int chunk, cudaStream_t st) {
+    constexpr int W = 8, R = 4;
+    using Sm = fastk::Smem<W, R>;
+    auto kern = fastk::fast_step_kernel<W, R>;
+    const int smem = (int)sizeof(Sm) + 1024;
+    static unsigned long long attr_set = 0;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev >= 64 || !(attr_set & (1ull << dev))) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess) return e;
+        if (dev < 64) attr_set |= 1ull << dev;
+    }
+    const int blocks = step_grid_blocks(a.nx, a.ny, a.nz, kFastF32, chunk);
+    kern<<<blocks, dim3(32, W), smem, st>>>(a, *tmap, chunk);
+    return cudaGetLastError();
+}
 template cudaError_t launch_reduce_policy<float, false>(const GridArgs<float> &, int, cudaStream_t);
 template cudaError_t launch_cons_to_prim_policy<float, false>(const GridArgs<float> &, const float *, float *,
                                                               long long, int, cudaStream_t);
