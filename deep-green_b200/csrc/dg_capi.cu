@@ -104,16 +104,7 @@ template <class T> GridArgs<T> grid_args(const dg_ctx *c, const void *src, void 
 }
 
 int auto_chunk(const dg_ctx *c) {
-    if (c->chunk > 0) return c->chunk;
-    const int ty = step_tile_rows(c->kind);
-    const long long tiles = (long long)((c->ny - 4 + ty - 1) / ty) * ((c->nz - 4 + kTZ - 1) / kTZ);
-    const int nxi = c->nx - 4;
-    const long long target = 148LL * 2 * 4;   // ~4 waves of resident CTAs (2 per SM)
-    long long chunks = (target + tiles - 1) / tiles;
-    long long maxc = nxi / 8 > 0 ? nxi / 8 : 1;
-    if (chunks > maxc) chunks = maxc;
-    if (chunks < 1) chunks = 1;
-    return (int)((nxi + chunks - 1) / chunks);
+    return c->chunk > 0 ? c->chunk : choose_chunk(c->nx, c->ny, c->nz, c->kind);
 }
 
 int encode_map(dg_ctx *c, int i) {
@@ -234,6 +225,11 @@ int read_dts(dg_ctx *c, int nsteps, double *dts) {
 }
 
 }  // namespace
+
+void dg::set_global_error(const std::string &msg) {
+    std::lock_guard<std::mutex> g(g_err_mu);
+    g_create_err = msg;
+}
 
 extern "C" {
 

@@ -145,7 +145,7 @@ __device__ __forceinline__ void face(const V a[5], const V b[5], bool grav, V gh
 __device__ __forceinline__ float wave_dt1(const float w[5], const FK &k) {
     const float g = k.gamma * w[4];
     const float cs = g * rsqrtf(g * w[0]);
-    const float vm = __fsqrt_rn(w[1] * w[1] + w[2] * w[2] + w[3] * w[3]);
+    const float vm = sqrtf(fmaf(w[3], w[3], fmaf(w[2], w[2], w[1] * w[1])));
     return k.ds * __fdividef(1.0f, cs + vm);
 }
 

@@ -6,6 +6,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
+
 #include "dg_physics.cuh"
 
 namespace dg {
@@ -72,6 +74,20 @@ inline int step_grid_blocks(int nx, int ny, int nz, int kind, int chunk) {
     const int chunks = (nx - 4 + chunk - 1) / chunk;
     return tiles_z * tiles_y * chunks;
 }
+// Default x-planes per block: enough blocks for ~4 waves of resident CTAs
+// (2 per SM on 148 SMs), at least 8 planes per block.
+inline int choose_chunk(int nx, int ny, int nz, int kind) {
+    const int ty = step_tile_rows(kind);
+    const long long tiles = (long long)((ny - 4 + ty - 1) / ty) * ((nz - 4 + kTZ - 1) / kTZ);
+    const int nxi = nx - 4;
+    const long long target = 148LL * 2 * 4;
+    long long chunks = (target + tiles - 1) / tiles;
+    const long long maxc = nxi / 8 > 0 ? nxi / 8 : 1;
+    if (chunks > maxc) chunks = maxc;
+    if (chunks < 1) chunks = 1;
+    return (int)((nxi + chunks - 1) / chunks);
+}
+
 template <class T> int step_grid_blocks(const GridArgs<T> &a, int chunk) {
     return step_grid_blocks(a.nx, a.ny, a.nz, sizeof(T) == 8 ? kRefF64 : kRefF32, chunk);
 }
@@ -86,6 +102,9 @@ template <class T, bool EXACT> cudaError_t launch_reduce_policy(const GridArgs<T
 template <class T, bool EXACT>
 cudaError_t launch_cons_to_prim_policy(const GridArgs<T> &a, const T *cons, T *prim, long long prim_fstride,
                                        int prim_pitch, cudaStream_t st);
+// Message returned by dg_last_error(NULL) (errors not tied to a context).
+void set_global_error(const std::string &msg);
+
 cudaError_t launch_fast_step(const GridArgs<float> &a, const CUtensorMap *tmap_src, int chunk, cudaStream_t st);
 template <class T> cudaError_t launch_fill_ghosts(const GridArgs<T> &a, T *buf, cudaStream_t st);
 template <class T>

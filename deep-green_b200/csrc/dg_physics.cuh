@@ -159,20 +159,25 @@ template <class T> struct Phys<T, true> {
 // Fast
 // ---------------------------------------------------------------------------
 template <class T> struct Phys<T, false> {
+    // Same operation sequence as the packed FP32 step kernel's epilogue
+    // (dg_fast_impl.cuh), so dt agrees bit for bit between the two.
     static __device__ __forceinline__ void prim(const T u[5], T w[5], const Consts<T> &k) {
         const T ir = fast_rcp(u[0]);   // 1 / (rho V)
         const T rho = u[0] * k.inv_vol;
         const T vx = u[1] * ir, vy = u[2] * ir, vz = u[3] * ir;
+        const T v2 = fma(vz, vz, fma(vy, vy, vx * vx));
         w[0] = rho;
         w[1] = vx;
         w[2] = vy;
         w[3] = vz;
-        w[4] = (u[4] * k.inv_vol - T(0.5) * rho * (vx * vx + vy * vy + vz * vz)) * k.gm1;
+        w[4] = fma(T(-0.5) * rho, v2, u[4] * k.inv_vol) * k.gm1;
     }
 
+    // sqrt(gamma p / rho) as g * rsqrt(g * rho), g = gamma p
     static __device__ __forceinline__ T wave_dt(const T w[5], const Consts<T> &k) {
-        const T cs = sqrt(k.gamma * w[4] * fast_rcp(w[0]));
-        const T vm = sqrt(w[1] * w[1] + w[2] * w[2] + w[3] * w[3]);
+        const T g = k.gamma * w[4];
+        const T cs = g * rsqrt(g * w[0]);
+        const T vm = sqrt(fma(w[3], w[3], fma(w[2], w[2], w[1] * w[1])));
         return k.ds * fast_rcp(cs + vm);
     }
 
