@@ -75,6 +75,7 @@ SIGNATURES = {
     "dg_set_chunk": [_P, _I],
     "dg_status": [_P, ctypes.POINTER(ctypes.c_uint32)],
     "dg_last_error": [_P],
+    "dg_compute_step_noalloc": [ctypes.POINTER(SimInfo), _P, _P, ctypes.POINTER(ctypes.c_double), _P],
 }
 
 

@@ -148,6 +148,32 @@ int32_t dg_step_launch_shape(dg_ctx *ctx, int32_t *blocks, int32_t *threads, int
 /* Override the x-planes per block of the step kernel (0 = automatic). */
 int32_t dg_set_chunk(dg_ctx *ctx, int32_t chunk);
 
+/* One compute_step on caller-owned device memory; the library allocates
+ * nothing.  No counterpart in the reference: it is for callers that must
+ * not let a library call cudaMalloc, such as a host program whose device
+ * memory is owned by its own pool allocator sized at start-up.
+ *   cons_in   device pointer, 5 consecutive fields (mass, mom_x, mom_y,
+ *             mom_z, energy), each (nx+4)(ny+4)(nz+4) elements, C order,
+ *             float or double per info->precision; (nz+4)*element size
+ *             must be a multiple of 16 bytes and the pointer 16-byte
+ *             aligned.  Its ghost cells are rewritten in place by the
+ *             boundary rules before the step.
+ *   cons_out  same layout, distinct from cons_in: the state after the
+ *             step, ghosts filled.
+ *   dt_used   host pointer or NULL: the dt of the step (from cons_in, as
+ *             calc_timestep computes it); when given, the call waits for
+ *             the stream.
+ *   stream    cudaStream_t or NULL.
+ * The step's scratch (control block and per-block partials) is a 1 MiB
+ * array in the library's device image, held by every GPU that loads the
+ * library until exit; grids needing more than it holds are rejected with
+ * DG_ERR_INVALID.  All calls share that array: calls that overlap on the
+ * GPU race.  The first call on a device looks up the array's address with
+ * that device current; make it before any stream capture.  Errors:
+ * dg_last_error(NULL). */
+int32_t dg_compute_step_noalloc(const dg_sim_info *info, void *cons_in, void *cons_out, double *dt_used,
+                                void *stream);
+
 /* Sticky DG_STATUS_* flags raised by the device since the state was last
  * set (dg_set_*). */
 int32_t dg_status(dg_ctx *ctx, uint32_t *flags);
