@@ -141,30 +141,28 @@ __device__ __forceinline__ void face(const V a[5], const V b[5], bool grav, V gh
     F[4] = vfma(nhc, vsub(eb, ea), fe);
 }
 
-// ds/(c_s + |v|) of one state (calc_timestep body, physics.rs:187-189).
-__device__ __forceinline__ float wave_dt1(const float w[5], const FK &k) {
-    const float g = k.gamma * w[4];
-    const float cs = g * rsqrtf(g * w[0]);
-    const float vm = sqrtf(fmaf(w[3], w[3], fmaf(w[2], w[2], w[1] * w[1])));
-    return k.ds * __fdividef(1.0f, cs + vm);
-}
-
 __device__ __forceinline__ float comp(f2 v, int i) { return i ? v.y : v.x; }
 __device__ __forceinline__ void setc(f2 &v, int i, float s) {
     if (i) v.y = s;
     else v.x = s;
 }
 
+// W warps, each owning 32 columns x 2 rows (a y-pair per thread): the tile
+// is TY = 2W rows x 32 columns.  The tile's halo ring (rows y0-1 and y0+TY,
+// columns z0-1 and z0+32) is computed two cells per thread with the same
+// packed code by the first 32+TY threads, and the tile's edge faces by the
+// first 16+TY/2.
 template <int W, int R> struct Smem {
     static constexpr int TY = 2 * W;
     static constexpr int NT = 32 * W;
+    static constexpr int NOWN = NT;
     static constexpr int RY = TY + 4;
     static constexpr int kFieldElems = RY * kRZ;
     static constexpr int kBoxBytes = 5 * kFieldElems * 4;
     static constexpr int kSlotElems = ((kBoxBytes + 127) / 128) * 128 / 4;
 
     float ring[R * kSlotElems];   // TMA destinations; primitives after conversion
-    f2 own_cons[3][5][NT];        // each thread's conserved pair, 3 planes
+    f2 own_cons[3][5][NOWN];      // each own thread's conserved pair, 3 planes
     float ypl[W + 1][5][32];      // y+ states: [0] halo row y0-1, [w+1] upper row of pair w
     float ymn_top[5][32];         // y- state of halo row y0+TY
     float zpl_left[5][TY];        // z+ state of halo column z0-1
@@ -181,7 +179,7 @@ template <int W, int R> struct Smem {
 
 template <int W, int R> struct Kernel {
     using Sm = Smem<W, R>;
-    static constexpr int TY = Sm::TY, NT = Sm::NT;
+    static constexpr int TY = Sm::TY, NT = Sm::NT, NOWN = Sm::NOWN;
 
     static __device__ __forceinline__ float &P(Sm &s, int slot, int f, int ry, int rz) {
         return s.ring[slot * Sm::kSlotElems + f * Sm::kFieldElems + ry * kRZ + rz];
@@ -235,20 +233,25 @@ template <int W, int R> struct Kernel {
                                                     bool val1, int gy0, int gzo, int nyi0, int nyi1, int nzi,
                                                     const int *yimg0, const int *yflp0, const int *yimg1,
                                                     const int *yflp1, const int *zimg, const int *zflp,
-                                                    bool col_img, double sum[5], float &wmin, unsigned &nanf) {
+                                                    bool col_img, double sum[5], float &smax) {
         f2 q[5];
         prim(u, q, k);
+        smax = max_nan(smax, fast_speed(q[0].x, q[1].x, q[2].x, q[3].x, q[4].x, k.gamma));
+        if (val1) smax = max_nan(smax, fast_speed(q[0].y, q[1].y, q[2].y, q[3].y, q[4].y, k.gamma));
+        // the pair is added in FP32, then accumulated in FP64
 #pragma unroll
-        for (int r = 0; r < 2; ++r) {
-            if (r == 1 && !val1) break;
-            float qq[5];
+        for (int f = 0; f < 5; ++f) sum[f] += (double)(val1 ? u[f].x + u[f].y : u[f].x);
+        // ghost images exist only next to the x faces or on boundary columns
+        const bool x_edge = xu <= 3 || xu >= a.nx - 4;
+        if (!x_edge && !col_img) {
+            const long long o0 = ((long long)xu * a.ny + gy0) * a.pitch + gzo;
+            const long long o1 = o0 + a.pitch;
 #pragma unroll
-            for (int f = 0; f < 5; ++f) qq[f] = comp(q[f], r);
-            const float wd = wave_dt1(qq, k);
-            if (wd != wd) nanf = 1;
-            else wmin = fminf(wmin, wd);
-#pragma unroll
-            for (int f = 0; f < 5; ++f) sum[f] += (double)comp(u[f], r);
+            for (int f = 0; f < 5; ++f) {
+                a.dst[f * a.fstride + o0] = u[f].x;
+                if (val1) a.dst[f * a.fstride + o1] = u[f].y;
+            }
+            return;
         }
         int ximg[4], xflp[4];
         const int nxi = axis_images(xu, a.nx, a.bc[0], a.bc[1], ximg, xflp);
@@ -282,10 +285,53 @@ template <int W, int R> struct Kernel {
         }
     }
 
+    // Predicted state and slopes of two arbitrary cells A, B (region
+    // coordinates) as one packed computation, or cell by cell with the
+    // boundary rules when either is outside the interior.
+    static __device__ __forceinline__ void pair_state(Sm &s, const GridArgs<float> &a, const FK &k, float hd, int sm,
+                                                      int s0, int sp, int ryA, int rzA, int ryB, int rzB, int y0, int z0,
+                                                      f2 xt[5], f2 sx[5], f2 sy[5], f2 sz[5]) {
+        const int gyA = y0 - 2 + ryA, gzA = z0 - 2 + rzA, gyB = y0 - 2 + ryB, gzB = z0 - 2 + rzB;
+        const bool regA = gyA >= 2 && gyA <= a.ny - 3 && gzA >= 2 && gzA <= a.nz - 3;
+        const bool regB = gyB >= 2 && gyB <= a.ny - 3 && gzB >= 2 && gzB <= a.nz - 3;
+        if (regA && regB) {
+            f2 c[5];
+#pragma unroll
+            for (int f = 0; f < 5; ++f) {
+                c[f] = make_float2(P(s, s0, f, ryA, rzA), P(s, s0, f, ryB, rzB));
+                const f2 xm = make_float2(P(s, sm, f, ryA, rzA), P(s, sm, f, ryB, rzB));
+                const f2 xp = make_float2(P(s, sp, f, ryA, rzA), P(s, sp, f, ryB, rzB));
+                const f2 ym = make_float2(P(s, s0, f, ryA - 1, rzA), P(s, s0, f, ryB - 1, rzB));
+                const f2 yp = make_float2(P(s, s0, f, ryA + 1, rzA), P(s, s0, f, ryB + 1, rzB));
+                const f2 zm = make_float2(P(s, s0, f, ryA, rzA - 1), P(s, s0, f, ryB, rzB - 1));
+                const f2 zp = make_float2(P(s, s0, f, ryA, rzA + 1), P(s, s0, f, ryB, rzB + 1));
+                sx[f] = slope(xm, c[f], xp, k.lim);
+                sy[f] = slope(ym, c[f], yp, k.lim);
+                sz[f] = slope(zm, c[f], zp, k.lim);
+            }
+            predict(c, sx, sy, sz, hd, k, xt);
+        } else {
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                float t[5], gx[5], gy[5], gz[5];
+                cell_scalar(s, a, k, hd, sm, s0, sp, r ? ryB : ryA, r ? rzB : rzA, r ? gyB : gyA, r ? gzB : gzA, t, gx,
+                            gy, gz);
+#pragma unroll
+                for (int f = 0; f < 5; ++f) {
+                    setc(xt[f], r, t[f]);
+                    setc(sx[f], r, gx[f]);
+                    setc(sy[f], r, gy[f]);
+                    setc(sz[f], r, gz[f]);
+                }
+            }
+        }
+    }
+
     static __device__ void run(const GridArgs<float> &a, const CUtensorMap *tmap, int chunk, unsigned char *raw) {
         Sm &s = *reinterpret_cast<Sm *>(raw);
         const int lane = threadIdx.x, w = threadIdx.y;
         const int tid = w * 32 + lane;
+        constexpr bool own = true;
 
         const int tiles_z = (a.nz - 4 + kTZ - 1) / kTZ;
         const int tiles_y = (a.ny - 4 + TY - 1) / TY;
@@ -297,11 +343,12 @@ template <int W, int R> struct Kernel {
         const int xs = 2 + cx * chunk;
         const int xe = min(xs + chunk, a.nx - 2);
         const int np = xe - xs + 4;
-        const int gy0 = y0 + 2 * w, gy1 = gy0 + 1, gzo = z0 + lane;   // own pair
+        // own pair (own warps): rows y0+2w, y0+2w+1 at column z0+lane
+        const int gy0 = y0 + 2 * w, gy1 = gy0 + 1, gzo = z0 + lane;
         const int ry0 = 2 + 2 * w, ry1 = ry0 + 1, rzo = lane + 2;
-        const bool zval = gzo <= a.nz - 3;
+        const bool zval = own && gzo <= a.nz - 3;
         const bool val0 = zval && gy0 <= a.ny - 3, val1 = zval && gy1 <= a.ny - 3;
-        const bool regular = val1;   // both rows and the column interior
+        const bool regular = val1;
 
         if (*(volatile unsigned *)&a.ctl->flags & kStatusTimeout) return;
         const unsigned step = (unsigned)a.ctl->step;
@@ -345,11 +392,13 @@ template <int W, int R> struct Kernel {
 #pragma unroll
         for (int f = 0; f < 5; ++f) xt_prev[f] = sx_prev[f] = acc[f] = make_float2(0.f, 0.f);
         double sum[5] = {0, 0, 0, 0, 0};
-        float wmin = INFINITY;
-        unsigned nanf = 0;
+        float smax = 0.0f;   // max wave speed of the updated cells (NaN-propagating)
 
         constexpr int HR = 4 * kRZ + 4 * TY;   // staged halo cells (rows 0,1,TY+2,TY+3; cols 0,1,34,35)
 
+        // (a) wait for staged plane l, convert to primitives in place: own
+        // warps their pairs (keeping the conserved values), halo warps the
+        // staged halo cells
         auto convert = [&](int l) -> bool {
             const int slot = l % R;
             if (!mbar_wait(&s.bar[slot], (l / R) & 1, kWaitBudget)) return false;
@@ -365,23 +414,25 @@ template <int W, int R> struct Kernel {
                     s.own_cons[l % 3][f][tid] = u[f];
                 }
             }
-            for (int h = tid; h < HR; h += NT) {
-                int ry, rz;
-                if (h < 4 * kRZ) {
-                    const int r4 = h / kRZ;
-                    rz = h - r4 * kRZ;
-                    ry = r4 < 2 ? r4 : TY + r4;
-                } else {
-                    const int j = h - 4 * kRZ, c4 = j & 3;
-                    ry = 2 + (j >> 2);
-                    rz = c4 < 2 ? c4 : kTZ + c4;
+            {
+                for (int h = tid; h < HR; h += NT) {
+                    int ry, rz;
+                    if (h < 4 * kRZ) {
+                        const int r4 = h / kRZ;
+                        rz = h - r4 * kRZ;
+                        ry = r4 < 2 ? r4 : TY + r4;
+                    } else {
+                        const int j = h - 4 * kRZ, c4 = j & 3;
+                        ry = 2 + (j >> 2);
+                        rz = c4 < 2 ? c4 : kTZ + c4;
+                    }
+                    float u[5], q[5];
+#pragma unroll
+                    for (int f = 0; f < 5; ++f) u[f] = P(s, slot, f, ry, rz);
+                    prim(u, q, k);
+#pragma unroll
+                    for (int f = 0; f < 5; ++f) P(s, slot, f, ry, rz) = q[f];
                 }
-                float u[5], q[5];
-#pragma unroll
-                for (int f = 0; f < 5; ++f) u[f] = P(s, slot, f, ry, rz);
-                prim(u, q, k);
-#pragma unroll
-                for (int f = 0; f < 5; ++f) P(s, slot, f, ry, rz) = q[f];
             }
             return true;
         };
@@ -400,109 +451,95 @@ template <int W, int R> struct Kernel {
             const int sm = (l - 2) % R, s0 = (l - 1) % R, sp = l % R;
             const bool plane_upd = m >= xs && m < xe;
 
-            // ---- (b) own pair: slopes and prediction ------------------------
-            f2 xt[5], sx[5], sy[5], sz[5];
-            if (regular) {
-                f2 c[5];
-#pragma unroll
-                for (int f = 0; f < 5; ++f) {
-                    c[f] = make_float2(P(s, s0, f, ry0, rzo), P(s, s0, f, ry1, rzo));
-                    const f2 xm = make_float2(P(s, sm, f, ry0, rzo), P(s, sm, f, ry1, rzo));
-                    const f2 xp = make_float2(P(s, sp, f, ry0, rzo), P(s, sp, f, ry1, rzo));
-                    const f2 ym = make_float2(P(s, s0, f, ry0 - 1, rzo), c[f].x);
-                    const f2 yp = make_float2(c[f].y, P(s, s0, f, ry1 + 1, rzo));
-                    const f2 zm = make_float2(P(s, s0, f, ry0, rzo - 1), P(s, s0, f, ry1, rzo - 1));
-                    const f2 zp = make_float2(P(s, s0, f, ry0, rzo + 1), P(s, s0, f, ry1, rzo + 1));
-                    sx[f] = slope(xm, c[f], xp, lim);
-                    sy[f] = slope(ym, c[f], yp, lim);
-                    sz[f] = slope(zm, c[f], zp, lim);
-                }
-                predict(c, sx, sy, sz, hd, k, xt);
-            } else {
-#pragma unroll
-                for (int r = 0; r < 2; ++r) {
-                    float t[5], gx[5], gy[5], gz[5];
-                    cell_scalar(s, a, k, hd, sm, s0, sp, ry0 + r, rzo, gy0 + r, gzo, t, gx, gy, gz);
+            // ---- (b') tile halo ring: rows y0-1 / y0+TY of each column, columns
+            // z0-1 / z0+32 of each row, one pair per thread
+            if (plane_upd && tid < 32 + TY) {
+                const bool rows = tid < 32;
+                const int hyA = rows ? 1 : tid - 32 + 2, hzA = rows ? tid + 2 : 1;
+                const int hyB = rows ? TY + 2 : tid - 32 + 2, hzB = rows ? tid + 2 : kTZ + 2;
+                f2 hxt[5], hsx[5], hsy[5], hsz[5];
+                pair_state(s, a, k, hd, sm, s0, sp, hyA, hzA, hyB, hzB, y0, z0, hxt, hsx, hsy, hsz);
+                if (rows) {
 #pragma unroll
                     for (int f = 0; f < 5; ++f) {
-                        setc(xt[f], r, t[f]);
-                        setc(sx[f], r, gx[f]);
-                        setc(sy[f], r, gy[f]);
-                        setc(sz[f], r, gz[f]);
+                        s.ypl[0][f][tid] = fmaf(hsy[f].x, 0.5f, hxt[f].x);
+                        s.ymn_top[f][tid] = fmaf(hsy[f].y, -0.5f, hxt[f].y);
+                    }
+                } else {
+#pragma unroll
+                    for (int f = 0; f < 5; ++f) {
+                        s.zpl_left[f][tid - 32] = fmaf(hsz[f].x, 0.5f, hxt[f].x);
+                        s.zmn_right[f][tid - 32] = fmaf(hsz[f].y, -0.5f, hxt[f].y);
                     }
                 }
             }
-            // publish the face states other threads need: the upper row's
-            // y+ state (pair above) and, from lane 31, the z+ states (edge pass)
-            if (plane_upd) {
+            f2 xt[5], sx[5], sy[5], sz[5], fx[5];
+            if (own) {
+                // ---- (b) own pair: slopes and prediction --------------------
+                if (regular) {
+                    f2 c[5];
+#pragma unroll
+                    for (int f = 0; f < 5; ++f) {
+                        c[f] = make_float2(P(s, s0, f, ry0, rzo), P(s, s0, f, ry1, rzo));
+                        const f2 xm = make_float2(P(s, sm, f, ry0, rzo), P(s, sm, f, ry1, rzo));
+                        const f2 xp = make_float2(P(s, sp, f, ry0, rzo), P(s, sp, f, ry1, rzo));
+                        const f2 ym = make_float2(P(s, s0, f, ry0 - 1, rzo), c[f].x);
+                        const f2 yp = make_float2(c[f].y, P(s, s0, f, ry1 + 1, rzo));
+                        const f2 zm = make_float2(P(s, s0, f, ry0, rzo - 1), P(s, s0, f, ry1, rzo - 1));
+                        const f2 zp = make_float2(P(s, s0, f, ry0, rzo + 1), P(s, s0, f, ry1, rzo + 1));
+                        sx[f] = slope(xm, c[f], xp, lim);
+                        sy[f] = slope(ym, c[f], yp, lim);
+                        sz[f] = slope(zm, c[f], zp, lim);
+                    }
+                    predict(c, sx, sy, sz, hd, k, xt);
+                } else {
+                    pair_state(s, a, k, hd, sm, s0, sp, ry0, rzo, ry1, rzo, y0, z0, xt, sx, sy, sz);
+                }
+                // publish the face states other threads need: the upper row's
+                // y+ state (pair above) and, from lane 31, the z+ states (edge)
+                if (plane_upd) {
+#pragma unroll
+                    for (int f = 0; f < 5; ++f) {
+                        s.ypl[w + 1][f][lane] = fmaf(sy[f].y, 0.5f, xt[f].y);
+                        if (lane == 31) {
+                            s.zpl_edge[f][2 * w] = fmaf(sz[f].x, 0.5f, xt[f].x);
+                            s.zpl_edge[f][2 * w + 1] = fmaf(sz[f].y, 0.5f, xt[f].y);
+                        }
+                    }
+                }
+                // ---- (c) x-face between planes m-1 and m ---------------------
+                if (m >= xs) {
+                    if (m == 2 && a.bc[0] == kWall) {
+#pragma unroll
+                        for (int f = 0; f < 5; ++f) xt_prev[f] = xt[f];
+                        xt_prev[1] = vmul(xt_prev[1], S<f2>(-1.0f));
+                    }
+                    if (m == a.nx - 2) {
+                        if (a.bc[1] == kOutflow) {
+#pragma unroll
+                            for (int f = 0; f < 5; ++f) { xt[f] = xt_prev[f]; sx[f] = sx_prev[f]; }
+                        } else if (a.bc[1] == kWall) {
+#pragma unroll
+                            for (int f = 0; f < 5; ++f) xt[f] = xt_prev[f];
+                            xt[1] = vmul(xt[1], S<f2>(-1.0f));
+                        }
+                    }
+                    f2 lo[5], up[5];
+#pragma unroll
+                    for (int f = 0; f < 5; ++f) {
+                        lo[f] = vfma(sx_prev[f], S<f2>(0.5f), xt_prev[f]);
+                        up[f] = vfma(sx[f], S<f2>(-0.5f), xt[f]);
+                    }
+                    face<1>(lo, up, false, S<f2>(0.f), k, fx);
+                } else {
+#pragma unroll
+                    for (int f = 0; f < 5; ++f) fx[f] = make_float2(0.f, 0.f);
+                }
 #pragma unroll
                 for (int f = 0; f < 5; ++f) {
-                    s.ypl[w + 1][f][lane] = fmaf(sy[f].y, 0.5f, xt[f].y);
-                    if (lane == 31) {
-                        s.zpl_edge[f][2 * w] = fmaf(sz[f].x, 0.5f, xt[f].x);
-                        s.zpl_edge[f][2 * w + 1] = fmaf(sz[f].y, 0.5f, xt[f].y);
-                    }
+                    xt_prev[f] = xt[f];
+                    sx_prev[f] = sx[f];
                 }
-                // tile halo ring, two cells per work unit
-                for (int h = tid; h < 32 + TY; h += NT) {
-                    int ryA, rzA, ryB, rzB;
-                    if (h < 32) {   // rows y0-1 and y0+TY of column h
-                        ryA = 1; rzA = h + 2; ryB = TY + 2; rzB = h + 2;
-                    } else {        // columns z0-1 and z0+32 of row h-32
-                        ryA = ryB = h - 32 + 2; rzA = 1; rzB = kTZ + 2;
-                    }
-                    float t[2][5], gx[5], gy[2][5], gz[2][5];
-                    cell_scalar(s, a, k, hd, sm, s0, sp, ryA, rzA, y0 - 2 + ryA, z0 - 2 + rzA, t[0], gx, gy[0], gz[0]);
-                    cell_scalar(s, a, k, hd, sm, s0, sp, ryB, rzB, y0 - 2 + ryB, z0 - 2 + rzB, t[1], gx, gy[1], gz[1]);
-                    if (h < 32) {
-#pragma unroll
-                        for (int f = 0; f < 5; ++f) {
-                            s.ypl[0][f][h] = t[0][f] + 0.5f * gy[0][f];
-                            s.ymn_top[f][h] = t[1][f] - 0.5f * gy[1][f];
-                        }
-                    } else {
-#pragma unroll
-                        for (int f = 0; f < 5; ++f) {
-                            s.zpl_left[f][h - 32] = t[0][f] + 0.5f * gz[0][f];
-                            s.zmn_right[f][h - 32] = t[1][f] - 0.5f * gz[1][f];
-                        }
-                    }
-                }
-            }
-
-            // ---- (c) x-face between planes m-1 and m ---------------------------
-            f2 fx[5];
-            if (m >= xs) {
-                if (m == 2 && a.bc[0] == kWall) {
-#pragma unroll
-                    for (int f = 0; f < 5; ++f) xt_prev[f] = xt[f];
-                    xt_prev[1] = vmul(xt_prev[1], S<f2>(-1.0f));
-                }
-                if (m == a.nx - 2) {
-                    if (a.bc[1] == kOutflow) {
-#pragma unroll
-                        for (int f = 0; f < 5; ++f) { xt[f] = xt_prev[f]; sx[f] = sx_prev[f]; }
-                    } else if (a.bc[1] == kWall) {
-#pragma unroll
-                        for (int f = 0; f < 5; ++f) xt[f] = xt_prev[f];
-                        xt[1] = vmul(xt[1], S<f2>(-1.0f));
-                    }
-                }
-                f2 lo[5], up[5];
-#pragma unroll
-                for (int f = 0; f < 5; ++f) {
-                    lo[f] = vfma(sx_prev[f], S<f2>(0.5f), xt_prev[f]);
-                    up[f] = vfma(sx[f], S<f2>(-0.5f), xt[f]);
-                }
-                face<1>(lo, up, false, S<f2>(0.f), k, fx);
-            } else {
-#pragma unroll
-                for (int f = 0; f < 5; ++f) fx[f] = make_float2(0.f, 0.f);
-            }
-#pragma unroll
-            for (int f = 0; f < 5; ++f) {
-                xt_prev[f] = xt[f];
-                sx_prev[f] = sx[f];
             }
             __syncthreads();   // S2: halo states and pair publications ready; slot of m-1 free
 
@@ -513,9 +550,9 @@ template <int W, int R> struct Kernel {
             }
             if (issued < np) ++issued;
 
-            // ---- (d) y- and z-faces of plane m -------------------------------
+            // ---- (d) y- and z-faces of plane m --------------------------------
             f2 fy[5], fz[5];
-            if (plane_upd) {
+            if (plane_upd && own) {
                 {   // y: faces (y0+2w-1 | y0+2w) and (y0+2w | y0+2w+1)
                     f2 lo[5], up[5];
 #pragma unroll
@@ -542,81 +579,79 @@ template <int W, int R> struct Kernel {
                     const float ghs = grav ? grav_h(a, gzo - 1) : 0.f;
                     face<3>(lo, up, grav, make_float2(ghs, ghs), k, fz);
                 }
-                // tile edge faces: y (y0+TY-1 | y0+TY) x 32 and z (z0+31 | z0+32) x TY,
-                // two per work unit
-                for (int h = tid; h < 16 + TY / 2; h += NT) {
-                    if (h < 16) {
-                        f2 lo[5], up[5], F[5];
+            }
+            if (plane_upd && tid < 16 + TY / 2) {
+                // tile edge faces: y (y0+TY-1 | y0+TY) x 32 and z (z0+31 | z0+32) x TY
+                if (tid < 16) {
+                    const int h = tid;
+                    f2 lo[5], up[5], F[5];
 #pragma unroll
-                        for (int f = 0; f < 5; ++f) {
-                            lo[f] = make_float2(s.ypl[W][f][h], s.ypl[W][f][h + 16]);
-                            up[f] = make_float2(s.ymn_top[f][h], s.ymn_top[f][h + 16]);
-                        }
-                        face<2>(lo, up, false, S<f2>(0.f), k, F);
+                    for (int f = 0; f < 5; ++f) {
+                        lo[f] = make_float2(s.ypl[W][f][h], s.ypl[W][f][h + 16]);
+                        up[f] = make_float2(s.ymn_top[f][h], s.ymn_top[f][h + 16]);
+                    }
+                    face<2>(lo, up, false, S<f2>(0.f), k, F);
 #pragma unroll
-                        for (int f = 0; f < 5; ++f) {
-                            s.fy_edge[f][h] = F[f].x;
-                            s.fy_edge[f][h + 16] = F[f].y;
-                        }
-                    } else {
-                        const int r = h - 16;
-                        f2 lo[5], up[5], F[5];
+                    for (int f = 0; f < 5; ++f) {
+                        s.fy_edge[f][h] = F[f].x;
+                        s.fy_edge[f][h + 16] = F[f].y;
+                    }
+                } else {
+                    const int r = tid - 16;
+                    f2 lo[5], up[5], F[5];
 #pragma unroll
-                        for (int f = 0; f < 5; ++f) {
-                            lo[f] = make_float2(s.zpl_edge[f][r], s.zpl_edge[f][r + TY / 2]);
-                            up[f] = make_float2(s.zmn_right[f][r], s.zmn_right[f][r + TY / 2]);
-                        }
-                        const float ghs = grav ? grav_h(a, z0 + kTZ - 1) : 0.f;
-                        face<3>(lo, up, grav, make_float2(ghs, ghs), k, F);
+                    for (int f = 0; f < 5; ++f) {
+                        lo[f] = make_float2(s.zpl_edge[f][r], s.zpl_edge[f][r + TY / 2]);
+                        up[f] = make_float2(s.zmn_right[f][r], s.zmn_right[f][r + TY / 2]);
+                    }
+                    const float ghs = grav ? grav_h(a, z0 + kTZ - 1) : 0.f;
+                    face<3>(lo, up, grav, make_float2(ghs, ghs), k, F);
 #pragma unroll
-                        for (int f = 0; f < 5; ++f) {
-                            s.fz_edge[f][r] = F[f].x;
-                            s.fz_edge[f][r + TY / 2] = F[f].y;
-                        }
+                    for (int f = 0; f < 5; ++f) {
+                        s.fz_edge[f][r] = F[f].x;
+                        s.fz_edge[f][r + TY / 2] = F[f].y;
                     }
                 }
-            } else {
-#pragma unroll
-                for (int f = 0; f < 5; ++f) fy[f] = fz[f] = make_float2(0.f, 0.f);
             }
             __syncthreads();   // S3: published fluxes ready
 
-            // (e) update plane m-1: cons - scale * (fx_hi + acc)
-            const int xu = m - 1;
-            if (xu >= xs && xu < xe && val0) {
-                const bool x_out = xu == 2 && a.bc[0] == kOutflow;   // acc holds no x-flux then
-                const int cs = (xu - xs + 2) % 3;
-                f2 u[5];
+            if (own) {
+                // ---- (e) update plane m-1: cons - scale * (fx_hi + acc) -------
+                const int xu = m - 1;
+                if (xu >= xs && xu < xe && val0) {
+                    const bool x_out = xu == 2 && a.bc[0] == kOutflow;   // acc holds no x-flux then
+                    const int cs = (xu - xs + 2) % 3;
+                    f2 u[5];
 #pragma unroll
-                for (int f = 0; f < 5; ++f) {
-                    const f2 cA = s.own_cons[cs][f][tid];
-                    const f2 t = x_out ? acc[f] : vadd(fx[f], acc[f]);
-                    u[f] = vfma(S<f2>(-k.scale), t, cA);
+                    for (int f = 0; f < 5; ++f) {
+                        const f2 cA = s.own_cons[cs][f][tid];
+                        const f2 t = x_out ? acc[f] : vadd(fx[f], acc[f]);
+                        u[f] = vfma(S<f2>(-k.scale), t, cA);
+                    }
+                    epilogue(a, k, xu, u, val1, gy0, gzo, nyi0, nyi1, nzi, yimg0, yflp0, yimg1, yflp1, zimg, zflp,
+                             col_img, sum, smax);
                 }
-                epilogue(a, k, xu, u, val1, gy0, gzo, nyi0, nyi1, nzi, yimg0, yflp0, yimg1, yflp1, zimg, zflp,
-                         col_img, sum, wmin, nanf);
-            }
-
-            if (plane_upd) {
-                // lower x-outflow face repeats the next face's flux: plane 2
-                // gets no x-divergence (boundaries.rs:107-111 on the fluxes)
-                const bool x_out = m == 2 && a.bc[0] == kOutflow;
-                const bool y_out = gy0 == 2 && a.bc[2] == kOutflow;
-                const bool z_out = gzo == 2 && a.bc[4] == kOutflow;
+                if (plane_upd) {
+                    // lower x-outflow face repeats the next face's flux: plane 2
+                    // gets no x-divergence (boundaries.rs:107-111 on the fluxes)
+                    const bool x_out = m == 2 && a.bc[0] == kOutflow;
+                    const bool y_out = gy0 == 2 && a.bc[2] == kOutflow;
+                    const bool z_out = gzo == 2 && a.bc[4] == kOutflow;
 #pragma unroll
-                for (int f = 0; f < 5; ++f) {
-                    const float fy_top = (w + 1 < W) ? s.fy_pub[w + 1][f][lane] : s.fy_edge[f][lane];
-                    f2 dy;
-                    // lower outflow face repeats the next face's flux (cell 2 sees none)
-                    dy.x = y_out ? 0.f : fy[f].y - fy[f].x;
-                    dy.y = fy_top - fy[f].y;
-                    f2 zh;
-                    zh.x = __shfl_down_sync(0xffffffffu, fz[f].x, 1);
-                    zh.y = __shfl_down_sync(0xffffffffu, fz[f].y, 1);
-                    if (lane == 31) zh = make_float2(s.fz_edge[f][2 * w], s.fz_edge[f][2 * w + 1]);
-                    const f2 dz = z_out ? make_float2(0.f, 0.f) : vsub(zh, fz[f]);
-                    const f2 d = vadd(dy, dz);
-                    acc[f] = x_out ? d : vsub(d, fx[f]);
+                    for (int f = 0; f < 5; ++f) {
+                        const float fy_top = (w + 1 < W) ? s.fy_pub[w + 1][f][lane] : s.fy_edge[f][lane];
+                        f2 dy;
+                        // lower outflow face repeats the next face's flux (cell 2 sees none)
+                        dy.x = y_out ? 0.f : fy[f].y - fy[f].x;
+                        dy.y = fy_top - fy[f].y;
+                        f2 zh;
+                        zh.x = __shfl_down_sync(0xffffffffu, fz[f].x, 1);
+                        zh.y = __shfl_down_sync(0xffffffffu, fz[f].y, 1);
+                        if (lane == 31) zh = make_float2(s.fz_edge[f][2 * w], s.fz_edge[f][2 * w + 1]);
+                        const f2 dz = z_out ? make_float2(0.f, 0.f) : vsub(zh, fz[f]);
+                        const f2 d = vadd(dy, dz);
+                        acc[f] = x_out ? d : vsub(d, fx[f]);
+                    }
                 }
             }
         }
@@ -629,7 +664,10 @@ template <int W, int R> struct Kernel {
             }
             return;
         }
-        if (block_partial(a, sum, (double)wmin, nanf, tid, NT, s.red, &s.is_last)) {
+        // min over cells of ds/speed = ds / max speed
+        const unsigned nanf = smax != smax;
+        const double wmin = nanf ? INFINITY : (double)__fdiv_rn(k.ds, smax);
+        if (block_partial(a, sum, wmin, nanf, tid, NT, s.red, &s.is_last)) {
             __threadfence();
             final_reduce<float>(a, tid, NT, s.red, kAdvance);
         }
@@ -638,7 +676,8 @@ template <int W, int R> struct Kernel {
 
 template <int W, int R>
 __global__ void __launch_bounds__(32 * W, 2) fast_step_kernel(const GridArgs<float> a,
-                                                           const __grid_constant__ CUtensorMap tmap, int chunk) {
+                                                                   const __grid_constant__ CUtensorMap tmap,
+                                                                   int chunk) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     Kernel<W, R>::run(a, &tmap, chunk, smem_raw);
 }

@@ -61,9 +61,14 @@ constexpr int kReduceBlocks = 148 * 8;   // grid of the state-reduction kernel
 // (dg_step_impl.cuh) and the fast float kernel (dg_fast_impl.cuh).
 enum KernelKind : int { kRefF64 = 0, kRefF32 = 1, kFastF32 = 2 };
 
+// Warps of the fast kernel; each owns 2 rows of the tile.
+constexpr int kFastOwnWarps = 8;
+
 // Tile rows (y) of each kernel; every tile is 32 cells wide in z.
-inline int step_tile_rows(int kind) { return kind == kRefF64 ? 4 : (kind == kRefF32 ? 8 : 16); }
-inline int step_threads(int kind) { return kind == kFastF32 ? 32 * 8 : 32 * step_tile_rows(kind); }
+inline int step_tile_rows(int kind) {
+    return kind == kRefF64 ? 4 : (kind == kRefF32 ? 8 : 2 * kFastOwnWarps);
+}
+inline int step_threads(int kind) { return kind == kFastF32 ? 32 * kFastOwnWarps : 32 * step_tile_rows(kind); }
 
 // Blocks of one step launch: (y tiles) x (z tiles) x (x chunks of `chunk`
 // planes).
@@ -74,15 +79,16 @@ inline int step_grid_blocks(int nx, int ny, int nz, int kind, int chunk) {
     const int chunks = (nx - 4 + chunk - 1) / chunk;
     return tiles_z * tiles_y * chunks;
 }
-// Default x-planes per block: enough blocks for ~4 waves of resident CTAs
-// (2 per SM on 148 SMs), at least 8 planes per block.
+// Default x-planes per block: enough blocks for ~14 waves of resident CTAs
+// (2 per SM on 148 SMs; measured best on 512^3: 64 planes per block), at
+// least 32 planes per block (each block re-stages 4 planes at its ends).
 inline int choose_chunk(int nx, int ny, int nz, int kind) {
     const int ty = step_tile_rows(kind);
     const long long tiles = (long long)((ny - 4 + ty - 1) / ty) * ((nz - 4 + kTZ - 1) / kTZ);
     const int nxi = nx - 4;
-    const long long target = 148LL * 2 * 4;
+    const long long target = 148LL * 2 * 14;
     long long chunks = (target + tiles - 1) / tiles;
-    const long long maxc = nxi / 8 > 0 ? nxi / 8 : 1;
+    const long long maxc = nxi / 32 > 0 ? nxi / 32 : 1;
     if (chunks > maxc) chunks = maxc;
     if (chunks < 1) chunks = 1;
     return (int)((nxi + chunks - 1) / chunks);

@@ -54,6 +54,28 @@ template <class T> __device__ __forceinline__ T minmod(T a, T b) {
 
 template <class T, bool EXACT> struct Phys;
 
+// NaN-propagating maximum (PTX max.NaN): a NaN wave speed anywhere must
+// reach the reduction, as it does in the reference (physics.rs:191-195).
+__device__ __forceinline__ float max_nan(float a, float b) {
+    float r;
+    asm("max.NaN.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+    return r;
+}
+
+// Fast-policy wave speed c_s + |v| of one primitive state (the quantity
+// whose maximum sets dt, physics.rs:186-190): sqrt(gamma p / rho) as
+// g*rsqrt(g*rho) with g = gamma p, |v| as v2*rsqrt(v2).  The fast kernels
+// take dt = CFL * ds / max(speed), the same minimum as CFL * min(ds/speed)
+// without a divide per cell.  Explicit _rn operations: every kernel that
+// calls this rounds the same way.
+__device__ __forceinline__ float fast_speed(float rho, float vx, float vy, float vz, float p, float gamma) {
+    const float g = __fmul_rn(gamma, p);
+    const float cs = __fmul_rn(g, rsqrtf(__fmul_rn(g, rho)));
+    const float v2 = __fmaf_rn(vz, vz, __fmaf_rn(vy, vy, __fmul_rn(vx, vx)));
+    const float vm = __fmul_rn(v2, rsqrtf(fmaxf(v2, 1e-30f)));
+    return __fadd_rn(cs, vm);
+}
+
 // ---------------------------------------------------------------------------
 // Reference rounding
 // ---------------------------------------------------------------------------
@@ -171,14 +193,6 @@ template <class T> struct Phys<T, false> {
         w[2] = vy;
         w[3] = vz;
         w[4] = fma(T(-0.5) * rho, v2, u[4] * k.inv_vol) * k.gm1;
-    }
-
-    // sqrt(gamma p / rho) as g * rsqrt(g * rho), g = gamma p
-    static __device__ __forceinline__ T wave_dt(const T w[5], const Consts<T> &k) {
-        const T g = k.gamma * w[4];
-        const T cs = g * rsqrt(g * w[0]);
-        const T vm = sqrt(fma(w[3], w[3], fma(w[2], w[2], w[1] * w[1])));
-        return k.ds * fast_rcp(cs + vm);
     }
 
     template <int LIM> static __device__ __forceinline__ T slope(T qm, T q0, T qp, const Consts<T> &k) {

@@ -6,7 +6,7 @@
 namespace dg {
 
 cudaError_t launch_fast_step(const GridArgs<float> &a, const CUtensorMap *tmap, int chunk, cudaStream_t st) {
-    constexpr int W = 8, R = 4;
+    constexpr int W = kFastOwnWarps, R = 4;
     using Sm = fastk::Smem<W, R>;
     auto kern = fastk::fast_step_kernel<W, R>;
     const int smem = (int)sizeof(Sm) + 1024;

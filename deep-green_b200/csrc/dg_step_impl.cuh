@@ -468,16 +468,25 @@ __global__ void __launch_bounds__(256) reduce_kernel(const GridArgs<T> a, int se
     double sum[5] = {0, 0, 0, 0, 0};
     double wm = INFINITY;
     unsigned nanf = 0;
+    float smax = 0.0f;   // fast policy: max wave speed (NaN-propagating)
     for (long long c = blockIdx.x * 256LL + tid; c < total; c += (long long)gridDim.x * 256) {
         const long long x = c / (nyi * nzi) + 2, y = (c / nzi) % nyi + 2, z = c % nzi + 2;
         const long long o = (x * a.ny + y) * a.pitch + z;
         T u[5], w[5];
         for (int f = 0; f < 5; ++f) u[f] = a.src[f * a.fstride + o];
         Phys<T, EXACT>::prim(u, w, a.k);
-        const T wd = Phys<T, EXACT>::wave_dt(w, a.k);
-        if (wd != wd) nanf = 1;
-        else wm = fmin(wm, (double)wd);
+        if constexpr (EXACT) {
+            const T wd = Phys<T, EXACT>::wave_dt(w, a.k);
+            if (wd != wd) nanf = 1;
+            else wm = fmin(wm, (double)wd);
+        } else {
+            smax = max_nan(smax, fast_speed(w[0], w[1], w[2], w[3], w[4], a.k.gamma));
+        }
         for (int f = 0; f < 5; ++f) sum[f] += (double)u[f];
+    }
+    if constexpr (!EXACT) {
+        if (smax != smax) nanf = 1;
+        else wm = (double)__fdiv_rn(a.k.ds, smax);
     }
     for (int o = 16; o > 0; o >>= 1) {
         for (int f = 0; f < 5; ++f) sum[f] += __shfl_xor_sync(0xffffffffu, sum[f], o);
