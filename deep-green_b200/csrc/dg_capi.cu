@@ -458,6 +458,16 @@ int32_t dg_conservation_sums(dg_ctx *c, double out[5]) {
     if (!c->has_state) return fail(c, DG_ERR_NO_STATE, "no state set");
     int r;
     if ((r = use_device(c)) != DG_OK) return r;
+    // FP64 sums of the current state, reduced on the device in a fixed order
+    cudaError_t e;
+    if (c->elem == 8) {
+        e = launch_reduce_policy<double, true>(grid_args<double>(c, c->buf[c->cur], nullptr), 0, c->stream);
+    } else {
+        auto a = grid_args<float>(c, c->buf[c->cur], nullptr);
+        e = c->exact ? launch_reduce_policy<float, true>(a, 0, c->stream)
+                     : launch_reduce_policy<float, false>(a, 0, c->stream);
+    }
+    if (e != cudaSuccess) return cuda_fail(c, e, "sum reduction");
     DG_CUDA(c, cudaMemcpyAsync(out, c->ctl->sums, 5 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     DG_CUDA(c, cudaStreamSynchronize(c->stream));
     return DG_OK;

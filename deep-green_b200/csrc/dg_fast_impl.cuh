@@ -168,9 +168,12 @@ template <int W, int R> struct Smem {
     float zpl_left[5][TY];        // z+ state of halo column z0-1
     float zmn_right[5][TY];       // z- state of halo column z0+32
     float zpl_edge[5][TY];        // z+ state of own column z0+31
-    float fy_pub[W][5][32];       // y-flux of the lower face of pair w
-    float fy_edge[5][32];         // y-flux of face (y0+TY-1 | y0+TY)
-    float fz_edge[5][TY];         // z-flux of face (z0+31 | z0+32)
+    // fluxes exchanged between threads, double-buffered by plane parity: a
+    // plane's divergence is completed after the next plane's first barrier
+    float fy_pub[2][W][5][32];    // y-flux of the lower face of pair w
+    float fy_edge[2][5][32];      // y-flux of face (y0+TY-1 | y0+TY)
+    float fz_edge[2][5][TY];      // z-flux of face (z0+31 | z0+32)
+    float fz_last[2][5][TY];      // lower z-flux of own column z0+31 (lane 31)
     uint64_t bar[R];
     double red[W * 7];
     int abort_flag;
@@ -227,20 +230,18 @@ template <int W, int R> struct Kernel {
         return a.k.g * (float(a.nz - 4) * a.k.ds - float(klow - 2) * a.k.ds);
     }
 
-    // New state of the pair: next-dt wave time, FP64 sums, and the store
-    // with its ghost-cell images.
+    // New state of the pair: its wave speed (next dt) and the store with its
+    // ghost-cell images.  (Conservation sums are computed on demand by the
+    // state reduction, not every step.)
     static __device__ __forceinline__ void epilogue(const GridArgs<float> &a, const FK &k, int xu, const f2 u[5],
                                                     bool val1, int gy0, int gzo, int nyi0, int nyi1, int nzi,
                                                     const int *yimg0, const int *yflp0, const int *yimg1,
                                                     const int *yflp1, const int *zimg, const int *zflp,
-                                                    bool col_img, double sum[5], float &smax) {
+                                                    bool col_img, float &smax) {
         f2 q[5];
         prim(u, q, k);
         smax = max_nan(smax, fast_speed(q[0].x, q[1].x, q[2].x, q[3].x, q[4].x, k.gamma));
         if (val1) smax = max_nan(smax, fast_speed(q[0].y, q[1].y, q[2].y, q[3].y, q[4].y, k.gamma));
-        // the pair is added in FP32, then accumulated in FP64
-#pragma unroll
-        for (int f = 0; f < 5; ++f) sum[f] += (double)(val1 ? u[f].x + u[f].y : u[f].x);
         // ghost images exist only next to the x faces or on boundary columns
         const bool x_edge = xu <= 3 || xu >= a.nx - 4;
         if (!x_edge && !col_img) {
@@ -389,9 +390,12 @@ template <int W, int R> struct Kernel {
         // plane, and acc = (y/z flux divergence of the previous plane) minus
         // (its lower x-face flux), so the update is cons - scale*(fx + acc)
         f2 xt_prev[5], sx_prev[5], acc[5];
+        float fyy[5];   // upper row's lower y-flux, kept until the face above it is known
 #pragma unroll
-        for (int f = 0; f < 5; ++f) xt_prev[f] = sx_prev[f] = acc[f] = make_float2(0.f, 0.f);
-        double sum[5] = {0, 0, 0, 0, 0};
+        for (int f = 0; f < 5; ++f) {
+            xt_prev[f] = sx_prev[f] = acc[f] = make_float2(0.f, 0.f);
+            fyy[f] = 0.f;
+        }
         float smax = 0.0f;   // max wave speed of the updated cells (NaN-propagating)
 
         constexpr int HR = 4 * kRZ + 4 * TY;   // staged halo cells (rows 0,1,TY+2,TY+3; cols 0,1,34,35)
@@ -446,10 +450,29 @@ template <int W, int R> struct Kernel {
             const int l = m - xs + 3;   // staged index of plane m+1
             if (!convert(l)) s.abort_flag = 1;
             fence_proxy_async();
-            __syncthreads();   // S1
+            __syncthreads();   // S1: primitives of planes m-1..m+1 and plane m-1's fluxes ready
             if (s.abort_flag) break;
             const int sm = (l - 2) % R, s0 = (l - 1) % R, sp = l % R;
             const bool plane_upd = m >= xs && m < xe;
+
+            // ---- (e1) complete the divergence of plane m-1 with the fluxes
+            // other threads published: the upper row's upper y-face and, on
+            // lane 31, the tile's edge z-face
+            if (m - 1 >= xs && m - 1 < xe) {
+                const int pb = (m - 1) & 1;
+                const bool z_out = gzo == 2 && a.bc[4] == kOutflow;
+#pragma unroll
+                for (int f = 0; f < 5; ++f) {
+                    // each deferred term enters as a difference of the two
+                    // faces, as the other terms did
+                    const float top = (w + 1 < W) ? s.fy_pub[pb][w + 1][f][lane] : s.fy_edge[pb][f][lane];
+                    acc[f].y += top - fyy[f];
+                    if (lane == 31 && !z_out) {
+                        acc[f].x += s.fz_edge[pb][f][2 * w] - s.fz_last[pb][f][2 * w];
+                        acc[f].y += s.fz_edge[pb][f][2 * w + 1] - s.fz_last[pb][f][2 * w + 1];
+                    }
+                }
+            }
 
             // ---- (b') tile halo ring: rows y0-1 / y0+TY of each column, columns
             // z0-1 / z0+32 of each row, one pair per thread
@@ -540,6 +563,21 @@ template <int W, int R> struct Kernel {
                     xt_prev[f] = xt[f];
                     sx_prev[f] = sx[f];
                 }
+                // ---- (e2) update plane m-1: cons - scale * (fx_hi + acc) ------
+                const int xu = m - 1;
+                if (xu >= xs && xu < xe && val0) {
+                    const bool x_out = xu == 2 && a.bc[0] == kOutflow;   // acc holds no x-flux then
+                    const int cs = (xu - xs + 2) % 3;
+                    f2 u[5];
+#pragma unroll
+                    for (int f = 0; f < 5; ++f) {
+                        const f2 cA = s.own_cons[cs][f][tid];
+                        const f2 t = x_out ? acc[f] : vadd(fx[f], acc[f]);
+                        u[f] = vfma(S<f2>(-k.scale), t, cA);
+                    }
+                    epilogue(a, k, xu, u, val1, gy0, gzo, nyi0, nyi1, nzi, yimg0, yflp0, yimg1, yflp1, zimg, zflp,
+                             col_img, smax);
+                }
             }
             __syncthreads();   // S2: halo states and pair publications ready; slot of m-1 free
 
@@ -562,7 +600,7 @@ template <int W, int R> struct Kernel {
                     }
                     face<2>(lo, up, false, S<f2>(0.f), k, fy);
 #pragma unroll
-                    for (int f = 0; f < 5; ++f) s.fy_pub[w][f][lane] = fy[f].x;
+                    for (int f = 0; f < 5; ++f) s.fy_pub[m & 1][w][f][lane] = fy[f].x;
                 }
                 {   // z: lower face of each cell, left state from lane-1
                     f2 lo[5], up[5];
@@ -593,8 +631,8 @@ template <int W, int R> struct Kernel {
                     face<2>(lo, up, false, S<f2>(0.f), k, F);
 #pragma unroll
                     for (int f = 0; f < 5; ++f) {
-                        s.fy_edge[f][h] = F[f].x;
-                        s.fy_edge[f][h + 16] = F[f].y;
+                        s.fy_edge[m & 1][f][h] = F[f].x;
+                        s.fy_edge[m & 1][f][h + 16] = F[f].y;
                     }
                 } else {
                     const int r = tid - 16;
@@ -608,50 +646,38 @@ template <int W, int R> struct Kernel {
                     face<3>(lo, up, grav, make_float2(ghs, ghs), k, F);
 #pragma unroll
                     for (int f = 0; f < 5; ++f) {
-                        s.fz_edge[f][r] = F[f].x;
-                        s.fz_edge[f][r + TY / 2] = F[f].y;
+                        s.fz_edge[m & 1][f][r] = F[f].x;
+                        s.fz_edge[m & 1][f][r + TY / 2] = F[f].y;
                     }
                 }
             }
-            __syncthreads();   // S3: published fluxes ready
 
-            if (own) {
-                // ---- (e) update plane m-1: cons - scale * (fx_hi + acc) -------
-                const int xu = m - 1;
-                if (xu >= xs && xu < xe && val0) {
-                    const bool x_out = xu == 2 && a.bc[0] == kOutflow;   // acc holds no x-flux then
-                    const int cs = (xu - xs + 2) % 3;
-                    f2 u[5];
+            if (plane_upd) {
+                // ---- (e0) this plane's divergence, minus its lower x-face flux,
+                // from what this thread holds; completed at the next plane
+                // lower x-outflow face repeats the next face's flux: plane 2
+                // gets no x-divergence (boundaries.rs:107-111 on the fluxes)
+                const bool x_out = m == 2 && a.bc[0] == kOutflow;
+                const bool y_out = gy0 == 2 && a.bc[2] == kOutflow;
+                const bool z_out = gzo == 2 && a.bc[4] == kOutflow;
 #pragma unroll
-                    for (int f = 0; f < 5; ++f) {
-                        const f2 cA = s.own_cons[cs][f][tid];
-                        const f2 t = x_out ? acc[f] : vadd(fx[f], acc[f]);
-                        u[f] = vfma(S<f2>(-k.scale), t, cA);
+                for (int f = 0; f < 5; ++f) {
+                    f2 dy;
+                    // lower outflow face repeats the next face's flux (cell 2 sees none)
+                    dy.x = y_out ? 0.f : fy[f].y - fy[f].x;
+                    dy.y = 0.f;
+                    fyy[f] = fy[f].y;
+                    f2 zh;
+                    zh.x = __shfl_down_sync(0xffffffffu, fz[f].x, 1);
+                    zh.y = __shfl_down_sync(0xffffffffu, fz[f].y, 1);
+                    f2 dz = z_out ? make_float2(0.f, 0.f) : vsub(zh, fz[f]);
+                    if (lane == 31) {
+                        s.fz_last[m & 1][f][2 * w] = fz[f].x;
+                        s.fz_last[m & 1][f][2 * w + 1] = fz[f].y;
+                        dz = make_float2(0.f, 0.f);
                     }
-                    epilogue(a, k, xu, u, val1, gy0, gzo, nyi0, nyi1, nzi, yimg0, yflp0, yimg1, yflp1, zimg, zflp,
-                             col_img, sum, smax);
-                }
-                if (plane_upd) {
-                    // lower x-outflow face repeats the next face's flux: plane 2
-                    // gets no x-divergence (boundaries.rs:107-111 on the fluxes)
-                    const bool x_out = m == 2 && a.bc[0] == kOutflow;
-                    const bool y_out = gy0 == 2 && a.bc[2] == kOutflow;
-                    const bool z_out = gzo == 2 && a.bc[4] == kOutflow;
-#pragma unroll
-                    for (int f = 0; f < 5; ++f) {
-                        const float fy_top = (w + 1 < W) ? s.fy_pub[w + 1][f][lane] : s.fy_edge[f][lane];
-                        f2 dy;
-                        // lower outflow face repeats the next face's flux (cell 2 sees none)
-                        dy.x = y_out ? 0.f : fy[f].y - fy[f].x;
-                        dy.y = fy_top - fy[f].y;
-                        f2 zh;
-                        zh.x = __shfl_down_sync(0xffffffffu, fz[f].x, 1);
-                        zh.y = __shfl_down_sync(0xffffffffu, fz[f].y, 1);
-                        if (lane == 31) zh = make_float2(s.fz_edge[f][2 * w], s.fz_edge[f][2 * w + 1]);
-                        const f2 dz = z_out ? make_float2(0.f, 0.f) : vsub(zh, fz[f]);
-                        const f2 d = vadd(dy, dz);
-                        acc[f] = x_out ? d : vsub(d, fx[f]);
-                    }
+                    const f2 d = vadd(dy, dz);
+                    acc[f] = x_out ? d : vsub(d, fx[f]);
                 }
             }
         }
@@ -667,6 +693,7 @@ template <int W, int R> struct Kernel {
         // min over cells of ds/speed = ds / max speed
         const unsigned nanf = smax != smax;
         const double wmin = nanf ? INFINITY : (double)__fdiv_rn(k.ds, smax);
+        double sum[5] = {0, 0, 0, 0, 0};
         if (block_partial(a, sum, wmin, nanf, tid, NT, s.red, &s.is_last)) {
             __threadfence();
             final_reduce<float>(a, tid, NT, s.red, kAdvance);
