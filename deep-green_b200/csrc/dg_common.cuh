@@ -19,6 +19,10 @@ __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
 
+__device__ __forceinline__ void mbar_inval(uint64_t *bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 __device__ __forceinline__ void fence_mbar_init() {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
@@ -113,14 +117,14 @@ __host__ __device__ __forceinline__ int axis_source(int g, int n, int lo, int hi
 enum ReduceMode { kSumsOnly = 0, kSetDt = 1, kAdvance = 2 };
 
 template <class T>
-__device__ void final_reduce(const GridArgs<T> &a, int tid, int nt, double *red, int mode);
+__device__ void final_reduce(const GridArgs<T> &a, int tid, int nt, double *red, int mode, int nb);
 
 // Block-level reduction of (sums, min wave time, NaN flag) into
-// a.part[blockIdx.x] in a fixed order.  Returns true, in every thread, in
-// the launch's last block to finish.
+// a.part[idx] in a fixed order.  Returns true, in every thread, in the last
+// of the nb blocks (work items) of this grid to finish.
 template <class T>
 __device__ bool block_partial(const GridArgs<T> &a, double sum[5], double wm, unsigned nanf, int tid, int nt,
-                              double *red, int *is_last) {
+                              double *red, int *is_last, int idx, int nb) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
 #pragma unroll
@@ -146,10 +150,10 @@ __device__ bool block_partial(const GridArgs<T> &a, double sum[5], double wm, un
             p.nan |= red[w * 7 + 6] != 0.0;
         }
         p.pad = 0;
-        a.part[blockIdx.x] = p;
+        a.part[idx] = p;
         __threadfence();
         const unsigned ticket = atomicAdd(&a.ctl->counter, 1u);
-        *is_last = ticket == gridDim.x - 1;
+        *is_last = ticket == (unsigned)nb - 1;
     }
     __syncthreads();
     return *is_last != 0;
@@ -159,8 +163,7 @@ __device__ bool block_partial(const GridArgs<T> &a, double sum[5], double wm, un
 // kAdvance: a step finished -> record its dt, set the next dt, step += 1;
 // kSetDt: a state was just set -> dt of the coming step; kSumsOnly: sums.
 template <class T>
-__device__ void final_reduce(const GridArgs<T> &a, int tid, int nt, double *red, int mode) {
-    const int nb = gridDim.x;
+__device__ void final_reduce(const GridArgs<T> &a, int tid, int nt, double *red, int mode, int nb) {
     double acc[5] = {0, 0, 0, 0, 0};
     double wm = INFINITY;
     unsigned nanf = 0;

@@ -328,18 +328,17 @@ template <int W, int R> struct Kernel {
         }
     }
 
-    static __device__ void run(const GridArgs<float> &a, const CUtensorMap *tmap, int chunk, unsigned char *raw) {
+    // One work item: tile (ty, tz) of grid `a`, x-planes of chunk cx.  Its
+    // partial result goes to a.part[part_idx]; the last of the grid's nparts
+    // items reduces them (next dt).  Returns false after a device-side wait
+    // timed out (status flag set).
+    static __device__ bool run_tile(const GridArgs<float> &a, const CUtensorMap *tmap, int tz, int ty, int cx, int chunk,
+                                    int part_idx, int nparts, unsigned char *raw) {
         Sm &s = *reinterpret_cast<Sm *>(raw);
         const int lane = threadIdx.x, w = threadIdx.y;
         const int tid = w * 32 + lane;
         constexpr bool own = true;
 
-        const int tiles_z = (a.nz - 4 + kTZ - 1) / kTZ;
-        const int tiles_y = (a.ny - 4 + TY - 1) / TY;
-        int b = blockIdx.x;
-        const int tz = b % tiles_z; b /= tiles_z;
-        const int ty = b % tiles_y; b /= tiles_y;
-        const int cx = b;
         const int y0 = 2 + ty * TY, z0 = 2 + tz * kTZ;
         const int xs = 2 + cx * chunk;
         const int xe = min(xs + chunk, a.nx - 2);
@@ -351,7 +350,7 @@ template <int W, int R> struct Kernel {
         const bool val0 = zval && gy0 <= a.ny - 3, val1 = zval && gy1 <= a.ny - 3;
         const bool regular = val1;
 
-        if (*(volatile unsigned *)&a.ctl->flags & kStatusTimeout) return;
+        if (*(volatile unsigned *)&a.ctl->flags & kStatusTimeout) return false;
         const unsigned step = (unsigned)a.ctl->step;
         const float dt = (float)a.ctl->dt[step & 1];
         FK k;
@@ -688,16 +687,21 @@ template <int W, int R> struct Kernel {
                     mbar_wait(&s.bar[l2 % R], (l2 / R) & 1, kWaitBudget);
                 atomicOr(&a.ctl->flags, kStatusTimeout);
             }
-            return;
+            return false;
         }
+        // every staged plane was consumed: the barriers can be re-initialised
+        // by the next work item of a persistent launch
+        if (tid == 0)
+            for (int i = 0; i < R; ++i) mbar_inval(&s.bar[i]);
         // min over cells of ds/speed = ds / max speed
         const unsigned nanf = smax != smax;
         const double wmin = nanf ? INFINITY : (double)__fdiv_rn(k.ds, smax);
         double sum[5] = {0, 0, 0, 0, 0};
-        if (block_partial(a, sum, wmin, nanf, tid, NT, s.red, &s.is_last)) {
+        if (block_partial(a, sum, wmin, nanf, tid, NT, s.red, &s.is_last, part_idx, nparts)) {
             __threadfence();
-            final_reduce<float>(a, tid, NT, s.red, kAdvance);
+            final_reduce<float>(a, tid, NT, s.red, kAdvance, nparts);
         }
+        return true;
     }
 };
 
@@ -706,7 +710,49 @@ __global__ void __launch_bounds__(32 * W, 2) fast_step_kernel(const GridArgs<flo
                                                                    const __grid_constant__ CUtensorMap tmap,
                                                                    int chunk) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    Kernel<W, R>::run(a, &tmap, chunk, smem_raw);
+    constexpr int TY = Smem<W, R>::TY;
+    const int tiles_z = (a.nz - 4 + kTZ - 1) / kTZ;
+    const int tiles_y = (a.ny - 4 + TY - 1) / TY;
+    int b = blockIdx.x;
+    const int tz = b % tiles_z;
+    b /= tiles_z;
+    const int ty = b % tiles_y;
+    Kernel<W, R>::run_tile(a, &tmap, tz, ty, b / tiles_y, chunk, blockIdx.x, gridDim.x, smem_raw);
+}
+
+// Batched step: one persistent launch advances many independent grids by
+// one step each.  Work items (grid, tile, x-chunk) are taken from an atomic
+// queue; each grid keeps its own control block, so its dt is its own CFL
+// dt.  Grid arguments are copied to shared memory per item; the grid's TMA
+// descriptor is read from global memory (written by the host before launch).
+struct BatchItem {
+    int g, local, tz, ty, cx;
+};
+
+template <int W, int R>
+__global__ void __launch_bounds__(32 * W, 2) batch_step_kernel(const GridArgs<float> *__restrict__ args,
+                                                              const CUtensorMap *__restrict__ maps,
+                                                              const BatchItem *__restrict__ items, int nitems,
+                                                              unsigned *queue, int chunk) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ int s_item;
+    __shared__ __align__(16) GridArgs<float> s_args;
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    for (;;) {
+        if (tid == 0) s_item = (int)atomicAdd(queue, 1u);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= nitems) return;
+        const BatchItem bi = items[it];
+        constexpr int kWords = (int)(sizeof(GridArgs<float>) / 4);
+        for (int i = tid; i < kWords; i += 32 * W)
+            reinterpret_cast<int *>(&s_args)[i] = reinterpret_cast<const int *>(&args[bi.g])[i];
+        __syncthreads();
+        const bool ok = Kernel<W, R>::run_tile(s_args, &maps[bi.g], bi.tz, bi.ty, bi.cx, chunk, bi.local, s_args.nparts,
+                                               smem_raw);
+        __syncthreads();
+        if (!ok) return;
+    }
 }
 
 }  // namespace fastk

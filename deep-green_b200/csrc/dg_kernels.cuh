@@ -50,6 +50,7 @@ template <class T> struct GridArgs {
     int bc[6];
     int gravity;
     int limiter;               // 0 central slopes, 1 minmod
+    int nparts;                // work items of this grid in a batched launch
     Consts<T> k;
     DevCtl *ctl;
     Partial *part;

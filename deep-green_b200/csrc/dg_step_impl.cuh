@@ -442,7 +442,7 @@ struct StepKernel {
         __syncthreads();
         if (!s.is_last) return;
         __threadfence();
-        final_reduce<T>(a, tid, NT, s.red, kAdvance);
+        final_reduce<T>(a, tid, NT, s.red, kAdvance, gridDim.x);
     }
 };
 
@@ -517,7 +517,7 @@ __global__ void __launch_bounds__(256) reduce_kernel(const GridArgs<T> a, int se
     __syncthreads();
     if (!is_last) return;
     __threadfence();
-    final_reduce<T>(a, tid, 256, red, set_dt ? kSetDt : kSumsOnly);
+    final_reduce<T>(a, tid, 256, red, set_dt ? kSetDt : kSumsOnly, gridDim.x);
 }
 
 // Copy every ghost cell of buf from its interior source (boundary rules).

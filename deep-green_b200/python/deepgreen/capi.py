@@ -76,6 +76,18 @@ SIGNATURES = {
     "dg_status": [_P, ctypes.POINTER(ctypes.c_uint32)],
     "dg_last_error": [_P],
     "dg_compute_step_noalloc": [ctypes.POINTER(SimInfo), _P, _P, ctypes.POINTER(ctypes.c_double), _P],
+    "dg_batch_create": [_I, ctypes.POINTER(SimInfo), ctypes.POINTER(ctypes.c_void_p)],
+    "dg_batch_destroy": [_P],
+    "dg_batch_set_primitives": [_P, _I, _PP5],
+    "dg_batch_step": [_P, _I],
+    "dg_batch_enqueue": [_P, _I],
+    "dg_batch_get_dts": [_P, _I, _I, ctypes.POINTER(ctypes.c_double)],
+    "dg_batch_get_conserved": [_P, _I, _PP5],
+    "dg_batch_set_tiling": [_P, _I, _I],
+    "dg_batch_get_tiling": [_P, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(_I)],
+    "dg_batch_autotune": [_P, _I, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_double)],
+    "dg_batch_get_stream": [_P, ctypes.POINTER(ctypes.c_void_p)],
+    "dg_batch_last_error": [_P],
 }
 
 
@@ -91,7 +103,7 @@ def load(path: os.PathLike | None = None):
     for name, args in SIGNATURES.items():
         fn = getattr(lib, name)
         fn.argtypes = args
-        fn.restype = ctypes.c_char_p if name == "dg_last_error" else ctypes.c_int32
+        fn.restype = ctypes.c_char_p if name in ("dg_last_error", "dg_batch_last_error") else ctypes.c_int32
     _lib = lib
     return lib
 
@@ -217,3 +229,94 @@ class Context:
         f = ctypes.c_uint32()
         self._check(self.lib.dg_status(self.h, ctypes.byref(f)))
         return f.value
+
+
+class Batch:
+    """Owner of one dg_batch: independent grids stepped by one launch per
+    step.  ``specs`` is a list of dicts with keys shape, ds, bcs and
+    optionally gamma, cfl, limiter, g, gravity."""
+
+    def __init__(self, specs, device=0):
+        self.lib = load()
+        self.n = len(specs)
+        arr = (SimInfo * self.n)()
+        self.shapes = []
+        for i, sp in enumerate(specs):
+            inf = arr[i]
+            inf.nx, inf.ny, inf.nz = (int(x) for x in sp["shape"])
+            inf.nghosts = 2
+            inf.ds = float(sp["ds"])
+            inf.gamma = float(sp.get("gamma", 1.4))
+            inf.cfl = float(sp.get("cfl", 0.4))
+            inf.g = float(sp.get("g", -0.1))
+            for f, bc in enumerate(sp["bcs"]):
+                inf.bcs[f] = int(bc)
+            inf.gravity = int(bool(sp.get("gravity", False)))
+            inf.limiter = int(sp.get("limiter", LIMITER_MINMOD))
+            inf.precision = F32
+            inf.device = int(device)
+            inf.rounding = ROUNDING_DEFAULT
+            self.shapes.append(tuple(int(x) + 4 for x in sp["shape"]))
+        self.infos = arr
+        h = ctypes.c_void_p()
+        rc = self.lib.dg_batch_create(self.n, arr, ctypes.byref(h))
+        if rc != DG_OK:
+            raise DgError(rc, self.lib.dg_last_error(None).decode())
+        self.h = h
+
+    def _check(self, rc):
+        if rc != DG_OK:
+            raise DgError(rc, self.lib.dg_batch_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.dg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_primitives(self, i, prim):
+        prim = [np.ascontiguousarray(a, dtype=np.float32) for a in prim]
+        for a in prim:
+            if a.shape != self.shapes[i]:
+                raise ValueError(f"grid {i}: field shape {a.shape} != {self.shapes[i]}")
+        self._check(self.lib.dg_batch_set_primitives(self.h, int(i), _ptrs(prim)))
+
+    def step(self, nsteps=1):
+        self._check(self.lib.dg_batch_step(self.h, int(nsteps)))
+
+    def enqueue(self, nsteps):
+        self._check(self.lib.dg_batch_enqueue(self.h, int(nsteps)))
+
+    def get_dts(self, i, nsteps):
+        dts = np.zeros(max(nsteps, 1), dtype=np.float64)
+        self._check(self.lib.dg_batch_get_dts(self.h, int(i), int(nsteps),
+                                              dts.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return dts[:nsteps]
+
+    def get_conserved(self, i):
+        out = [np.empty(self.shapes[i], dtype=np.float32) for _ in range(5)]
+        self._check(self.lib.dg_batch_get_conserved(self.h, int(i), _ptrs(out)))
+        return out
+
+    def set_tiling(self, tile_rows, chunk=0):
+        self._check(self.lib.dg_batch_set_tiling(self.h, int(tile_rows), int(chunk)))
+
+    def tiling(self):
+        r, c, n = _I(), _I(), _I()
+        self._check(self.lib.dg_batch_get_tiling(self.h, ctypes.byref(r), ctypes.byref(c), ctypes.byref(n)))
+        return r.value, c.value, n.value
+
+    def autotune(self, steps=3):
+        r, c, ms = _I(), _I(), ctypes.c_double()
+        self._check(self.lib.dg_batch_autotune(self.h, int(steps), ctypes.byref(r), ctypes.byref(c), ctypes.byref(ms)))
+        return r.value, c.value, ms.value
+
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        self._check(self.lib.dg_batch_get_stream(self.h, ctypes.byref(s)))
+        return s.value or 0

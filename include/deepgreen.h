@@ -174,6 +174,35 @@ int32_t dg_set_chunk(dg_ctx *ctx, int32_t chunk);
 int32_t dg_compute_step_noalloc(const dg_sim_info *info, void *cons_in, void *cons_out, double *dt_used,
                                 void *stream);
 
+/* ---- Batches: many independent grids, one persistent launch per step ----
+ * No counterpart in the reference, which steps one grid per compute_step
+ * call (physics.rs:595-681); a batch is N such grids advanced together.
+ * Each grid keeps its own state, boundary types, constants and CFL dt.
+ * Steps are replayed from a captured CUDA graph.  Batches run the FP32 fast
+ * kernel (precision DG_F32, rounding DEFAULT); all grids on one device. */
+typedef struct dg_batch dg_batch;
+int32_t dg_batch_create(int32_t n, const dg_sim_info *infos, dg_batch **out);
+int32_t dg_batch_destroy(dg_batch *b);
+/* grid i's state from host primitives, as dg_set_primitives */
+int32_t dg_batch_set_primitives(dg_batch *b, int32_t i, const void *const prim[5]);
+/* nsteps steps of every grid; blocks until done */
+int32_t dg_batch_step(dg_batch *b, int32_t nsteps);
+/* same, returning at once (ordered on dg_batch_get_stream's stream) */
+int32_t dg_batch_enqueue(dg_batch *b, int32_t nsteps);
+/* dt of grid i over the last nsteps steps (nsteps <= 4096) */
+int32_t dg_batch_get_dts(dg_batch *b, int32_t i, int32_t nsteps, double *dts);
+/* grid i's conserved state, ghosts filled, as dg_get_conserved */
+int32_t dg_batch_get_conserved(dg_batch *b, int32_t i, void *const cons[5]);
+/* tile rows (16 or 8) and x-planes per work item (0 = automatic) */
+int32_t dg_batch_set_tiling(dg_batch *b, int32_t tile_rows, int32_t chunk);
+int32_t dg_batch_get_tiling(dg_batch *b, int32_t *tile_rows, int32_t *chunk, int32_t *items);
+/* times `steps` steps of each candidate tiling on the live batch, keeps the
+ * fastest and restores the state it started from */
+int32_t dg_batch_autotune(dg_batch *b, int32_t steps, int32_t *tile_rows, int32_t *chunk, double *ms_per_step);
+int32_t dg_batch_get_stream(dg_batch *b, void **stream);
+/* message of the last failure on b (NULL: as dg_last_error(NULL)) */
+const char *dg_batch_last_error(const dg_batch *b);
+
 /* Sticky DG_STATUS_* flags raised by the device since the state was last
  * set (dg_set_*). */
 int32_t dg_status(dg_ctx *ctx, uint32_t *flags);
