@@ -1,0 +1,660 @@
+// dg_net.cu -- the correction network: parameters, Adam, workspace and the
+// C ABI of deepgreen_net.h.  The convolutions are the tcgen05 kernels of
+// dg_conv.cuh; everything else here is small element-wise kernels.
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/deepgreen_net.h"
+#include "dg_conv.cuh"
+
+using namespace dg;
+using namespace dg::net;
+
+namespace {
+
+constexpr int kIO = DG_NET_IO_CHANNELS;
+constexpr int kH = DG_NET_HIDDEN;
+constexpr int kCin[4] = {kIO, kH, kH, kH};
+constexpr int kCout[4] = {kH, kH, kH, kIO};
+
+struct Workspace {
+    int n = 0, x = 0, y = 0, z = 0;   // input extents it was sized for
+    bool train = false;
+    __nv_bfloat16 *act[3] = {};        // A1..A3 dense
+    __nv_bfloat16 *pre[3] = {};        // Z1..Z3 dense (training)
+    float *out = nullptr;              // network output (training)
+    __nv_bfloat16 *dz[4] = {};         // gradients w.r.t. Z1..Z3 and the output, padded by 2
+    size_t act_bytes[3] = {}, dz_bytes[4] = {}, out_bytes = 0;
+};
+
+}  // namespace
+
+struct dg_net {
+    int device = 0;
+    int inputs = 0, outputs = 0;
+    cudaStream_t stream = nullptr;
+    float *w[4] = {}, *b[4] = {};
+    float *gw[4] = {}, *gb[4] = {};
+    float *mw[4] = {}, *vw[4] = {}, *mb[4] = {}, *vb[4] = {};
+    __nv_bfloat16 *wf[4] = {};         // forward packing
+    __nv_bfloat16 *wd[4] = {};         // input-gradient packing (layers 1..3)
+    unsigned *status = nullptr;
+    float *wpart = nullptr;            // weight-gradient partials, one row per block
+    double *loss_part = nullptr;
+    int nsm = 148;
+    long long adam_t = 0;
+    Workspace ws;
+    std::string err;
+};
+
+namespace {
+
+std::mutex g_net_err_mu;
+std::string g_net_err;
+
+int fail(dg_net *n, int code, const std::string &m) {
+    if (n) n->err = m;
+    else {
+        std::lock_guard<std::mutex> g(g_net_err_mu);
+        g_net_err = m;
+    }
+    return code;
+}
+
+#define NET_CUDA(net, call)                                                                  \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess) return fail(net, DG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// 4-D view (C, y*z, x, n) of a channels-last tensor; box (8, kWz, 3, 1).
+bool map_conv_input(CUtensorMap *m, const void *base, int c, int n, int x, int y, int z) {
+    auto fn = encode_fn();
+    if (!fn) return false;
+    const cuuint64_t e = 2;
+    cuuint64_t dims[4] = {(cuuint64_t)c, (cuuint64_t)y * z, (cuuint64_t)x, (cuuint64_t)n};
+    cuuint64_t strides[3] = {c * e, (cuuint64_t)y * z * c * e, (cuuint64_t)x * y * z * c * e};
+    cuuint32_t box[4] = {8, (cuuint32_t)kWz, 3, 1};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void *>(base), dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// 5-D view (C, z, y, x, n); box (8, bz, by, 1, 1).
+bool map_5d(CUtensorMap *m, const void *base, int c, int n, int x, int y, int z, int bz, int by) {
+    auto fn = encode_fn();
+    if (!fn) return false;
+    const cuuint64_t e = 2;
+    cuuint64_t dims[5] = {(cuuint64_t)c, (cuuint64_t)z, (cuuint64_t)y, (cuuint64_t)x, (cuuint64_t)n};
+    cuuint64_t strides[4] = {c * e, (cuuint64_t)z * c * e, (cuuint64_t)y * z * c * e, (cuuint64_t)x * y * z * c * e};
+    cuuint32_t box[5] = {8, (cuuint32_t)bz, (cuuint32_t)by, 1, 1};
+    cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void *>(base), dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// Element-wise kernels
+// ---------------------------------------------------------------------------
+
+// Forward packing [tap][ci/8][co][8] of W[co][ci][tap].
+__global__ void pack_fwd_kernel(const float *__restrict__ w, __nv_bfloat16 *__restrict__ out, int cin, int cout) {
+    const int total = 27 * cin * cout;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const int e = i & 7;
+        int r = i >> 3;
+        const int co = r % cout;
+        r /= cout;
+        const int cg = r % (cin / 8);
+        const int t = r / (cin / 8);
+        out[i] = __float2bfloat16_rn(w[((size_t)co * cin + cg * 8 + e) * 27 + t]);
+    }
+}
+
+// Input-gradient packing: a convolution with cin' = cout, cout' = cin and
+// W'_t[co'][ci'] = W_{26-t}[ci'][co'] (taps flipped, channels transposed),
+// packed [t][ci'/8][co'][8].
+__global__ void pack_dgrad_kernel(const float *__restrict__ w, __nv_bfloat16 *__restrict__ out, int cin, int cout) {
+    const int total = 27 * cin * cout;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const int e = i & 7;
+        int r = i >> 3;
+        const int cop = r % cin;              // output channel of the transposed conv = ci of W
+        r /= cin;
+        const int g = r % (cout / 8);         // input channel group of the transposed conv = co of W
+        const int t = r / (cout / 8);
+        const int co = g * 8 + e;
+        out[i] = __float2bfloat16_rn(w[((size_t)co * cin + cop) * 27 + (26 - t)]);
+    }
+}
+
+// Fixed-order sum of the per-block weight-gradient partials.
+__global__ void wgrad_reduce_kernel(const float *__restrict__ part, int nblocks, int cin, int cout, float *gw,
+                                    float *gb) {
+    const int nw = cout * cin * 27, row = nw + cout;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < row; i += gridDim.x * blockDim.x) {
+        float s = 0.0f;
+        for (int k = 0; k < nblocks; ++k) s += part[(size_t)k * row + i];
+        if (i < nw) gw[i] = s;
+        else gb[i - nw] = s;
+    }
+}
+
+// Loss and its gradient w.r.t. the network output: L = mean (out - t)^2 over
+// positions and the first `nout` channels.  The gradient (BF16) goes to the
+// interior of a buffer padded by 2 on each side; per-block partial sums of
+// the squared error go to part[blockIdx.x].
+__global__ void loss_kernel(const float *__restrict__ out, const float *__restrict__ tgt, int n, int x, int y, int z,
+                            int nout, float scale, __nv_bfloat16 *__restrict__ dz, double *part) {
+    __shared__ double red[32];
+    const long long total = (long long)n * x * y * z;
+    double acc = 0.0;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < total;
+         v += (long long)gridDim.x * blockDim.x) {
+        long long r = v;
+        const int iz = r % z; r /= z;
+        const int iy = r % y; r /= y;
+        const int ix = r % x;
+        const int b = (int)(r / x);
+        float g[kIO];
+#pragma unroll
+        for (int c = 0; c < kIO; ++c) {
+            const float d = c < nout ? out[v * kIO + c] - tgt[v * kIO + c] : 0.0f;
+            acc += (double)d * d;
+            g[c] = scale * d;
+        }
+        const long long o = ((((long long)b * (x + 4) + ix + 2) * (y + 4) + iy + 2) * (z + 4) + iz + 2) * kIO;
+        store_bf16(dz + o, g, kIO);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += red[i];
+        part[blockIdx.x] = s;
+    }
+}
+
+__global__ void adam_kernel(float *__restrict__ p, const float *__restrict__ g, float *__restrict__ m,
+                            float *__restrict__ v, int count, float lr, float b1, float b2, float eps, float c1,
+                            float c2) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.0f - b1) * gi;
+        const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    }
+}
+
+// Unpadded copy of the interior of a padded BF16 tensor (test access).
+__global__ void unpad_kernel(const __nv_bfloat16 *__restrict__ src, __nv_bfloat16 *__restrict__ dst, int n, int x,
+                             int y, int z, int c) {
+    const long long total = (long long)n * x * y * z * c;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        long long r = i;
+        const int ic = r % c; r /= c;
+        const int iz = r % z; r /= z;
+        const int iy = r % y; r /= y;
+        const int ix = r % x;
+        const int b = (int)(r / x);
+        dst[i] = src[((((long long)b * (x + 4) + ix + 2) * (y + 4) + iy + 2) * (z + 4) + iz + 2) * c + ic];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Launch helpers
+// ---------------------------------------------------------------------------
+template <int CIN, int COUT, int EPI>
+cudaError_t launch_conv(dg_net *net, const void *in, int nb, int xi, int yi, int zi, const __nv_bfloat16 *w,
+                        ConvArgs a) {
+    using L = ConvSmem<CIN, COUT>;
+    auto kern = conv_fwd_kernel<CIN, COUT, EPI>;
+    static std::once_flag once;
+    static cudaError_t attr_err = cudaSuccess;
+    static int occ = 1;
+    std::call_once(once, [&] {
+        attr_err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::BYTES);
+        if (attr_err == cudaSuccess)
+            attr_err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kConvThreads, L::BYTES);
+    });
+    if (attr_err != cudaSuccess) return attr_err;
+    CUtensorMap m;
+    if (!map_conv_input(&m, in, CIN, nb, xi, yi, zi)) return cudaErrorInvalidValue;
+    a.nb = nb;
+    a.xi = xi; a.yi = yi; a.zi = zi;
+    a.xo = xi - 2; a.yo = yi - 2; a.zo = zi - 2;
+    a.tpp = (a.yo * zi + kM - 1) / kM;
+    a.ntiles = nb * a.xo * a.tpp;
+    a.status = net->status;
+    const int grid = std::max(1, std::min(a.ntiles, std::max(1, occ) * net->nsm));
+    kern<<<grid, kConvThreads, L::BYTES, net->stream>>>(m, w, a);
+    return cudaGetLastError();
+}
+
+template <int CIN, int COUT>
+cudaError_t launch_wgrad(dg_net *net, const void *x_in, const void *g_pad, int nb, int xo, int yo, int zo, float *gw,
+                         float *gb) {
+    using L = WgradSmem<CIN, COUT>;
+    auto kern = conv_wgrad_kernel<CIN, COUT>;
+    static std::once_flag once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(once, [&] {
+        attr_err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::BYTES);
+    });
+    if (attr_err != cudaSuccess) return attr_err;
+    CUtensorMap mx, mg;
+    if (!map_5d(&mx, x_in, CIN, nb, xo + 2, yo + 2, zo + 2, kWz, 3)) return cudaErrorInvalidValue;
+    if (!map_5d(&mg, g_pad, COUT, nb, xo + 4, yo + 4, zo + 4, kM, 1)) return cudaErrorInvalidValue;
+    WgradArgs a;
+    a.nb = nb; a.xo = xo; a.yo = yo; a.zo = zo;
+    a.nseg = (zo + kM - 1) / kM;
+    a.ntiles = nb * xo * yo * a.nseg;
+    a.part = net->wpart;
+    a.status = net->status;
+    const int grid = std::max(1, std::min(a.ntiles, net->nsm));
+    kern<<<grid, kConvThreads, L::BYTES, net->stream>>>(mx, mg, a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    wgrad_reduce_kernel<<<64, 256, 0, net->stream>>>(net->wpart, grid, CIN, COUT, gw, gb);
+    return cudaGetLastError();
+}
+
+int repack(dg_net *net) {
+    for (int l = 0; l < 4; ++l) {
+        pack_fwd_kernel<<<64, 256, 0, net->stream>>>(net->w[l], net->wf[l], kCin[l], kCout[l]);
+        if (l > 0) pack_dgrad_kernel<<<64, 256, 0, net->stream>>>(net->w[l], net->wd[l], kCin[l], kCout[l]);
+    }
+    NET_CUDA(net, cudaGetLastError());
+    return DG_OK;
+}
+
+void free_ws(Workspace &ws) {
+    for (int i = 0; i < 3; ++i) {
+        cudaFree(ws.act[i]);
+        cudaFree(ws.pre[i]);
+        ws.act[i] = ws.pre[i] = nullptr;
+    }
+    for (int i = 0; i < 4; ++i) {
+        cudaFree(ws.dz[i]);
+        ws.dz[i] = nullptr;
+    }
+    cudaFree(ws.out);
+    ws.out = nullptr;
+    ws.n = 0;
+}
+
+int ensure_ws(dg_net *net, int n, int x, int y, int z, bool train) {
+    Workspace &ws = net->ws;
+    if (ws.n == n && ws.x == x && ws.y == y && ws.z == z && (ws.train || !train)) return DG_OK;
+    NET_CUDA(net, cudaStreamSynchronize(net->stream));
+    free_ws(ws);
+    for (int l = 0; l < 3; ++l) {
+        const size_t e = (size_t)n * (x - 2 * (l + 1)) * (y - 2 * (l + 1)) * (z - 2 * (l + 1));
+        ws.act_bytes[l] = e * kH * 2;
+        NET_CUDA(net, cudaMalloc(&ws.act[l], ws.act_bytes[l]));
+        if (train) NET_CUDA(net, cudaMalloc(&ws.pre[l], ws.act_bytes[l]));
+    }
+    if (train) {
+        const size_t eo = (size_t)n * (x - 8) * (y - 8) * (z - 8);
+        ws.out_bytes = eo * kIO * 4;
+        NET_CUDA(net, cudaMalloc(&ws.out, ws.out_bytes));
+        for (int l = 0; l < 4; ++l) {
+            // gradient w.r.t. the output of layer l (extent x - 2(l+1)), padded by 2
+            const int k = 2 * (l + 1);
+            const size_t e = (size_t)n * (x - k + 4) * (y - k + 4) * (z - k + 4);
+            ws.dz_bytes[l] = e * kCout[l] * 2;
+            NET_CUDA(net, cudaMalloc(&ws.dz[l], ws.dz_bytes[l]));
+            NET_CUDA(net, cudaMemsetAsync(ws.dz[l], 0, ws.dz_bytes[l], net->stream));
+        }
+    }
+    ws.n = n; ws.x = x; ws.y = y; ws.z = z;
+    ws.train = train;
+    return DG_OK;
+}
+
+int check_status(dg_net *net) {
+    unsigned st = 0;
+    NET_CUDA(net, cudaMemcpyAsync(&st, net->status, sizeof(st), cudaMemcpyDeviceToHost, net->stream));
+    NET_CUDA(net, cudaStreamSynchronize(net->stream));
+    if (st & kNetTimeout) return fail(net, DG_ERR_TIMEOUT, "a device-side wait timed out; results invalid");
+    return DG_OK;
+}
+
+uint64_t splitmix(uint64_t &s) {
+    uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+int check_extents(dg_net *net, int n, int x, int y, int z) {
+    if (n < 1 || x < 9 || y < 9 || z < 9)
+        return fail(net, DG_ERR_INVALID, "input extents must be at least 9 per axis and n >= 1");
+    if ((long long)(y - 2) * z >= (1LL << 31) / 2 || (long long)n * x * y * z >= (1LL << 40))
+        return fail(net, DG_ERR_INVALID, "input too large");
+    return DG_OK;
+}
+
+// Forward pass; stores pre-activations when the workspace is a training one.
+int forward(dg_net *net, const void *feat, int n, int x, int y, int z, float *out, bool train) {
+    Workspace &ws = net->ws;
+    cudaError_t e;
+    const void *in = feat;
+    int xi = x, yi = y, zi = z;
+    for (int l = 0; l < 3; ++l) {
+        ConvArgs a{};
+        a.ox = xi - 2; a.oy = yi - 2; a.oz = zi - 2; a.off = 0;
+        a.bias = net->b[l];
+        a.out_a = ws.act[l];
+        a.out_z = train ? ws.pre[l] : nullptr;
+        if (l == 0) e = launch_conv<kIO, kH, kEpiGelu>(net, in, n, xi, yi, zi, net->wf[l], a);
+        else e = launch_conv<kH, kH, kEpiGelu>(net, in, n, xi, yi, zi, net->wf[l], a);
+        if (e != cudaSuccess) return fail(net, DG_ERR_CUDA, std::string("conv launch: ") + cudaGetErrorString(e));
+        in = ws.act[l];
+        xi -= 2; yi -= 2; zi -= 2;
+    }
+    ConvArgs a{};
+    a.ox = xi - 2; a.oy = yi - 2; a.oz = zi - 2; a.off = 0;
+    a.bias = net->b[3];
+    a.out_f = out;
+    e = launch_conv<kH, kIO, kEpiLinear>(net, in, n, xi, yi, zi, net->wf[3], a);
+    if (e != cudaSuccess) return fail(net, DG_ERR_CUDA, std::string("conv launch: ") + cudaGetErrorString(e));
+    return DG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t dg_net_create(const dg_net_info *info, dg_net **out) {
+    if (!info || !out) return fail(nullptr, DG_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (info->inputs < 1 || info->inputs > kIO || info->outputs < 1 || info->outputs > kIO)
+        return fail(nullptr, DG_ERR_INVALID, "inputs and outputs must be in 1..16");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(nullptr, DG_ERR_NO_DEVICE, "no CUDA device");
+    if (info->device < 0 || info->device >= ndev) return fail(nullptr, DG_ERR_INVALID, "bad device ordinal");
+    if (cudaSetDevice(info->device) != cudaSuccess) return fail(nullptr, DG_ERR_NO_DEVICE, "cannot select device");
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, info->device) != cudaSuccess || prop.major != 10)
+        return fail(nullptr, DG_ERR_NO_DEVICE, "the network kernels need an sm_100 GPU");
+    dg_net *net = new dg_net();
+    net->device = info->device;
+    net->inputs = info->inputs;
+    net->outputs = info->outputs;
+    net->nsm = prop.multiProcessorCount;
+    auto bail = [&](int code) {
+        dg_net_destroy(net);
+        return code;
+    };
+    auto cu = [&](cudaError_t e, const char *what) {
+        if (e != cudaSuccess) {
+            fail(nullptr, DG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+            return false;
+        }
+        return true;
+    };
+    if (!cu(cudaStreamCreateWithFlags(&net->stream, cudaStreamNonBlocking), "stream")) return bail(DG_ERR_CUDA);
+    size_t maxrow = 0;
+    for (int l = 0; l < 4; ++l) {
+        const size_t nw = (size_t)27 * kCin[l] * kCout[l], nb = kCout[l];
+        maxrow = std::max(maxrow, nw + nb);
+        float **fl[] = {&net->w[l], &net->gw[l], &net->mw[l], &net->vw[l]};
+        for (auto p : fl)
+            if (!cu(cudaMalloc(p, nw * 4), "cudaMalloc") || !cu(cudaMemset(*p, 0, nw * 4), "memset"))
+                return bail(DG_ERR_CUDA);
+        float **fb[] = {&net->b[l], &net->gb[l], &net->mb[l], &net->vb[l]};
+        for (auto p : fb)
+            if (!cu(cudaMalloc(p, nb * 4), "cudaMalloc") || !cu(cudaMemset(*p, 0, nb * 4), "memset"))
+                return bail(DG_ERR_CUDA);
+        if (!cu(cudaMalloc(&net->wf[l], nw * 2), "cudaMalloc")) return bail(DG_ERR_CUDA);
+        if (l > 0 && !cu(cudaMalloc(&net->wd[l], nw * 2), "cudaMalloc")) return bail(DG_ERR_CUDA);
+    }
+    if (!cu(cudaMalloc(&net->wpart, maxrow * net->nsm * 4), "cudaMalloc")) return bail(DG_ERR_CUDA);
+    if (!cu(cudaMalloc(&net->loss_part, 4096 * sizeof(double)), "cudaMalloc")) return bail(DG_ERR_CUDA);
+    if (!cu(cudaMalloc(&net->status, sizeof(unsigned)), "cudaMalloc") ||
+        !cu(cudaMemset(net->status, 0, sizeof(unsigned)), "memset"))
+        return bail(DG_ERR_CUDA);
+    // Seeded initialisation: uniform with the variance of He initialisation
+    // (GELU layers), the last layer scaled by out_scale; biases zero.
+    uint64_t s = info->seed;
+    for (int l = 0; l < 4; ++l) {
+        const int ci_real = l == 0 ? info->inputs : kH, co_real = l == 3 ? info->outputs : kH;
+        std::vector<float> w((size_t)27 * kCin[l] * kCout[l], 0.0f);
+        const double bound = std::sqrt(6.0 / (27.0 * ci_real)) * (l == 3 ? info->out_scale : 1.0);
+        for (int co = 0; co < co_real; ++co)
+            for (int ci = 0; ci < ci_real; ++ci)
+                for (int t = 0; t < 27; ++t) {
+                    const double u = (double)(splitmix(s) >> 11) * (1.0 / 9007199254740992.0);
+                    w[((size_t)co * kCin[l] + ci) * 27 + t] = (float)((2.0 * u - 1.0) * bound);
+                }
+        if (!cu(cudaMemcpy(net->w[l], w.data(), w.size() * 4, cudaMemcpyHostToDevice), "upload"))
+            return bail(DG_ERR_CUDA);
+    }
+    if (repack(net) != DG_OK || !cu(cudaStreamSynchronize(net->stream), "init")) return bail(DG_ERR_CUDA);
+    *out = net;
+    return DG_OK;
+}
+
+int32_t dg_net_destroy(dg_net *net) {
+    if (!net) return DG_OK;
+    cudaSetDevice(net->device);
+    if (net->stream) cudaStreamSynchronize(net->stream);
+    free_ws(net->ws);
+    for (int l = 0; l < 4; ++l) {
+        float *ps[] = {net->w[l], net->b[l], net->gw[l], net->gb[l], net->mw[l], net->vw[l], net->mb[l], net->vb[l]};
+        for (auto p : ps) cudaFree(p);
+        cudaFree(net->wf[l]);
+        cudaFree(net->wd[l]);
+    }
+    cudaFree(net->wpart);
+    cudaFree(net->loss_part);
+    cudaFree(net->status);
+    if (net->stream) cudaStreamDestroy(net->stream);
+    delete net;
+    return DG_OK;
+}
+
+static int layer_dims(dg_net *net, int layer, int *ci_real, int *co_real) {
+    if (layer < 0 || layer > 3) return fail(net, DG_ERR_INVALID, "layer must be 0..3");
+    *ci_real = layer == 0 ? net->inputs : kH;
+    *co_real = layer == 3 ? net->outputs : kH;
+    return DG_OK;
+}
+
+int32_t dg_net_set_layer(dg_net *net, int32_t layer, const float *w, const float *b) {
+    if (!net || !w || !b) return fail(net, DG_ERR_INVALID, "null argument");
+    int cr, orl;
+    if (int r = layer_dims(net, layer, &cr, &orl)) return r;
+    NET_CUDA(net, cudaSetDevice(net->device));
+    std::vector<float> wp((size_t)27 * kCin[layer] * kCout[layer], 0.0f), bp(kCout[layer], 0.0f);
+    for (int co = 0; co < orl; ++co) {
+        bp[co] = b[co];
+        for (int ci = 0; ci < cr; ++ci)
+            for (int t = 0; t < 27; ++t) wp[((size_t)co * kCin[layer] + ci) * 27 + t] = w[((size_t)co * cr + ci) * 27 + t];
+    }
+    NET_CUDA(net, cudaStreamSynchronize(net->stream));
+    NET_CUDA(net, cudaMemcpy(net->w[layer], wp.data(), wp.size() * 4, cudaMemcpyHostToDevice));
+    NET_CUDA(net, cudaMemcpy(net->b[layer], bp.data(), bp.size() * 4, cudaMemcpyHostToDevice));
+    if (int r = repack(net)) return r;
+    NET_CUDA(net, cudaStreamSynchronize(net->stream));
+    return DG_OK;
+}
+
+static int get_pair(dg_net *net, int layer, const float *dw, const float *db, float *w, float *b) {
+    int cr, orl;
+    if (int r = layer_dims(net, layer, &cr, &orl)) return r;
+    NET_CUDA(net, cudaSetDevice(net->device));
+    NET_CUDA(net, cudaStreamSynchronize(net->stream));
+    std::vector<float> wp((size_t)27 * kCin[layer] * kCout[layer]), bp(kCout[layer]);
+    NET_CUDA(net, cudaMemcpy(wp.data(), dw, wp.size() * 4, cudaMemcpyDeviceToHost));
+    NET_CUDA(net, cudaMemcpy(bp.data(), db, bp.size() * 4, cudaMemcpyDeviceToHost));
+    for (int co = 0; co < orl; ++co) {
+        if (b) b[co] = bp[co];
+        if (w)
+            for (int ci = 0; ci < cr; ++ci)
+                for (int t = 0; t < 27; ++t) w[((size_t)co * cr + ci) * 27 + t] = wp[((size_t)co * kCin[layer] + ci) * 27 + t];
+    }
+    return DG_OK;
+}
+
+int32_t dg_net_get_layer(dg_net *net, int32_t layer, float *w, float *b) {
+    if (!net) return fail(net, DG_ERR_INVALID, "null argument");
+    if (layer < 0 || layer > 3) return fail(net, DG_ERR_INVALID, "layer must be 0..3");
+    return get_pair(net, layer, net->w[layer], net->b[layer], w, b);
+}
+
+int32_t dg_net_get_grad(dg_net *net, int32_t layer, float *gw, float *gb) {
+    if (!net) return fail(net, DG_ERR_INVALID, "null argument");
+    if (layer < 0 || layer > 3) return fail(net, DG_ERR_INVALID, "layer must be 0..3");
+    return get_pair(net, layer, net->gw[layer], net->gb[layer], gw, gb);
+}
+
+int32_t dg_net_forward(dg_net *net, const void *feat, int32_t n, int32_t x, int32_t y, int32_t z, float *out) {
+    if (!net || !feat || !out) return fail(net, DG_ERR_INVALID, "null argument");
+    if (int r = check_extents(net, n, x, y, z)) return r;
+    if ((reinterpret_cast<uintptr_t>(feat) | reinterpret_cast<uintptr_t>(out)) & 15)
+        return fail(net, DG_ERR_INVALID, "device pointers must be 16-byte aligned");
+    NET_CUDA(net, cudaSetDevice(net->device));
+    if (int r = ensure_ws(net, n, x, y, z, false)) return r;
+    return forward(net, feat, n, x, y, z, out, false);
+}
+
+int32_t dg_net_forward_backward(dg_net *net, const void *feat, const float *target, int32_t n, int32_t x, int32_t y,
+                                int32_t z, double *loss) {
+    if (!net || !feat || !target) return fail(net, DG_ERR_INVALID, "null argument");
+    if (int r = check_extents(net, n, x, y, z)) return r;
+    if ((reinterpret_cast<uintptr_t>(feat) | reinterpret_cast<uintptr_t>(target)) & 15)
+        return fail(net, DG_ERR_INVALID, "device pointers must be 16-byte aligned");
+    NET_CUDA(net, cudaSetDevice(net->device));
+    if (int r = ensure_ws(net, n, x, y, z, true)) return r;
+    Workspace &ws = net->ws;
+    if (int r = forward(net, feat, n, x, y, z, ws.out, true)) return r;
+    const int xo = x - 8, yo = y - 8, zo = z - 8;
+    const long long nvox = (long long)n * xo * yo * zo;
+    const float scale = (float)(2.0 / ((double)nvox * net->outputs));
+    const int lblocks = (int)std::min<long long>(4096, (nvox + 255) / 256);
+    loss_kernel<<<lblocks, 256, 0, net->stream>>>(ws.out, target, n, xo, yo, zo, net->outputs, scale, ws.dz[3],
+                                                  net->loss_part);
+    NET_CUDA(net, cudaGetLastError());
+    // backward, layer 3 down to layer 0
+    cudaError_t e;
+    for (int l = 3; l >= 0; --l) {
+        const int k = 2 * (l + 1);
+        const int ex = x - k, ey = y - k, ez = z - k;        // extents of layer l's output
+        const void *xin = l == 0 ? feat : ws.act[l - 1];
+        if (l == 3) e = launch_wgrad<kH, kIO>(net, xin, ws.dz[l], n, ex, ey, ez, net->gw[l], net->gb[l]);
+        else if (l == 0) e = launch_wgrad<kIO, kH>(net, xin, ws.dz[l], n, ex, ey, ez, net->gw[l], net->gb[l]);
+        else e = launch_wgrad<kH, kH>(net, xin, ws.dz[l], n, ex, ey, ez, net->gw[l], net->gb[l]);
+        if (e != cudaSuccess) return fail(net, DG_ERR_CUDA, std::string("wgrad launch: ") + cudaGetErrorString(e));
+        if (l == 0) break;
+        // gradient w.r.t. the pre-activation of layer l-1 (extent ex+2), into its padded buffer
+        ConvArgs a{};
+        a.ox = ex + 2 + 4; a.oy = ey + 2 + 4; a.oz = ez + 2 + 4; a.off = 2;
+        a.out_a = ws.dz[l - 1];
+        a.zsrc = ws.pre[l - 1];
+        if (l == 3) e = launch_conv<kIO, kH, kEpiDGelu>(net, ws.dz[l], n, ex + 4, ey + 4, ez + 4, net->wd[l], a);
+        else e = launch_conv<kH, kH, kEpiDGelu>(net, ws.dz[l], n, ex + 4, ey + 4, ez + 4, net->wd[l], a);
+        if (e != cudaSuccess) return fail(net, DG_ERR_CUDA, std::string("dgrad launch: ") + cudaGetErrorString(e));
+    }
+    if (int r = check_status(net)) return r;
+    if (loss) {
+        std::vector<double> part(lblocks);
+        NET_CUDA(net, cudaMemcpy(part.data(), net->loss_part, lblocks * sizeof(double), cudaMemcpyDeviceToHost));
+        double s = 0.0;
+        for (double v : part) s += v;
+        *loss = s / ((double)nvox * net->outputs);
+    }
+    return DG_OK;
+}
+
+int32_t dg_net_adam_step(dg_net *net, float lr, float beta1, float beta2, float eps) {
+    if (!net) return fail(net, DG_ERR_INVALID, "null argument");
+    NET_CUDA(net, cudaSetDevice(net->device));
+    net->adam_t += 1;
+    const float c1 = (float)(1.0 - std::pow((double)beta1, (double)net->adam_t));
+    const float c2 = (float)(1.0 - std::pow((double)beta2, (double)net->adam_t));
+    for (int l = 0; l < 4; ++l) {
+        const int nw = 27 * kCin[l] * kCout[l];
+        adam_kernel<<<64, 256, 0, net->stream>>>(net->w[l], net->gw[l], net->mw[l], net->vw[l], nw, lr, beta1, beta2,
+                                                 eps, c1, c2);
+        adam_kernel<<<1, 64, 0, net->stream>>>(net->b[l], net->gb[l], net->mb[l], net->vb[l], kCout[l], lr, beta1,
+                                               beta2, eps, c1, c2);
+    }
+    NET_CUDA(net, cudaGetLastError());
+    return repack(net);
+}
+
+int32_t dg_net_get_tensor(dg_net *net, int32_t layer, int32_t which, void *host, uint64_t bytes) {
+    if (!net || !host) return fail(net, DG_ERR_INVALID, "null argument");
+    Workspace &ws = net->ws;
+    if (!ws.train || ws.n == 0) return fail(net, DG_ERR_NO_STATE, "no forward_backward has run");
+    if (layer < 0 || layer > 3 || which < 0 || which > 3) return fail(net, DG_ERR_INVALID, "bad layer or tensor");
+    NET_CUDA(net, cudaSetDevice(net->device));
+    NET_CUDA(net, cudaStreamSynchronize(net->stream));
+    const int k = 2 * (layer + 1);
+    const int ex = ws.x - k, ey = ws.y - k, ez = ws.z - k;
+    const size_t count = (size_t)ws.n * ex * ey * ez * kCout[layer];
+    if (which == 0 || which == 1) {
+        if (layer == 3) return fail(net, DG_ERR_INVALID, "layer 3 has no activation; use which = 2");
+        if (bytes < count * 2) return fail(net, DG_ERR_INVALID, "host buffer too small");
+        NET_CUDA(net, cudaMemcpy(host, which == 0 ? ws.act[layer] : ws.pre[layer], count * 2, cudaMemcpyDeviceToHost));
+    } else if (which == 2) {
+        if (layer != 3) return fail(net, DG_ERR_INVALID, "the output belongs to layer 3");
+        if (bytes < count * 4) return fail(net, DG_ERR_INVALID, "host buffer too small");
+        NET_CUDA(net, cudaMemcpy(host, ws.out, count * 4, cudaMemcpyDeviceToHost));
+    } else {
+        if (bytes < count * 2) return fail(net, DG_ERR_INVALID, "host buffer too small");
+        __nv_bfloat16 *tmp = nullptr;
+        NET_CUDA(net, cudaMalloc(&tmp, count * 2));
+        unpad_kernel<<<256, 256, 0, net->stream>>>(ws.dz[layer], tmp, ws.n, ex, ey, ez, kCout[layer]);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(host, tmp, count * 2, cudaMemcpyDeviceToHost, net->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(net->stream);
+        cudaFree(tmp);
+        if (e != cudaSuccess) return fail(net, DG_ERR_CUDA, std::string("get_tensor: ") + cudaGetErrorString(e));
+    }
+    return DG_OK;
+}
+
+int32_t dg_net_synchronize(dg_net *net) {
+    if (!net) return fail(net, DG_ERR_INVALID, "null argument");
+    NET_CUDA(net, cudaStreamSynchronize(net->stream));
+    return check_status(net);
+}
+
+void *dg_net_get_stream(dg_net *net) { return net ? net->stream : nullptr; }
+
+const char *dg_net_last_error(const dg_net *net) {
+    if (net) return net->err.c_str();
+    std::lock_guard<std::mutex> g(g_net_err_mu);
+    return g_net_err.c_str();
+}
+
+}  // extern "C"

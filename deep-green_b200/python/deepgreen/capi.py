@@ -14,6 +14,7 @@ import numpy as np
 PKG_ROOT = Path(__file__).resolve().parents[2]          # deep-green_b200/
 LIB_PATH = PKG_ROOT / "lib" / "libdeepgreen.so"
 HEADER_PATH = PKG_ROOT.parent / "include" / "deepgreen.h"
+NET_HEADER_PATH = PKG_ROOT.parent / "include" / "deepgreen_net.h"
 
 DG_OK = 0
 DG_ERR_INVALID = -1
@@ -88,6 +89,26 @@ SIGNATURES = {
     "dg_batch_autotune": [_P, _I, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_double)],
     "dg_batch_get_stream": [_P, ctypes.POINTER(ctypes.c_void_p)],
     "dg_batch_last_error": [_P],
+    # learned correction (deepgreen_net.h)
+    "dg_net_create": [_P, ctypes.POINTER(ctypes.c_void_p)],
+    "dg_net_destroy": [_P],
+    "dg_net_set_layer": [_P, _I, _P, _P],
+    "dg_net_get_layer": [_P, _I, _P, _P],
+    "dg_net_get_grad": [_P, _I, _P, _P],
+    "dg_net_forward": [_P, _P, _I, _I, _I, _I, _P],
+    "dg_net_forward_backward": [_P, _P, _P, _I, _I, _I, _I, ctypes.POINTER(ctypes.c_double)],
+    "dg_net_adam_step": [_P, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float],
+    "dg_net_get_tensor": [_P, _I, _I, _P, ctypes.c_uint64],
+    "dg_net_synchronize": [_P],
+    "dg_net_get_stream": [_P],
+    "dg_net_last_error": [_P],
+}
+
+_RESTYPES = {
+    "dg_last_error": ctypes.c_char_p,
+    "dg_batch_last_error": ctypes.c_char_p,
+    "dg_net_last_error": ctypes.c_char_p,
+    "dg_net_get_stream": ctypes.c_void_p,
 }
 
 
@@ -103,7 +124,7 @@ def load(path: os.PathLike | None = None):
     for name, args in SIGNATURES.items():
         fn = getattr(lib, name)
         fn.argtypes = args
-        fn.restype = ctypes.c_char_p if name in ("dg_last_error", "dg_batch_last_error") else ctypes.c_int32
+        fn.restype = _RESTYPES.get(name, ctypes.c_int32)
     _lib = lib
     return lib
 

@@ -1,5 +1,6 @@
 """CPU checks of the C ABI boundary: the library is built, loads, and
-exports every entry point include/deepgreen.h declares (no compute call)."""
+exports every entry point include/deepgreen.h and include/deepgreen_net.h
+declare (no compute call)."""
 import re
 import subprocess
 
@@ -9,8 +10,8 @@ from deepgreen import capi
 
 
 def header_symbols():
-    text = capi.HEADER_PATH.read_text()
-    return sorted(set(re.findall(r"^\s*(?:int32_t|const char \*)\s*(dg_\w+)\s*\(", text, re.M)))
+    text = capi.HEADER_PATH.read_text() + capi.NET_HEADER_PATH.read_text()
+    return sorted(set(re.findall(r"^\s*(?:int32_t|const char \*|void \*)\s*(dg_\w+)\s*\(", text, re.M)))
 
 
 def test_header_declares_expected_entry_points():
