@@ -5,6 +5,7 @@
 // the per-block partials buffer, plus one TMA descriptor per state buffer.
 #include <cudaTypedefs.h>
 
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -13,32 +14,10 @@
 #include <string>
 
 #include "../../include/deepgreen.h"
-#include "dg_kernels.cuh"
+#include "dg_ctx.h"
 
 using namespace dg;
 
-struct dg_ctx {
-    dg_sim_info info;
-    int elem;                  // 4 or 8
-    int nx, ny, nz;            // ghosted extents
-    int pitch;                 // z-row pitch in elements
-    long long fstride;         // elements per field
-    size_t state_bytes;
-    void *buf[2];
-    int cur;                   // buffer holding the current state
-    bool has_state;
-    unsigned long long steps;  // steps since the state was set
-    DevCtl *ctl;
-    Partial *part;
-    int part_cap;
-    void *prim_scratch;        // lazily allocated: dense primitives for dg_get_primitives
-    CUtensorMap tmap[2];
-    cudaStream_t stream;
-    int chunk;                 // 0 = automatic
-    bool exact;                // reference-rounding policy
-    int kind;                  // KernelKind of the step kernel
-    std::string err;
-};
 
 namespace {
 
@@ -56,51 +35,6 @@ PFN_cuTensorMapEncodeTiled_v12000 get_encode_fn() {
             fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
     });
     return fn;
-}
-
-int fail(dg_ctx *c, int code, const std::string &msg) {
-    if (c) c->err = msg;
-    return code;
-}
-
-int cuda_fail(dg_ctx *c, cudaError_t e, const char *where) {
-    return fail(c, DG_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
-}
-
-#define DG_CUDA(c, expr)                                         \
-    do {                                                         \
-        cudaError_t e_ = (expr);                                 \
-        if (e_ != cudaSuccess) return cuda_fail((c), e_, #expr); \
-    } while (0)
-
-template <class T> GridArgs<T> grid_args(const dg_ctx *c, const void *src, void *dst) {
-    GridArgs<T> a;
-    a.src = static_cast<const T *>(src);
-    a.dst = static_cast<T *>(dst);
-    a.nx = c->nx;
-    a.ny = c->ny;
-    a.nz = c->nz;
-    a.pitch = c->pitch;
-    a.fstride = c->fstride;
-    for (int i = 0; i < 6; ++i) a.bc[i] = c->info.bcs[i];
-    a.gravity = c->info.gravity;
-    a.limiter = c->info.limiter;
-    const T ds = (T)c->info.ds;
-    a.k.ds = ds;
-    a.k.vol = ds * ds * ds;
-    a.k.inv_vol = T(1) / a.k.vol;
-    a.k.gamma = (T)c->info.gamma;
-    a.k.gm1 = a.k.gamma - T(1);
-    a.k.inv_gm1 = T(1) / a.k.gm1;
-    a.k.half_ds = ds / T(2);
-    a.k.two_ds = T(2) * ds;
-    a.k.inv_ds = T(1) / ds;
-    a.k.inv_2ds = T(1) / (T(2) * ds);
-    a.k.cfl = (T)c->info.cfl;
-    a.k.g = (T)c->info.g;
-    a.ctl = c->ctl;
-    a.part = c->part;
-    return a;
 }
 
 int auto_chunk(const dg_ctx *c) {
@@ -224,6 +158,23 @@ int read_dts(dg_ctx *c, int nsteps, double *dts) {
     return DG_OK;
 }
 
+}  // namespace
+
+// Entry points for the other C-ABI sources of the library (dg_ctx.h).
+int dg::ctx_enqueue(dg_ctx *c, int nsteps) { return enqueue(c, nsteps); }
+
+int dg::ctx_begin_state(dg_ctx *c) {
+    int r = use_device(c);
+    return r != DG_OK ? r : reset_ctl(c);
+}
+
+int dg::ctx_finish_state(dg_ctx *c) { return finish_state(c); }
+
+int dg::ctx_check_flags(dg_ctx *c) { return check_flags(c); }
+
+namespace {
+// dt of the coming step := dt (the step counter lives on the device)
+__global__ void set_next_dt_kernel(DevCtl *ctl, double dt) { ctl->dt[ctl->step & 1] = dt; }
 }  // namespace
 
 void dg::set_global_error(const std::string &msg) {
@@ -403,6 +354,29 @@ int32_t dg_compute_step(dg_ctx *c, int32_t nsteps, double *dts) {
         }
         done += n;
     }
+    DG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return check_flags(c);
+}
+
+int32_t dg_next_dt(dg_ctx *c, double *dt) {
+    if (!c || !dt) return fail(c, DG_ERR_INVALID, "null argument");
+    if (!c->has_state) return fail(c, DG_ERR_NO_STATE, "no state set");
+    int r;
+    if ((r = use_device(c)) != DG_OK) return r;
+    DG_CUDA(c, cudaMemcpyAsync(dt, &c->ctl->dt[c->steps & 1], sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    DG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return check_flags(c);
+}
+
+int32_t dg_compute_step_dt(dg_ctx *c, double dt) {
+    if (!c) return fail(c, DG_ERR_INVALID, "null argument");
+    if (!(dt > 0.0) || !std::isfinite(dt)) return fail(c, DG_ERR_INVALID, "dt must be positive and finite");
+    if (!c->has_state) return fail(c, DG_ERR_NO_STATE, "no state set");
+    int r;
+    if ((r = use_device(c)) != DG_OK) return r;
+    set_next_dt_kernel<<<1, 1, 0, c->stream>>>(c->ctl, dt);
+    DG_CUDA(c, cudaGetLastError());
+    if ((r = enqueue(c, 1)) != DG_OK) return r;
     DG_CUDA(c, cudaStreamSynchronize(c->stream));
     return check_flags(c);
 }

@@ -12,6 +12,7 @@
 
 #include "../../include/deepgreen_net.h"
 #include "dg_conv.cuh"
+#include "dg_net_impl.h"
 
 using namespace dg;
 using namespace dg::net;
@@ -232,7 +233,7 @@ __global__ void unpad_kernel(const __nv_bfloat16 *__restrict__ src, __nv_bfloat1
 // ---------------------------------------------------------------------------
 template <int CIN, int COUT, int EPI>
 cudaError_t launch_conv(dg_net *net, const void *in, int nb, int xi, int yi, int zi, const __nv_bfloat16 *w,
-                        ConvArgs a) {
+                        ConvArgs a, cudaStream_t st) {
     using L = ConvSmem<CIN, COUT>;
     auto kern = conv_fwd_kernel<CIN, COUT, EPI>;
     static std::once_flag once;
@@ -253,7 +254,7 @@ cudaError_t launch_conv(dg_net *net, const void *in, int nb, int xi, int yi, int
     a.ntiles = nb * a.xo * a.tpp;
     a.status = net->status;
     const int grid = std::max(1, std::min(a.ntiles, std::max(1, occ) * net->nsm));
-    kern<<<grid, kConvThreads, L::BYTES, net->stream>>>(m, w, a);
+    kern<<<grid, kConvThreads, L::BYTES, st>>>(m, w, a);
     return cudaGetLastError();
 }
 
@@ -312,7 +313,9 @@ void free_ws(Workspace &ws) {
 int ensure_ws(dg_net *net, int n, int x, int y, int z, bool train) {
     Workspace &ws = net->ws;
     if (ws.n == n && ws.x == x && ws.y == y && ws.z == z && (ws.train || !train)) return DG_OK;
-    NET_CUDA(net, cudaStreamSynchronize(net->stream));
+    // the workspace may be in use on any stream (the corrector runs the
+    // network on its grid's stream)
+    NET_CUDA(net, cudaDeviceSynchronize());
     free_ws(ws);
     for (int l = 0; l < 3; ++l) {
         const size_t e = (size_t)n * (x - 2 * (l + 1)) * (y - 2 * (l + 1)) * (z - 2 * (l + 1));
@@ -361,8 +364,8 @@ int check_extents(dg_net *net, int n, int x, int y, int z) {
     return DG_OK;
 }
 
-// Forward pass; stores pre-activations when the workspace is a training one.
-int forward(dg_net *net, const void *feat, int n, int x, int y, int z, float *out, bool train) {
+// Forward pass on stream st; stores pre-activations when train is set.
+int forward(dg_net *net, const void *feat, int n, int x, int y, int z, float *out, bool train, cudaStream_t st) {
     Workspace &ws = net->ws;
     cudaError_t e;
     const void *in = feat;
@@ -373,8 +376,8 @@ int forward(dg_net *net, const void *feat, int n, int x, int y, int z, float *ou
         a.bias = net->b[l];
         a.out_a = ws.act[l];
         a.out_z = train ? ws.pre[l] : nullptr;
-        if (l == 0) e = launch_conv<kIO, kH, kEpiGelu>(net, in, n, xi, yi, zi, net->wf[l], a);
-        else e = launch_conv<kH, kH, kEpiGelu>(net, in, n, xi, yi, zi, net->wf[l], a);
+        if (l == 0) e = launch_conv<kIO, kH, kEpiGelu>(net, in, n, xi, yi, zi, net->wf[l], a, st);
+        else e = launch_conv<kH, kH, kEpiGelu>(net, in, n, xi, yi, zi, net->wf[l], a, st);
         if (e != cudaSuccess) return fail(net, DG_ERR_CUDA, std::string("conv launch: ") + cudaGetErrorString(e));
         in = ws.act[l];
         xi -= 2; yi -= 2; zi -= 2;
@@ -383,12 +386,25 @@ int forward(dg_net *net, const void *feat, int n, int x, int y, int z, float *ou
     a.ox = xi - 2; a.oy = yi - 2; a.oz = zi - 2; a.off = 0;
     a.bias = net->b[3];
     a.out_f = out;
-    e = launch_conv<kH, kIO, kEpiLinear>(net, in, n, xi, yi, zi, net->wf[3], a);
+    e = launch_conv<kH, kIO, kEpiLinear>(net, in, n, xi, yi, zi, net->wf[3], a, st);
     if (e != cudaSuccess) return fail(net, DG_ERR_CUDA, std::string("conv launch: ") + cudaGetErrorString(e));
     return DG_OK;
 }
 
 }  // namespace
+
+// Entry points for the other sources of the library (dg_net_impl.h).
+int dg::net_forward_stream(dg_net *net, const void *feat, int n, int x, int y, int z, float *out, cudaStream_t st) {
+    if (int r = check_extents(net, n, x, y, z)) return r;
+    if (int r = ensure_ws(net, n, x, y, z, false)) return r;
+    return forward(net, feat, n, x, y, z, out, false, st);
+}
+
+int dg::net_inputs(const dg_net *net) { return net->inputs; }
+int dg::net_device(const dg_net *net) { return net->device; }
+int dg::net_outputs(const dg_net *net) { return net->outputs; }
+unsigned *dg::net_status(dg_net *net) { return net->status; }
+const char *dg::net_error(const dg_net *net) { return net->err.c_str(); }
 
 extern "C" {
 
@@ -543,7 +559,7 @@ int32_t dg_net_forward(dg_net *net, const void *feat, int32_t n, int32_t x, int3
         return fail(net, DG_ERR_INVALID, "device pointers must be 16-byte aligned");
     NET_CUDA(net, cudaSetDevice(net->device));
     if (int r = ensure_ws(net, n, x, y, z, false)) return r;
-    return forward(net, feat, n, x, y, z, out, false);
+    return forward(net, feat, n, x, y, z, out, false, net->stream);
 }
 
 int32_t dg_net_forward_backward(dg_net *net, const void *feat, const float *target, int32_t n, int32_t x, int32_t y,
@@ -555,7 +571,7 @@ int32_t dg_net_forward_backward(dg_net *net, const void *feat, const float *targ
     NET_CUDA(net, cudaSetDevice(net->device));
     if (int r = ensure_ws(net, n, x, y, z, true)) return r;
     Workspace &ws = net->ws;
-    if (int r = forward(net, feat, n, x, y, z, ws.out, true)) return r;
+    if (int r = forward(net, feat, n, x, y, z, ws.out, true, net->stream)) return r;
     const int xo = x - 8, yo = y - 8, zo = z - 8;
     const long long nvox = (long long)n * xo * yo * zo;
     const float scale = (float)(2.0 / ((double)nvox * net->outputs));
@@ -579,8 +595,10 @@ int32_t dg_net_forward_backward(dg_net *net, const void *feat, const float *targ
         a.ox = ex + 2 + 4; a.oy = ey + 2 + 4; a.oz = ez + 2 + 4; a.off = 2;
         a.out_a = ws.dz[l - 1];
         a.zsrc = ws.pre[l - 1];
-        if (l == 3) e = launch_conv<kIO, kH, kEpiDGelu>(net, ws.dz[l], n, ex + 4, ey + 4, ez + 4, net->wd[l], a);
-        else e = launch_conv<kH, kH, kEpiDGelu>(net, ws.dz[l], n, ex + 4, ey + 4, ez + 4, net->wd[l], a);
+        if (l == 3) e = launch_conv<kIO, kH, kEpiDGelu>(net, ws.dz[l], n, ex + 4, ey + 4, ez + 4, net->wd[l], a,
+                                                        net->stream);
+        else e = launch_conv<kH, kH, kEpiDGelu>(net, ws.dz[l], n, ex + 4, ey + 4, ez + 4, net->wd[l], a,
+                                                net->stream);
         if (e != cudaSuccess) return fail(net, DG_ERR_CUDA, std::string("dgrad launch: ") + cudaGetErrorString(e));
     }
     if (int r = check_status(net)) return r;

@@ -76,6 +76,8 @@ SIGNATURES = {
     "dg_set_chunk": [_P, _I],
     "dg_status": [_P, ctypes.POINTER(ctypes.c_uint32)],
     "dg_last_error": [_P],
+    "dg_compute_step_dt": [_P, ctypes.c_double],
+    "dg_next_dt": [_P, ctypes.POINTER(ctypes.c_double)],
     "dg_compute_step_noalloc": [ctypes.POINTER(SimInfo), _P, _P, ctypes.POINTER(ctypes.c_double), _P],
     "dg_batch_create": [_I, ctypes.POINTER(SimInfo), ctypes.POINTER(ctypes.c_void_p)],
     "dg_batch_destroy": [_P],
@@ -99,6 +101,15 @@ SIGNATURES = {
     "dg_net_forward_backward": [_P, _P, _P, _I, _I, _I, _I, ctypes.POINTER(ctypes.c_double)],
     "dg_net_adam_step": [_P, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float],
     "dg_net_get_tensor": [_P, _I, _I, _P, ctypes.c_uint64],
+    "dg_coarsen": [_P, _P],
+    "dg_learned_features": [_P, _P, _P, _I, ctypes.c_double, ctypes.c_double, _I, _I, _I, _I, _P, _P],
+    "dg_learned_targets": [_P, _P, _P, _I, ctypes.c_double, _I, _I, _I, _I, _P, _P],
+    "dg_corrector_create": [_P, _P, _P, ctypes.POINTER(ctypes.c_void_p)],
+    "dg_corrector_destroy": [_P],
+    "dg_corrector_set_tolerance": [_P, ctypes.c_double],
+    "dg_corrector_step": [_P, _I],
+    "dg_corrector_stats": [_P, _P],
+    "dg_corrector_last_error": [_P],
     "dg_net_synchronize": [_P],
     "dg_net_get_stream": [_P],
     "dg_net_last_error": [_P],
@@ -108,6 +119,7 @@ _RESTYPES = {
     "dg_last_error": ctypes.c_char_p,
     "dg_batch_last_error": ctypes.c_char_p,
     "dg_net_last_error": ctypes.c_char_p,
+    "dg_corrector_last_error": ctypes.c_char_p,
     "dg_net_get_stream": ctypes.c_void_p,
 }
 
@@ -216,6 +228,16 @@ class Context:
         self._check(self.lib.dg_compute_step(self.h, int(nsteps),
                                              dts.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
         return dts[:nsteps]
+
+    def next_dt(self) -> float:
+        """dt of the coming step (dg_next_dt)."""
+        v = ctypes.c_double()
+        self._check(self.lib.dg_next_dt(self.h, ctypes.byref(v)))
+        return v.value
+
+    def compute_step_dt(self, dt):
+        """One step with the given dt (dg_compute_step_dt)."""
+        self._check(self.lib.dg_compute_step_dt(self.h, float(dt)))
 
     def enqueue_steps(self, nsteps):
         self._check(self.lib.dg_enqueue_steps(self.h, int(nsteps)))

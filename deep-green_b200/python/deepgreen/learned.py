@@ -1,0 +1,336 @@
+"""Learned coarse-grid correction: training pairs made by the solver, the
+training loop, and corrected coarse solves (include/deepgreen_net.h).
+
+Everything numerical runs in libdeepgreen.so: the Euler steps, coarsening,
+the network's input and target crops, the tensor-core convolutions, Adam and
+the corrector.  torch provides device buffers only.
+
+Pairs (one per coarse step): a fine periodic grid F (2n cells per axis) and
+a coarse grid C (n) that starts as the 2x2x2 sums of F.  F takes two steps
+(dt1, dt2, its own CFL dts); C takes one plain step of dt1 + dt2.  The pair
+is (C before, C after, truth = coarsened F after): the network learns
+truth - C_after from (C_before, C_after).
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import capi, setups
+from .net import IO_CHANNELS, Net
+
+INPUTS = 14
+OUTPUTS = 5
+GAMMA = 1.4
+CFL = 0.4
+
+
+class Norm(ctypes.Structure):
+    _fields_ = [("in_mean", ctypes.c_float * 16), ("in_inv_std", ctypes.c_float * 16),
+                ("out_std", ctypes.c_float * 16)]
+
+    @classmethod
+    def identity(cls):
+        n = cls()
+        for c in range(16):
+            n.in_mean[c] = 0.0
+            n.in_inv_std[c] = 1.0
+            n.out_std[c] = 1.0
+        return n
+
+    def to_dict(self):
+        return {k: list(getattr(self, k)) for k, _ in self._fields_}
+
+    @classmethod
+    def from_dict(cls, d):
+        n = cls()
+        for k, _ in cls._fields_:
+            for i, v in enumerate(d[k]):
+                getattr(n, k)[i] = float(v)
+        return n
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("steps", ctypes.c_uint64), ("fallback_steps", ctypes.c_uint64), ("masked_cells", ctypes.c_uint64),
+                ("cells", ctypes.c_uint64), ("max_drift", ctypes.c_double), ("last_drift", ctypes.c_double),
+                ("violations", ctypes.c_uint64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def _lib():
+    return capi.load()
+
+
+def _check(rc, msg_fn):
+    if rc != capi.DG_OK:
+        raise capi.DgError(rc, msg_fn())
+
+
+def grid(n: int, device: int = 0) -> capi.Context:
+    """A periodic FP32 grid of n^3 cells on the unit cube (minmod, CFL 0.4, gamma 1.4)."""
+    return capi.Context((n, n, n), 1.0 / n, (capi.PERIODIC,) * 6, gamma=GAMMA, cfl=CFL,
+                        limiter=capi.LIMITER_MINMOD, precision=capi.F32, device=device)
+
+
+def coarsen(fine: capi.Context, coarse: capi.Context):
+    lib = _lib()
+    _check(lib.dg_coarsen(fine.h, coarse.h), lambda: lib.dg_last_error(coarse.h).decode())
+
+
+class PackPool:
+    """Dense state packs on the device: slots x 5 x (n+4)^3 FP32."""
+
+    def __init__(self, n: int, slots: int, device: int = 0):
+        import torch
+        self.n = n
+        self.cells = (n + 4) ** 3
+        self.data = torch.empty((slots, 5, self.cells), dtype=torch.float32, device=torch.device("cuda", device))
+
+    def ptr(self, slot: int) -> int:
+        return self.data[slot].data_ptr()
+
+    def store(self, ctx: capi.Context, slot: int):
+        base = self.ptr(slot)
+        ctx.get_conserved_device([base + 4 * f * self.cells for f in range(5)])
+        ctx.synchronize()   # the copy runs on the grid's stream; later users may be on others
+
+
+def features(norm: Norm, before: int, after: int, n: int, origin, ext: int, out_ptr: int, stream=None):
+    lib = _lib()
+    ds = 1.0 / n
+    _check(lib.dg_learned_features(ctypes.byref(norm), before, after, n, ds, GAMMA, int(origin[0]), int(origin[1]),
+                                   int(origin[2]), ext, out_ptr, stream),
+           lambda: lib.dg_last_error(None).decode())
+
+
+def targets(norm: Norm, after: int, truth: int, n: int, origin, ext: int, out_ptr: int, stream=None):
+    lib = _lib()
+    ds = 1.0 / n
+    _check(lib.dg_learned_targets(ctypes.byref(norm), after, truth, n, ds, int(origin[0]), int(origin[1]),
+                                  int(origin[2]), ext, out_ptr, stream),
+           lambda: lib.dg_last_error(None).decode())
+
+
+class Corrector:
+    """dg_corrector: plain step + learned correction on a coarse grid."""
+
+    def __init__(self, ctx: capi.Context, net: Net, norm: Norm, tolerance: float | None = None):
+        self.lib = _lib()
+        self.ctx, self.net, self.norm = ctx, net, norm
+        h = ctypes.c_void_p()
+        _check(self.lib.dg_corrector_create(ctx.h, net.h, ctypes.byref(norm), ctypes.byref(h)),
+               lambda: self.lib.dg_corrector_last_error(None).decode())
+        self.h = h
+        if tolerance is not None:
+            _check(self.lib.dg_corrector_set_tolerance(self.h, float(tolerance)), self._err)
+
+    def _err(self):
+        return self.lib.dg_corrector_last_error(self.h).decode()
+
+    def step(self, nsteps: int = 1):
+        _check(self.lib.dg_corrector_step(self.h, int(nsteps)), self._err)
+
+    def stats(self) -> dict:
+        s = Stats()
+        _check(self.lib.dg_corrector_stats(self.h, ctypes.byref(s)), self._err)
+        return s.as_dict()
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.dg_corrector_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
+# Initial states of the training and evaluation workloads
+# ---------------------------------------------------------------------------
+def initial_state(kind: str, n: int, seed: int, **kw):
+    """'kh': KH layer with shear / ratio (kw, else drawn from seed: shear in
+    [0.2, 0.8], density ratio in [1, 4]); 'fourier': 8 random modes."""
+    if kind == "kh":
+        rng = np.random.default_rng(seed)
+        shear = kw.get("shear", rng.uniform(0.2, 0.8))
+        ratio = kw.get("ratio", rng.uniform(1.0, 4.0))
+        prim, _, _ = setups.kelvin_helmholtz(n, seed=seed, shear=shear, ratio=ratio)
+        return prim, {"kind": "kh", "seed": seed, "shear": float(shear), "ratio": float(ratio)}
+    if kind == "fourier":
+        prim, _, _ = setups.fourier_modes(n, seed)
+        return prim, {"kind": "fourier", "seed": seed}
+    raise ValueError(kind)
+
+
+# ---------------------------------------------------------------------------
+# Pairs
+# ---------------------------------------------------------------------------
+@dataclass
+class PairSet:
+    n: int                                   # coarse cells per axis
+    before: PackPool
+    after: PackPool
+    truth: PackPool
+    count: int = 0
+    meta: list = field(default_factory=list)
+
+
+def make_pairs(n_coarse: int, trajectories, pairs_per_trajectory: int, spacing: int, warmup_max: int, seed: int,
+               device: int = 0, log=print) -> PairSet:
+    """trajectories: list of (kind, seed).  Per trajectory: a fine grid
+    (2 n_coarse) from that initial state, a random warm-up of 0..warmup_max
+    fine steps, then pairs every `spacing` fine steps."""
+    total = len(trajectories) * pairs_per_trajectory
+    ps = PairSet(n_coarse, PackPool(n_coarse, total, device), PackPool(n_coarse, total, device),
+                 PackPool(n_coarse, total, device))
+    rng = np.random.default_rng(seed)
+    fine = grid(2 * n_coarse, device)
+    coarse = grid(n_coarse, device)
+    for kind, s in trajectories:
+        prim, meta = initial_state(kind, 2 * n_coarse, s)
+        fine.set_primitives(prim)
+        del prim
+        w = int(rng.integers(0, warmup_max + 1))
+        if w:
+            fine.compute_step(w)
+        t0 = time.time()
+        for k in range(pairs_per_trajectory):
+            slot = ps.count
+            coarsen(fine, coarse)
+            ps.before.store(coarse, slot)
+            dts = fine.compute_step(2)
+            coarse.compute_step_dt(float(dts[0] + dts[1]))
+            ps.after.store(coarse, slot)
+            coarsen(fine, coarse)
+            ps.truth.store(coarse, slot)
+            ps.count += 1
+            ps.meta.append(dict(meta, fine_step=w + k * (spacing + 2)))
+            if k + 1 < pairs_per_trajectory and spacing:
+                fine.compute_step(spacing)
+        log(f"pairs: {meta} warm-up {w}: {pairs_per_trajectory} pairs in {time.time() - t0:.2f}s")
+    fine.close()
+    coarse.close()
+    return ps
+
+
+# ---------------------------------------------------------------------------
+# Training
+# ---------------------------------------------------------------------------
+class Batcher:
+    """Random crops of the pair set into device batch buffers."""
+
+    def __init__(self, ps: PairSet, batch: int, crop: int, seed: int, device: int = 0):
+        import torch
+        self.ps, self.batch, self.crop = ps, batch, crop
+        self.ext = crop + 8
+        dev = torch.device("cuda", device)
+        self.feat = torch.zeros((batch, self.ext, self.ext, self.ext, IO_CHANNELS), dtype=torch.bfloat16, device=dev)
+        self.tgt = torch.zeros((batch, crop, crop, crop, IO_CHANNELS), dtype=torch.float32, device=dev)
+        self.rng = np.random.default_rng(seed)
+
+    def fill(self, norm: Norm, stream=None):
+        n = self.ps.n
+        fstride = self.ext ** 3 * IO_CHANNELS * 2
+        tstride = self.crop ** 3 * IO_CHANNELS * 4
+        for i in range(self.batch):
+            slot = int(self.rng.integers(0, self.ps.count))
+            o = self.rng.integers(0, n, 3)
+            features(norm, self.ps.before.ptr(slot), self.ps.after.ptr(slot), n, o - 4, self.ext,
+                     self.feat.data_ptr() + i * fstride, stream)
+            targets(norm, self.ps.after.ptr(slot), self.ps.truth.ptr(slot), n, o, self.crop,
+                    self.tgt.data_ptr() + i * tstride, stream)
+
+
+def fit_norm(ps: PairSet, samples: int = 16, crop: int = 48, seed: int = 0) -> Norm:
+    """Per-channel mean / std of the inputs and std of the targets over random
+    crops of the pair set (host statistics of device-made crops)."""
+    import torch
+    ident = Norm.identity()
+    b = Batcher(ps, samples, crop, seed)
+    b.fill(ident)
+    torch.cuda.synchronize()
+    f = b.feat.float().reshape(-1, IO_CHANNELS).cpu().numpy().astype(np.float64)
+    t = b.tgt.reshape(-1, IO_CHANNELS).cpu().numpy().astype(np.float64)
+    norm = Norm.identity()
+    for c in range(16):
+        if c < INPUTS:
+            norm.in_mean[c] = float(f[:, c].mean())
+            sd = float(f[:, c].std())
+            norm.in_inv_std[c] = 1.0 / sd if sd > 0 else 1.0
+        else:
+            norm.in_mean[c] = 0.0
+            norm.in_inv_std[c] = 0.0
+        norm.out_std[c] = float(t[:, c].std()) if c < OUTPUTS and t[:, c].std() > 0 else 1.0
+    return norm
+
+
+def train(net: Net, ps: PairSet, norm: Norm, steps: int, batch: int = 8, crop: int = 64, lr: float = 1e-3,
+          lr_min: float = 1e-5, seed: int = 0, log_every: int = 100, log=print):
+    """Adam on the MSE of the normalised correction; cosine learning-rate
+    decay from lr to lr_min.  Returns the loss history."""
+    b = Batcher(ps, batch, crop, seed)
+    hist = []
+    t0 = time.time()
+    for it in range(steps):
+        b.fill(norm)
+        loss = net.forward_backward(b.feat, b.tgt)
+        rate = lr_min + 0.5 * (lr - lr_min) * (1.0 + math.cos(math.pi * it / max(steps, 1)))
+        net.adam_step(rate)
+        hist.append(loss)
+        if log_every and (it % log_every == 0 or it == steps - 1):
+            log(f"train step {it}: loss {loss:.5f} lr {rate:.2e} ({time.time() - t0:.1f}s)")
+    return hist
+
+
+def save(path, net: Net, norm: Norm, extra=None):
+    params = [(w.tolist(), b.tolist()) for w, b in net.params()]
+    with open(path, "w") as fh:
+        json.dump({"norm": norm.to_dict(), "params": params, "extra": extra or {}}, fh)
+
+
+def load(path, device: int = 0):
+    with open(path) as fh:
+        d = json.load(fh)
+    net = Net(INPUTS, OUTPUTS, device=device)
+    net.set_params([(np.asarray(w, np.float32), np.asarray(b, np.float32)) for w, b in d["params"]])
+    return net, Norm.from_dict(d["norm"]), d.get("extra", {})
+
+
+# ---------------------------------------------------------------------------
+# Corrected and plain solves to a given time
+# ---------------------------------------------------------------------------
+def solve_to_time(ctx: capi.Context, t_end: float, corrector: Corrector | None = None, max_steps: int = 100000):
+    """Advance ctx from time 0 to t_end: CFL steps (plain, or corrected when a
+    corrector is given) while they stay short of t_end, then one plain step
+    of the remaining time.  Each step reads the coming dt first, as the
+    reference's loop reads dt every step.  Returns (steps, seconds)."""
+    import torch
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    t = 0.0
+    steps = 0
+    while steps < max_steps:
+        dt = ctx.next_dt()
+        if t + dt >= t_end:
+            if t_end > t:
+                ctx.compute_step_dt(t_end - t)
+                steps += 1
+            break
+        if corrector is not None:
+            corrector.step(1)
+        else:
+            ctx.enqueue_steps(1)
+        t += dt
+        steps += 1
+    ctx.synchronize()
+    return steps, time.perf_counter() - t0

@@ -48,10 +48,11 @@ def centres(n_int: int, ds: float, lo: float = 0.0) -> np.ndarray:
 
 
 def kelvin_helmholtz(n: int = 64, seed: int = 1, noise: float = 1e-3, ny: int | None = None,
-                     nz: int | None = None):
-    """KH layer: rho=2, vx=+0.5 for |y-0.5|<0.25, else rho=1, vx=-0.5;
-    p=2.5; vy=0.01 sin(4 pi x)(exp(-(y-0.25)^2/0.005)+exp(-(y-0.75)^2/0.005));
-    vz=0; plus uniform noise in [-noise, noise] on vx, vy, vz.
+                     nz: int | None = None, shear: float = 0.5, ratio: float = 2.0, p0: float = 2.5):
+    """KH layer: rho=ratio, vx=+shear for |y-0.5|<0.25, else rho=1,
+    vx=-shear; p=p0; vy=0.01 sin(4 pi x)(exp(-(y-0.25)^2/0.005)+exp(-(y-0.75)^2/0.005));
+    vz=0; plus uniform noise in [-noise, noise] on vx, vy, vz.  The defaults
+    (shear 0.5, ratio 2, p 2.5) are the 64^3 periodic parity workload.
     Returns (prims, ds, bcs)."""
     ny = ny or n
     nz = nz or n
@@ -60,12 +61,12 @@ def kelvin_helmholtz(n: int = 64, seed: int = 1, noise: float = 1e-3, ny: int | 
     y = centres(ny, ds)[None, :, None]
     shape = (n + 4, ny + 4, nz + 4)
     inner = np.abs(y - 0.5) < 0.25
-    rho = np.broadcast_to(np.where(inner, 2.0, 1.0), shape).copy()
-    vx = np.broadcast_to(np.where(inner, 0.5, -0.5), shape).copy()
+    rho = np.broadcast_to(np.where(inner, float(ratio), 1.0), shape).copy()
+    vx = np.broadcast_to(np.where(inner, float(shear), -float(shear)), shape).copy()
     vy = np.broadcast_to(0.01 * np.sin(4 * np.pi * x) * (np.exp(-(y - 0.25) ** 2 / 0.005)
                                                           + np.exp(-(y - 0.75) ** 2 / 0.005)), shape).copy()
     vz = np.zeros(shape)
-    p = np.full(shape, 2.5)
+    p = np.full(shape, float(p0))
     if noise:
         # noise indexed by interior cell (i, j, k) -> (i*ny + j)*nz + k
         ii = np.arange(shape[0])[:, None, None] - 2
@@ -76,6 +77,33 @@ def kelvin_helmholtz(n: int = 64, seed: int = 1, noise: float = 1e-3, ny: int | 
         for comp, v in enumerate((vx, vy, vz)):
             v += noise * (2.0 * counter_uniform(seed, idx, comp) - 1.0)
     return [rho, vx, vy, vz, p], ds, (PERIODIC,) * 6
+
+
+def fourier_modes(n: int, seed: int, modes: int = 8, amp: float = 0.1, kmax: int = 4):
+    """Smooth periodic state on the unit cube: rho = 1, p = 1, v = 0 plus
+    `modes` random Fourier modes sin(2 pi k.x + phase), integer wave vectors
+    k in [-kmax, kmax]^3 (not 0), each with its own amplitude in
+    [-amp, amp] on rho, p, vx, vy and vz.  Returns (prims, ds, bcs)."""
+    rng = np.random.default_rng(seed)
+    ds = 1.0 / n
+    c = centres(n, ds)
+    shape = (n + 4,) * 3
+    prim = [np.ones(shape), np.zeros(shape), np.zeros(shape), np.zeros(shape), np.ones(shape)]
+    for _ in range(modes):
+        k = np.zeros(3, dtype=np.int64)
+        while not k.any():
+            k = rng.integers(-kmax, kmax + 1, 3)
+        phase = rng.uniform(0.0, 2.0 * np.pi)
+        a = rng.uniform(-amp, amp, 5)
+        # sin(2 pi k.x + phase) = Im(e^{i phase} e^{i 2 pi kx x} e^{i 2 pi ky y} e^{i 2 pi kz z})
+        ex = np.exp(1j * (2 * np.pi * k[0] * c + phase))[:, None, None]
+        ey = np.exp(1j * 2 * np.pi * k[1] * c)[None, :, None]
+        ez = np.exp(1j * 2 * np.pi * k[2] * c)[None, None, :]
+        s = np.imag((ex * ey) * ez)
+        order = (0, 4, 1, 2, 3)          # amplitudes for rho, p, vx, vy, vz
+        for f, j in zip(order, range(5)):
+            prim[f] += a[j] * s
+    return prim, ds, (PERIODIC,) * 6
 
 
 def sod(n: int = 64, ny: int | None = None, nz: int | None = None):

@@ -148,6 +148,20 @@ int32_t dg_step_launch_shape(dg_ctx *ctx, int32_t *blocks, int32_t *threads, int
 /* Override the x-planes per block of the step kernel (0 = automatic). */
 int32_t dg_set_chunk(dg_ctx *ctx, int32_t chunk);
 
+/* The dt the next compute_step will take (calc_timestep, physics.rs:177, of
+ * the current state).  No counterpart in the reference, where dt is only
+ * known after the step; a solve that must end on a given time reads it to
+ * shorten its last step.  Synchronises. */
+int32_t dg_next_dt(dg_ctx *ctx, double *dt);
+
+/* One step with a caller-chosen dt instead of the CFL dt of calc_timestep
+ * (physics.rs:177).  No counterpart in the reference: it advances a coarse
+ * grid over exactly the time of two fine-grid steps when the solver
+ * generates training pairs for the learned correction, and lets a solve end
+ * on a given time.  The next dt is computed from the new state as usual.
+ * Synchronises. */
+int32_t dg_compute_step_dt(dg_ctx *ctx, double dt);
+
 /* One compute_step on caller-owned device memory; the library allocates
  * nothing.  No counterpart in the reference: it is for callers that must
  * not let a library call cudaMalloc, such as a host program whose device

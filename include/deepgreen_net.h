@@ -77,6 +77,81 @@ int32_t dg_net_adam_step(dg_net *net, float lr, float beta1, float beta2, float 
  * bits, unpadded).  Layer 0..3; host buffer sized by the caller. */
 int32_t dg_net_get_tensor(dg_net *net, int32_t layer, int32_t which, void *host, uint64_t bytes);
 
+/* ---- Learned coarse step -------------------------------------------------
+ *
+ * The network corrects a coarse grid after each plain step.  Its 14 input
+ * channels per cell, from the conserved densities before (U0) and after (U1)
+ * the plain step (density = per-cell total / ds^3):
+ *   0 rho1, 1-3 (rho v)1, 4 E1,  5-9 U1 - U0 (same order),
+ *   10-12 v1 = (rho v)1 / rho1,  13 p1 = (gamma-1)(E1 - |(rho v)1|^2 / (2 rho1)),
+ * each normalised as (raw - in_mean[c]) * in_inv_std[c] (channels 14, 15 are
+ * zero).  Output channel c < 5 is the correction of conserved density c in
+ * units of out_std[c].  Grids must be cubic and periodic: the network's
+ * 4-cell halo wraps around the domain.
+ *
+ * "State packs" are dense device copies of a grid's conserved state: 5
+ * fields (mass, mom_x, mom_y, mom_z, energy) of (n+4)^3 FP32 values each, C
+ * order with ghosts, consecutive -- what dg_get_conserved_device writes when
+ * given pointers 1, 2, ... fields apart. */
+#define DG_LEARNED_INPUTS 14
+#define DG_LEARNED_OUTPUTS 5
+
+typedef struct dg_learned_norm {
+    float in_mean[16];
+    float in_inv_std[16];
+    float out_std[16];
+} dg_learned_norm;
+
+/* coarse := 2x2x2 sums of fine's per-cell totals over the interior (fine
+ * interior extents twice the coarse ones, both FP32); ghosts and the next dt
+ * of the coarse grid follow as after dg_set_conserved.  Synchronises. */
+int32_t dg_coarsen(dg_ctx *fine, dg_ctx *coarse);
+
+/* Network inputs of a crop of a periodic cubic grid with n interior cells per
+ * axis, from state packs `before` and `after`: ext^3 cells starting at
+ * interior cell (ox, oy, oz) (wrapped), written as BF16 [ext][ext][ext][16]
+ * to feat.  Asynchronous on `stream` (cudaStream_t or NULL). */
+int32_t dg_learned_features(const dg_learned_norm *norm, const float *before, const float *after, int32_t n, double ds,
+                            double gamma, int32_t ox, int32_t oy, int32_t oz, int32_t ext, void *feat, void *stream);
+
+/* Training targets: (truth - after) / ds^3 / out_std per field over the ext^3
+ * cells starting at (ox, oy, oz), FP32 [ext][ext][ext][16] (channels >= 5
+ * zero).  Asynchronous on `stream`. */
+int32_t dg_learned_targets(const dg_learned_norm *norm, const float *after, const float *truth, int32_t n, double ds,
+                           int32_t ox, int32_t oy, int32_t oz, int32_t ext, float *out, void *stream);
+
+typedef struct dg_corrector dg_corrector;
+
+typedef struct dg_learned_stats {
+    uint64_t steps;           /* corrected steps attempted */
+    uint64_t fallback_steps;  /* steps that kept the plain coarse state everywhere */
+    uint64_t masked_cells;    /* cells that kept their plain value (rho or p would not stay positive) */
+    uint64_t cells;           /* cells examined: steps x n^3 */
+    double max_drift;         /* largest |sum(U' - U)| / sum|U| over fields, accepted steps */
+    double last_drift;        /* the same for the latest step, kept or not */
+    uint64_t violations;      /* cells that lost positivity after the mean removal (each rejects its step) */
+} dg_learned_stats;
+
+/* A corrector couples a coarse FP32 context (cubic, periodic) and a network
+ * (14 inputs, 5 outputs).  Each step: one plain step; the network's
+ * correction, zero in cells where rho or p of the corrected state would not
+ * be positive, minus its mean over the other cells; the whole step falls back
+ * to the plain state if a cell still loses positivity or the correction
+ * changes a field's total by more than `tolerance` (default 1e-10) of its
+ * L1 norm; the next dt comes from the state kept. */
+int32_t dg_corrector_create(dg_ctx *coarse, dg_net *net, const dg_learned_norm *norm, dg_corrector **out);
+/* The context and the network are not owned: they must outlive every step of
+ * the corrector.  Destroying the corrector touches neither, so it may come
+ * after them. */
+int32_t dg_corrector_destroy(dg_corrector *cor);
+int32_t dg_corrector_set_tolerance(dg_corrector *cor, double tolerance);
+/* nsteps corrected steps, asynchronous on the context's stream (dg_get_dts
+ * and dg_synchronize of the context apply). */
+int32_t dg_corrector_step(dg_corrector *cor, int32_t nsteps);
+/* Totals since creation; synchronises. */
+int32_t dg_corrector_stats(dg_corrector *cor, dg_learned_stats *out);
+const char *dg_corrector_last_error(const dg_corrector *cor);
+
 int32_t dg_net_synchronize(dg_net *net);
 void *dg_net_get_stream(dg_net *net);
 const char *dg_net_last_error(const dg_net *net);
