@@ -1,7 +1,10 @@
 // dg_conv.cuh -- BF16 3x3x3 convolution kernels of the correction network on
 // the 5th-generation tensor cores (tcgen05, FP32 accumulation in TMEM).
 //
-// Activations are channels-last, [n][x][y][z][C] BF16, z fastest.  Every
+// Activations are BF16 in a channel-blocked layout, [n][x][C/8][y][z][8]:
+// for each x-plane and group of 8 channels, the (y, z) plane is contiguous
+// with 16 bytes per cell, so every TMA box below reads 16-byte rows that
+// are contiguous in memory.  Every
 // convolution is "valid": an input of extents (X, Y, Z) gives an output of
 // (X-2, Y-2, Z-2), out[v] = sum_t W_t in[v + t], t = (dx, dy, dz) in 0..2,
 // weights W[co][ci][dx][dy][dz] (the layout of torch.nn.Conv3d on tensors
@@ -11,20 +14,34 @@
 // N=COUT] = sum over 27 taps x CIN channels):
 //   * positions are enumerated along the flattened (y, z) index of the INPUT,
 //     p = y * Zin + z, within one (n, x) plane; tap (dx, dy, dz) is then the
-//     plane x+dx shifted by dy*Zin + dz, so one tile of 128 consecutive p
-//     needs, per channel group of 8 and per dy, one window of 136 positions
-//     in each of the 3 planes x..x+2 -- one 4-D TMA box (8 ch, 136 p, 3 x, 1)
-//     that lands as [dx][p][8 ch], i.e. 8 positions x 16 bytes = one K-major
-//     core matrix; every tap's A operand is the same window at a different
-//     start address.  Positions with z >= Zin-2 wrap into the next row and
-//     are dropped by the epilogue (2 of every Zin positions).
-//   * all 27 x CIN x COUT weights stay in shared memory (K-major, packed on
-//     the host as [tap][ci/8][co][8]).
-//   * warp 0 issues TMA copies into a 2-stage ring, warp 1 owns TMEM and
-//     issues the MMAs (one thread), warps 2-5 drain the double-buffered
-//     accumulators (bias, GELU / GELU', BF16 or FP32 stores).
+//     plane x+dx shifted by dy*Zin + dz.  A tile of 128 consecutive p needs,
+//     per channel group of 8 and per dy, a window of 136 positions of an
+//     input plane, stored [p][8 ch]: 8 positions x 16 bytes = one K-major
+//     core matrix, so each (dy, dz) is a window at a different start
+//     address.  Positions with z >= Zin-2 wrap into the next row and are
+//     dropped by the epilogue (2 of every Zin positions).
+//   * a block walks along x through a column of tiles (fixed n and p range,
+//     x in a chunk).  Input plane P serves output planes P, P-1 and P-2 (taps
+//     dx = 0, 1, 2), so each (dy, dz, 16 channels) is ONE MMA with N = 3 COUT
+//     against the weights [W(dx=2) | W(dx=1) | W(dx=0)]: its three column
+//     blocks land in the TMEM accumulators of output planes P-2, P-1, P,
+//     which sit in a ring of 8 consecutive slots (an MMA that would wrap the
+//     ring is split in two).  Output plane P-2 is then complete; the epilogue
+//     drains its slot and zeroes it for reuse, so every MMA accumulates.
+//     Each input plane is read from shared memory once, by 9 x CIN/16 MMAs.
+//   * input planes arrive by TMA into a ring of shared-memory slots: 3 x
+//     CIN/8 boxes of 136 positions, read as 68 pairs of positions so every
+//     box row is one 32-byte sector.  Planes at the start of a chunk produce
+//     two partial outputs that are drained and discarded.
+//   * all weights stay in shared memory (K-major, packed on the host as
+//     [dy, dz][ci/8][dx' = 2-dx][co][8]).
+//   * warp 0 issues the TMA copies, warp 1 owns TMEM and issues the MMAs
+//     (one thread, descriptors advanced by constant offsets), warps 2-9
+//     drain the accumulators (two warps per TMEM sub-partition, each half
+//     of the columns: bias, GELU / GELU', BF16 or FP32 stores).
 //   The input-gradient of a layer is the same kernel run on the output
 //   gradient zero-padded by 2 with the taps flipped and W transposed.
+//   Input z extents must be even (pairs of positions).
 //
 // Weight-gradient kernel: dW_t[co][ci] = sum_v dZ[v][co] X[v+t][ci] over
 // all output positions v.  D[M=128, N=COUT] per (dy, dz) pair, 9 TMEM
@@ -48,22 +65,30 @@ constexpr int kM = 128;                    // positions per tile (MMA M)
 constexpr int kWz = 136;                   // window positions per row (>= kM + 2; 128-byte boxes)
 constexpr int kBox = 3 * kWz * 16;         // one TMA box: 3 rows of kWz positions x 8 channels (6528 B)
 constexpr int kStages = 2;
-constexpr int kConvThreads = 192;          // 6 warps: TMA, MMA, 4 x epilogue
+constexpr int kConvThreads = 192;          // weight gradient: 6 warps (TMA, MMA, 4 x epilogue)
+constexpr int kFwdThreads = 320;           // forward: 10 warps (TMA, MMA, 8 x epilogue)
+constexpr int kRing = 8;                   // TMEM accumulator slots (output planes) of the forward kernel
+constexpr int kPlaneRow = kWz * 16;        // one (channel group, dy) window of one x-plane (2176 B)
+constexpr int kSlots = 4;                  // input-plane slots of the forward kernel's shared-memory ring
 constexpr unsigned kNetTimeout = 0x2u;     // status bit: a wait ran out
 
 enum Epilogue : int { kEpiGelu = 0, kEpiLinear = 1, kEpiDGelu = 2 };
 
+// Output tensors: BF16 ones are channel-blocked like the inputs, the FP32
+// output of the linear layer is channels-last [n][x][y][z][COUT].
 struct ConvArgs {
-    int nb, xi, yi, zi;             // input extents
+    int nb, xi, yi, zi;             // input extents (zi even)
     int xo, yo, zo;                 // output extents (input - 2)
     int tpp;                        // tiles per (n, x) plane: ceil(yo * zi / kM)
-    int ntiles;                     // nb * xo * tpp
+    int xchunk;                     // planes of x per work unit
+    int nxc;                        // x chunks: ceil(xo / xchunk)
+    int nunits;                     // work units nb * tpp * nxc: (n, p range, x chunk)
     int ox, oy, oz, off;            // extents of the output buffer and offset of the output region in it
     const float *bias;              // [COUT] (kEpiGelu, kEpiLinear)
     __nv_bfloat16 *out_a;           // BF16 output: activation (kEpiGelu) or gradient (kEpiDGelu)
-    __nv_bfloat16 *out_z;           // BF16 pre-activation, dense [nb][xo][yo][zo][COUT] (kEpiGelu, may be null)
+    __nv_bfloat16 *out_z;           // BF16 pre-activation, extents (xo, yo, zo), no offset (kEpiGelu, may be null)
     float *out_f;                   // FP32 output (kEpiLinear)
-    const __nv_bfloat16 *zsrc;      // pre-activation below, dense [nb][xo][yo][zo][COUT] (kEpiDGelu)
+    const __nv_bfloat16 *zsrc;      // pre-activation below, extents (xo, yo, zo), no offset (kEpiDGelu)
     unsigned *status;
 };
 
@@ -80,15 +105,30 @@ __device__ __forceinline__ unsigned char *align128(unsigned char *p) {
     return p + ((128u - (s & 127u)) & 127u);
 }
 
-__device__ __forceinline__ float gelu(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+// GELU in its tanh form, x/2 (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3)))
+// (Hendrycks & Gimpel 2016), on the hardware tanh approximation
+// (tanh.approx.f32, relative error ~2^-11, far below BF16 rounding).
+__device__ __forceinline__ float tanh_approx(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+constexpr float kGeluC0 = 0.79788456080286536f;   // sqrt(2 / pi)
+constexpr float kGeluC1 = 0.044715f;
+
+__device__ __forceinline__ float gelu(float x) {
+    const float t = tanh_approx(kGeluC0 * (x + kGeluC1 * x * x * x));
+    return 0.5f * x * (1.0f + t);
+}
 
 __device__ __forceinline__ float gelu_grad(float x) {
-    return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+    const float t = tanh_approx(kGeluC0 * (x + kGeluC1 * x * x * x));
+    return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * kGeluC0 * (1.0f + 3.0f * kGeluC1 * x * x);
 }
 
 // All lanes of the warp agree on a wait's outcome.
 __device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity) {
-    const bool ok = mbar_wait(bar, parity, kWaitBudget);
+    const bool ok = tc::mbar_sleep_wait(bar, parity, kWaitBudget);
     return __all_sync(0xffffffffu, ok);
 }
 
@@ -123,35 +163,41 @@ template <int CIN, int COUT>
 struct ConvSmem {
     static constexpr int CG = CIN / 8;
     static constexpr int WB = 27 * CG * COUT * 16;           // weights
-    static constexpr int STAGE = CG * 3 * kBox;              // one input window
-    static constexpr int BYTES = WB + kStages * STAGE + 128 /*barriers*/ + 128 /*alignment*/;
+    static constexpr int SLOT = CG * 3 * kPlaneRow;          // windows of one x-plane: [cg][dy][kWz][8]
+    static constexpr int BYTES = WB + kSlots * SLOT + 512 /*barriers*/ + 128 /*alignment*/;
 };
 
 template <int CIN, int COUT, int EPI>
-__global__ void __launch_bounds__(kConvThreads, 1)
+__global__ void __launch_bounds__(kFwdThreads, 1)
     conv_fwd_kernel(const __grid_constant__ CUtensorMap in_map, const __nv_bfloat16 *__restrict__ wpack, ConvArgs a) {
     static_assert(CIN % 16 == 0 && (COUT == 16 || COUT == 32), "unsupported channel counts");
     using L = ConvSmem<CIN, COUT>;
     constexpr int CG = L::CG, KC = CIN / 16;
-    constexpr uint32_t TCOLS = 2 * COUT < 32 ? 32 : 2 * COUT;
-    constexpr uint32_t IDESC = tc::idesc_bf16(kM, COUT, 0, 0);
+    constexpr int NC = COUT / 2;                 // columns per epilogue warp
+    constexpr int NB = 3 * COUT;                 // rows of the weight operand (three dx blocks)
+    constexpr uint32_t TCOLS = kRing * COUT;     // 256 or 128
+    constexpr uint32_t ID3 = tc::idesc_bf16(kM, 3 * COUT, 0, 0);
+    constexpr uint32_t ID2 = tc::idesc_bf16(kM, 2 * COUT, 0, 0);
+    constexpr uint32_t ID1 = tc::idesc_bf16(kM, COUT, 0, 0);
 
     extern __shared__ unsigned char smem_raw[];
     unsigned char *smem = align128(smem_raw);
     unsigned char *wsm = smem;
-    unsigned char *stg = smem + L::WB;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(stg + kStages * L::STAGE);
-    uint64_t *full = bars, *empty = bars + 2, *tfull = bars + 4, *tempty = bars + 6, *wbar = bars + 8,
-             *drain = bars + 9;
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 10);
+    unsigned char *ring = smem + L::WB;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(ring + kSlots * L::SLOT);
+    uint64_t *full = bars, *empty = bars + kSlots, *tfull = bars + 2 * kSlots, *tempty = tfull + kRing,
+             *wbar = tempty + kRing, *drain = wbar + 1;
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(drain + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
-        for (int i = 0; i < 2; ++i) {
+        for (int i = 0; i < kSlots; ++i) {
             mbar_init(full + i, 1);
             mbar_init(empty + i, 1);
+        }
+        for (int i = 0; i < kRing; ++i) {
             mbar_init(tfull + i, 1);
-            mbar_init(tempty + i, 4);
+            mbar_init(tempty + i, 8);
         }
         mbar_init(wbar, 1);
         mbar_init(drain, 1);
@@ -162,114 +208,187 @@ __global__ void __launch_bounds__(kConvThreads, 1)
     __syncthreads();
     tc::fence_after();
     const uint32_t tbase = *tslot;
+    const int q = warp & 3;                      // epilogue: TMEM sub-partition (lanes 32q..32q+31)
+    const int c0 = ((warp - 2) >> 2) * NC;       // epilogue: first column of this warp's half
+    if (warp >= 2) {
+        // every accumulator starts at zero: all MMAs accumulate
+        float zero[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) zero[c] = 0.0f;
+        for (int sl = 0; sl < kRing; ++sl) {
+            const uint32_t ta = tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)(sl * COUT + c0);
+            if constexpr (NC == 16) tc::tmem_st16(ta, zero);
+            else tc::tmem_st8(ta, zero);
+        }
+        tc::tmem_wait_st();
+    }
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
     bool ok = true;
+    float bias[NC];                              // epilogue: this warp's bias columns
+#pragma unroll
+    for (int c = 0; c < NC; ++c) bias[c] = (EPI != kEpiDGelu && warp >= 2) ? __ldg(a.bias + c0 + c) : 0.0f;
 
     if (warp == 0) {
         if (lane == 0) {
             mbar_expect_tx(wbar, L::WB);
             tc::bulk_load(wsm, wpack, L::WB, wbar);
-            int it = 0;
-            for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, ++it) {
-                const int s = it & 1, u = it >> 1;
-                if (u > 0 && !mbar_wait(empty + s, (u - 1) & 1, kWaitBudget)) {
-                    ok = false;
-                    break;
+            long long g = 0;                      // planes issued by this block
+            for (int unit = blockIdx.x; ok && unit < a.nunits; unit += gridDim.x) {
+                const int xc = unit % a.nxc, r = unit / a.nxc;
+                const int pt = r % a.tpp, b = r / a.tpp;
+                const int x0 = xc * a.xchunk, len = min(a.xchunk, a.xo - x0);
+                const int pair0 = pt * (kM / 2);
+                for (int k = 0; k < len + 2; ++k, ++g) {
+                    const int slot = (int)(g % kSlots);
+                    const long long use = g / kSlots;
+                    if (use > 0 && !tc::mbar_sleep_wait(empty + slot, (uint32_t)((use - 1) & 1), kWaitBudget)) {
+                        ok = false;
+                        break;
+                    }
+                    mbar_expect_tx(full + slot, L::SLOT);
+                    unsigned char *dst = ring + slot * L::SLOT;
+                    for (int cg = 0; cg < CG; ++cg)
+                        for (int dy = 0; dy < 3; ++dy)
+                            tc::tma_load_5d(dst + (cg * 3 + dy) * kPlaneRow, &in_map, 0, pair0 + dy * (a.zi / 2), cg,
+                                            x0 + k, b, full + slot);
                 }
-                const int pt = tile % a.tpp, bx = tile / a.tpp;
-                const int x = bx % a.xo, b = bx / a.xo;
-                const int p0 = pt * kM;
-                mbar_expect_tx(full + s, L::STAGE);
-                unsigned char *dst = stg + s * L::STAGE;
-                for (int cg = 0; cg < CG; ++cg)
-                    for (int dy = 0; dy < 3; ++dy)
-                        tma_load_4d(dst + (cg * 3 + dy) * kBox, &in_map, cg * 8, p0 + dy * a.zi, x, b, full + s);
             }
             // copies still in flight must land before the block exits
-            for (int j = it - 2 < 0 ? 0 : it - 2; j < it; ++j) ok &= mbar_wait(full + (j & 1), (j >> 1) & 1, kWaitBudget);
-            ok &= mbar_wait(wbar, 0, kWaitBudget);
+            for (long long j = g - kSlots < 0 ? 0 : g - kSlots; j < g; ++j)
+                ok &= tc::mbar_sleep_wait(full + (int)(j % kSlots), (uint32_t)((j / kSlots) & 1), kWaitBudget);
+            ok &= tc::mbar_sleep_wait(wbar, 0, kWaitBudget);
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            ok = mbar_wait(wbar, 0, kWaitBudget);
-            int it = 0;
-            const uint32_t b0 = smem_u32(wsm);
-            for (int tile = blockIdx.x; ok && tile < a.ntiles; tile += gridDim.x, ++it) {
-                const int s = it & 1, u = it >> 1;
-                if (!mbar_wait(full + s, u & 1, kWaitBudget)) {
-                    ok = false;
-                    break;
+            ok = tc::mbar_sleep_wait(wbar, 0, kWaitBudget);
+            long long g = 0;                      // input planes consumed = output slots completed
+            const uint64_t b0 = tc::sdesc(smem_u32(wsm), NB * 16, 128);
+            for (int unit = blockIdx.x; ok && unit < a.nunits; unit += gridDim.x) {
+                const int xc = unit % a.nxc;
+                const int len = min(a.xchunk, a.xo - xc * a.xchunk);
+                for (int k = 0; k < len + 2; ++k, ++g) {
+                    const int ps = (int)(g % kSlots);
+                    if (!tc::mbar_sleep_wait(full + ps, (uint32_t)((g / kSlots) & 1), kWaitBudget)) {
+                        ok = false;
+                        break;
+                    }
+                    // the third block writes output slot g+2 first: its previous
+                    // occupant must have been drained and zeroed
+                    const long long w2 = g + 2;
+                    if (w2 >= kRing &&
+                        !tc::mbar_sleep_wait(tempty + (int)(w2 % kRing), (uint32_t)((w2 / kRing - 1) & 1), kWaitBudget)) {
+                        ok = false;
+                        break;
+                    }
+                    tc::fence_after();
+                    const int s0 = (int)(g % kRing);
+                    const int n1 = kRing - s0 < 3 ? kRing - s0 : 3;     // blocks before the ring wraps
+                    const uint32_t d0 = tbase + (uint32_t)(s0 * COUT);
+                    // descriptors advance by (byte offset >> 4) in their 14-bit address field;
+                    // every address stays below 256 KB, so no carry leaves the field
+                    const uint64_t a0 = tc::sdesc(smem_u32(ring + ps * L::SLOT), 3 * kPlaneRow, 128);
+#pragma unroll
+                    for (int t9 = 0; t9 < 9; ++t9) {
+                        const int dy = t9 / 3, dz = t9 % 3;
+#pragma unroll
+                        for (int kc = 0; kc < KC; ++kc) {
+                            const uint64_t ad = a0 + (uint32_t)(((2 * kc * 3 + dy) * kPlaneRow + dz * 16) >> 4);
+                            const uint64_t bd = b0 + (uint32_t)(((t9 * CG + 2 * kc) * NB * 16) >> 4);
+                            if (n1 == 3) {
+                                tc::mma_bf16(d0, ad, bd, ID3, 1u);
+                            } else {
+                                tc::mma_bf16(d0, ad, bd, n1 == 2 ? ID2 : ID1, 1u);
+                                tc::mma_bf16(tbase, ad, bd + (uint32_t)((n1 * COUT * 16) >> 4), n1 == 2 ? ID1 : ID2,
+                                             1u);
+                            }
+                        }
+                    }
+                    tc::commit(empty + ps);               // input plane g is not needed again
+                    tc::commit(tfull + s0);               // output slot g is complete
                 }
-                if (u > 0 && !mbar_wait(tempty + s, (u - 1) & 1, kWaitBudget)) {
+            }
+            tc::commit(drain);
+            ok &= tc::mbar_sleep_wait(drain, 0, kWaitBudget);
+        }
+    } else {
+        long long g = 0;
+        for (int unit = blockIdx.x; ok && unit < a.nunits; unit += gridDim.x) {
+            const int xc = unit % a.nxc, r = unit / a.nxc;
+            const int pt = r % a.tpp, b = r / a.tpp;
+            const int x0 = xc * a.xchunk, len = min(a.xchunk, a.xo - x0);
+            const int p = pt * kM + 32 * q + lane;
+            const int y = p / a.zi, z = p - y * a.zi;
+            const bool valid = y < a.yo && z < a.zo;
+            for (int k = 0; k < len + 2; ++k, ++g) {
+                const int sl = (int)(g % kRing);
+                if (!warp_wait(tfull + sl, (uint32_t)((g / kRing) & 1))) {
                     ok = false;
                     break;
                 }
                 tc::fence_after();
-                const uint32_t d = tbase + (uint32_t)(s * COUT);
-                const uint32_t a0 = smem_u32(stg + s * L::STAGE);
-#pragma unroll 1
-                for (int t = 0; t < 27; ++t) {
-                    const int dx = t / 9, dy = (t / 3) % 3, dz = t % 3;
+                float v[NC], zero[NC];
 #pragma unroll
-                    for (int kc = 0; kc < KC; ++kc) {
-                        const uint32_t aa = a0 + (uint32_t)((2 * kc * 3 + dy) * kBox + (dx * kWz + dz) * 16);
-                        const uint32_t ba = b0 + (uint32_t)((t * CG + 2 * kc) * COUT * 16);
-                        tc::mma_bf16(d, tc::sdesc(aa, 3 * kBox, 128), tc::sdesc(ba, COUT * 16, 128), IDESC,
-                                     (t | kc) != 0);
-                    }
+                for (int c = 0; c < NC; ++c) zero[c] = 0.0f;
+                const uint32_t ta = tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)(sl * COUT + c0);
+                if constexpr (NC == 16) {
+                    tc::tmem_ld16(ta, v);
+                    tc::tmem_wait_ld();
+                    tc::tmem_st16(ta, zero);
+                } else {
+                    tc::tmem_ld8(ta, v);
+                    tc::tmem_wait_ld();
+                    tc::tmem_st8(ta, zero);
                 }
-                tc::commit(empty + s);
-                tc::commit(tfull + s);
-            }
-            tc::commit(drain);
-            ok &= mbar_wait(drain, 0, kWaitBudget);
-        }
-    } else {
-        const int q = warp & 3;
-        int it = 0;
-        for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, ++it) {
-            const int s = it & 1, u = it >> 1;
-            if (!warp_wait(tfull + s, u & 1)) {
-                ok = false;
-                break;
-            }
-            tc::fence_after();
-            float acc[COUT];
-#pragma unroll
-            for (int c = 0; c < COUT; c += 16)
-                tc::tmem_ld16(tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)(s * COUT + c), acc + c);
-            tc::tmem_wait_ld();
-            tc::fence_before();
-            __syncwarp();
-            if (lane == 0) tc::mbar_arrive(tempty + s);
+                tc::tmem_wait_st();
+                tc::fence_before();
+                __syncwarp();
+                if (lane == 0) tc::mbar_arrive(tempty + sl);
+                // slot g holds output plane x0 + k - 2 of this chunk when k >= 2;
+                // the first two slots of a chunk mix planes of two chunks
+                if (k < 2 || !valid) continue;
 
-            const int pt = tile % a.tpp, bx = tile / a.tpp;
-            const int x = bx % a.xo, b = bx / a.xo;
-            const int p = pt * kM + 32 * q + lane;
-            const int y = p / a.zi, z = p - y * a.zi;
-            if (y >= a.yo || z >= a.zo) continue;
-            const long long o =
-                ((((long long)b * a.ox + x + a.off) * a.oy + y + a.off) * a.oz + z + a.off) * COUT;
-            const long long dn = ((((long long)b * a.xo + x) * a.yo + y) * a.zo + z) * COUT;
-            if constexpr (EPI == kEpiGelu) {
+                const int x = x0 + k - 2;
+                constexpr int G = COUT / 8;            // channel groups of the output
+                // blocked offsets of channel group g: ((row + g) * plane + yz) * 8
+                const long long orow = ((long long)b * a.ox + x + a.off) * G + c0 / 8;
+                const long long oplane = (long long)a.oy * a.oz;
+                const long long oyz = (long long)(y + a.off) * a.oz + z + a.off;
+                const long long drow = ((long long)b * a.xo + x) * G + c0 / 8;
+                const long long dplane = (long long)a.yo * a.zo;
+                const long long dyz = (long long)y * a.zo + z;
+                if constexpr (EPI == kEpiGelu) {
 #pragma unroll
-                for (int c = 0; c < COUT; ++c) acc[c] += __ldg(a.bias + c);
-                if (a.out_z) store_bf16(a.out_z + dn, acc, COUT);
+                    for (int c = 0; c < NC; ++c) v[c] += bias[c];
+                    if (a.out_z)
 #pragma unroll
-                for (int c = 0; c < COUT; ++c) acc[c] = gelu(acc[c]);
-                store_bf16(a.out_a + o, acc, COUT);
-            } else if constexpr (EPI == kEpiLinear) {
+                        for (int gg = 0; gg < NC / 8; ++gg)
+                            store_bf16(a.out_z + ((drow + gg) * dplane + dyz) * 8, v + 8 * gg, 8);
 #pragma unroll
-                for (int c = 0; c < COUT; c += 4) {
-                    float4 v = make_float4(acc[c] + __ldg(a.bias + c), acc[c + 1] + __ldg(a.bias + c + 1),
-                                           acc[c + 2] + __ldg(a.bias + c + 2), acc[c + 3] + __ldg(a.bias + c + 3));
-                    *reinterpret_cast<float4 *>(a.out_f + o + c) = v;
+                    for (int c = 0; c < NC; ++c) v[c] = gelu(v[c]);
+#pragma unroll
+                    for (int gg = 0; gg < NC / 8; ++gg)
+                        store_bf16(a.out_a + ((orow + gg) * oplane + oyz) * 8, v + 8 * gg, 8);
+                } else if constexpr (EPI == kEpiLinear) {
+                    float *dst = a.out_f + ((((long long)b * a.ox + x) * a.oy + y) * a.oz + z) * COUT + c0;
+#pragma unroll
+                    for (int c = 0; c < NC; c += 4) {
+                        float4 w = make_float4(v[c] + bias[c], v[c + 1] + bias[c + 1], v[c + 2] + bias[c + 2],
+                                               v[c + 3] + bias[c + 3]);
+                        *reinterpret_cast<float4 *>(dst + c) = w;
+                    }
+                } else {
+                    float zv[NC];
+#pragma unroll
+                    for (int gg = 0; gg < NC / 8; ++gg)
+                        load_bf16(a.zsrc + ((drow + gg) * dplane + dyz) * 8, zv + 8 * gg, 8);
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) v[c] *= gelu_grad(zv[c]);
+#pragma unroll
+                    for (int gg = 0; gg < NC / 8; ++gg)
+                        store_bf16(a.out_a + ((orow + gg) * oplane + oyz) * 8, v + 8 * gg, 8);
                 }
-            } else {
-                float zv[COUT];
-                load_bf16(a.zsrc + dn, zv, COUT);
-#pragma unroll
-                for (int c = 0; c < COUT; ++c) acc[c] *= gelu_grad(zv[c]);
-                store_bf16(a.out_a + o, acc, COUT);
             }
         }
     }
@@ -349,12 +468,15 @@ __global__ void __launch_bounds__(kConvThreads, 1)
                 const int z0 = seg * kM;
                 mbar_expect_tx(full + s, TX);
                 unsigned char *xd = xs + s * L::XSTAGE;
+                // maps: (8 ch, z, y, channel group, x + n * extent_x); the
+                // x + dx planes stay inside this batch entry
                 for (int dx = 0; dx < 3; ++dx)
                     for (int cg = 0; cg < CG; ++cg)
-                        tc::tma_load_5d(xd + (dx * CG + cg) * kBox, &x_map, cg * 8, z0, y, x + dx, b, full + s);
+                        tc::tma_load_5d(xd + (dx * CG + cg) * kBox, &x_map, 0, z0, y, cg, b * (a.xo + 2) + x + dx,
+                                        full + s);
                 unsigned char *gd = gs + s * L::GSTAGE;
                 for (int g = 0; g < GG; ++g)
-                    tc::tma_load_5d(gd + g * kM * 16, &g_map, g * 8, z0 + 2, y + 2, x + 2, b, full + s);
+                    tc::tma_load_5d(gd + g * kM * 16, &g_map, 0, z0 + 2, y + 2, g, b * (a.xo + 4) + x + 2, full + s);
             }
             for (int j = it - 2 < 0 ? 0 : it - 2; j < it; ++j) ok &= mbar_wait(full + (j & 1), (j >> 1) & 1, kWaitBudget);
         }

@@ -6,7 +6,8 @@ reference solver has no learned component, so this oracle restates the
 network the C ABI documents, not a reference file:
 
   4 "valid" 3x3x3 convolutions, channels 16 -> 32 -> 32 -> 32 -> 16 (real
-  channels padded with zeros), GELU(x) = x/2 (1 + erf(x/sqrt 2)) after the
+  channels padded with zeros), GELU(x) = x/2 (1 + tanh(sqrt(2/pi)(x + 0.044715 x^3)))
+  (the tanh form of Hendrycks & Gimpel) after the
   first three, a linear last layer; loss = mean over positions and the first
   `nout` output channels of (out - target)^2.
 
@@ -35,11 +36,14 @@ def bf16(t: torch.Tensor) -> torch.Tensor:
 
 
 def gelu(x):
-    return 0.5 * x * (1.0 + torch.erf(x / math.sqrt(2.0)))
+    t = torch.tanh(math.sqrt(2.0 / math.pi) * (x + 0.044715 * x ** 3))
+    return 0.5 * x * (1.0 + t)
 
 
 def gelu_grad(x):
-    return 0.5 * (1.0 + torch.erf(x / math.sqrt(2.0))) + x * torch.exp(-0.5 * x * x) / math.sqrt(2.0 * math.pi)
+    c0 = math.sqrt(2.0 / math.pi)
+    t = torch.tanh(c0 * (x + 0.044715 * x ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * x * (1.0 - t * t) * c0 * (1.0 + 3.0 * 0.044715 * x * x)
 
 
 def pad_params(params, inputs, outputs):
