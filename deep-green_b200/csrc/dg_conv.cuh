@@ -1,10 +1,7 @@
 // dg_conv.cuh -- BF16 3x3x3 convolution kernels of the correction network on
 // the 5th-generation tensor cores (tcgen05, FP32 accumulation in TMEM).
 //
-// Activations are BF16 in a channel-blocked layout, [n][x][C/8][y][z][8]:
-// for each x-plane and group of 8 channels, the (y, z) plane is contiguous
-// with 16 bytes per cell, so every TMA box below reads 16-byte rows that
-// are contiguous in memory.  Every
+// Activations are BF16 channels-last, [n][x][y][z][C], z fastest.  Every
 // convolution is "valid": an input of extents (X, Y, Z) gives an output of
 // (X-2, Y-2, Z-2), out[v] = sum_t W_t in[v + t], t = (dx, dy, dz) in 0..2,
 // weights W[co][ci][dx][dy][dz] (the layout of torch.nn.Conv3d on tensors
@@ -15,11 +12,12 @@
 //   * positions are enumerated along the flattened (y, z) index of the INPUT,
 //     p = y * Zin + z, within one (n, x) plane; tap (dx, dy, dz) is then the
 //     plane x+dx shifted by dy*Zin + dz.  A tile of 128 consecutive p needs,
-//     per channel group of 8 and per dy, a window of 136 positions of an
-//     input plane, stored [p][8 ch]: 8 positions x 16 bytes = one K-major
-//     core matrix, so each (dy, dz) is a window at a different start
-//     address.  Positions with z >= Zin-2 wrap into the next row and are
-//     dropped by the epilogue (2 of every Zin positions).
+//     per dy, a window of 136 positions of an input plane: one TMA box of
+//     rows of CIN channels (64 or 32 bytes), written with the hardware's 64-
+//     or 32-byte swizzle, which is the canonical swizzled K-major operand
+//     layout of the tensor cores; each (dy, dz) is that window at a start
+//     address dz rows further.  Positions with z >= Zin-2 wrap into the next
+//     row and are dropped by the epilogue (2 of every Zin positions).
 //   * a block walks along x through a column of tiles (fixed n and p range,
 //     x in a chunk).  Input plane P serves output planes P, P-1 and P-2 (taps
 //     dx = 0, 1, 2), so each (dy, dz, 16 channels) is ONE MMA with N = 3 COUT
@@ -29,19 +27,20 @@
 //     ring is split in two).  Output plane P-2 is then complete; the epilogue
 //     drains its slot and zeroes it for reuse, so every MMA accumulates.
 //     Each input plane is read from shared memory once, by 9 x CIN/16 MMAs.
-//   * input planes arrive by TMA into a ring of shared-memory slots: 3 x
-//     CIN/8 boxes of 136 positions, read as 68 pairs of positions so every
-//     box row is one 32-byte sector.  Planes at the start of a chunk produce
-//     two partial outputs that are drained and discarded.
-//   * all weights stay in shared memory (K-major, packed on the host as
-//     [dy, dz][ci/8][dx' = 2-dx][co][8]).
-//   * warp 0 issues the TMA copies, warp 1 owns TMEM and issues the MMAs
-//     (one thread, descriptors advanced by constant offsets), warps 2-9
-//     drain the accumulators (two warps per TMEM sub-partition, each half
-//     of the columns: bias, GELU / GELU', BF16 or FP32 stores).
+//   * input planes arrive by TMA into a ring of shared-memory slots (3
+//     windows each); planes at the start of a chunk produce two partial
+//     outputs that are drained and discarded.
+//   * all weights stay in shared memory, packed on the host as
+//     [dy, dz][dx' = 2-dx][co][ci] rows, swizzled like the windows.
+//   * warp 0 issues the TMA copies; warps 1 and 2 each issue half of every
+//     plane's MMAs (one thread each, descriptors advanced by constant
+//     offsets) into their own ring of accumulators -- a single thread's
+//     dependent issue loop, not the tensor core, would otherwise set the
+//     pace; warps 3-10 drain both rings (two warps per TMEM sub-partition,
+//     each half of the columns: sum, bias, GELU / GELU', BF16 or FP32
+//     stores) in a fixed order, so results do not depend on timing.
 //   The input-gradient of a layer is the same kernel run on the output
 //   gradient zero-padded by 2 with the taps flipped and W transposed.
-//   Input z extents must be even (pairs of positions).
 //
 // Weight-gradient kernel: dW_t[co][ci] = sum_v dZ[v][co] X[v+t][ci] over
 // all output positions v.  D[M=128, N=COUT] per (dy, dz) pair, 9 TMEM
@@ -66,18 +65,16 @@ constexpr int kWz = 136;                   // window positions per row (>= kM + 
 constexpr int kBox = 3 * kWz * 16;         // one TMA box: 3 rows of kWz positions x 8 channels (6528 B)
 constexpr int kStages = 2;
 constexpr int kConvThreads = 192;          // weight gradient: 6 warps (TMA, MMA, 4 x epilogue)
-constexpr int kFwdThreads = 320;           // forward: 10 warps (TMA, MMA, 8 x epilogue)
+constexpr int kIssuers = 2;                // forward: MMA-issuing warps, each with its own accumulators
+constexpr int kFwdThreads = 32 * (1 + kIssuers + 8);   // forward: TMA, issuers, 8 x epilogue
 constexpr int kRing = 8;                   // TMEM accumulator slots (output planes) of the forward kernel
-constexpr int kPlaneRow = kWz * 16;        // one (channel group, dy) window of one x-plane (2176 B)
 constexpr int kSlots = 4;                  // input-plane slots of the forward kernel's shared-memory ring
 constexpr unsigned kNetTimeout = 0x2u;     // status bit: a wait ran out
 
 enum Epilogue : int { kEpiGelu = 0, kEpiLinear = 1, kEpiDGelu = 2 };
 
-// Output tensors: BF16 ones are channel-blocked like the inputs, the FP32
-// output of the linear layer is channels-last [n][x][y][z][COUT].
 struct ConvArgs {
-    int nb, xi, yi, zi;             // input extents (zi even)
+    int nb, xi, yi, zi;             // input extents
     int xo, yo, zo;                 // output extents (input - 2)
     int tpp;                        // tiles per (n, x) plane: ceil(yo * zi / kM)
     int xchunk;                     // planes of x per work unit
@@ -103,6 +100,11 @@ struct WgradArgs {
 __device__ __forceinline__ unsigned char *align128(unsigned char *p) {
     const uint32_t s = smem_u32(p);
     return p + ((128u - (s & 127u)) & 127u);
+}
+
+__device__ __forceinline__ unsigned char *align1024(unsigned char *p) {
+    const uint32_t s = smem_u32(p);
+    return p + ((1024u - (s & 1023u)) & 1023u);
 }
 
 // GELU in its tanh form, x/2 (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3)))
@@ -161,46 +163,51 @@ __device__ __forceinline__ void load_bf16(const __nv_bfloat16 *src, float *v, in
 
 template <int CIN, int COUT>
 struct ConvSmem {
-    static constexpr int CG = CIN / 8;
-    static constexpr int WB = 27 * CG * COUT * 16;           // weights
-    static constexpr int SLOT = CG * 3 * kPlaneRow;          // windows of one x-plane: [cg][dy][kWz][8]
-    static constexpr int BYTES = WB + kSlots * SLOT + 512 /*barriers*/ + 128 /*alignment*/;
+    static constexpr int ROW = CIN * 2;                       // bytes of one position (swizzle width)
+    static constexpr int WB = 27 * COUT * ROW;                // weights
+    static constexpr int WIN = (kWz * ROW + 1023) / 1024 * 1024;   // one window, 1024-byte aligned
+    static constexpr int SLOT = 3 * WIN;                      // the dy windows of one x-plane
+    static constexpr int BYTES = WB + kSlots * SLOT + 512 /*barriers*/ + 1024 /*alignment*/;
 };
 
 template <int CIN, int COUT, int EPI>
 __global__ void __launch_bounds__(kFwdThreads, 1)
     conv_fwd_kernel(const __grid_constant__ CUtensorMap in_map, const __nv_bfloat16 *__restrict__ wpack, ConvArgs a) {
-    static_assert(CIN % 16 == 0 && (COUT == 16 || COUT == 32), "unsupported channel counts");
+    static_assert((CIN == 16 || CIN == 32) && (COUT == 16 || COUT == 32), "unsupported channel counts");
+    static_assert(kIssuers == 2, "the MMA split below is written for two issuers");
     using L = ConvSmem<CIN, COUT>;
-    constexpr int CG = L::CG, KC = CIN / 16;
+    constexpr int KC = CIN / 16;
+    constexpr int ROW = L::ROW;
     constexpr int NC = COUT / 2;                 // columns per epilogue warp
     constexpr int NB = 3 * COUT;                 // rows of the weight operand (three dx blocks)
-    constexpr uint32_t TCOLS = kRing * COUT;     // 256 or 128
+    constexpr int RING = kRing * COUT;           // TMEM columns of one issuer's ring
+    constexpr uint32_t TCOLS = kIssuers * RING;  // 512 or 256
     constexpr uint32_t ID3 = tc::idesc_bf16(kM, 3 * COUT, 0, 0);
     constexpr uint32_t ID2 = tc::idesc_bf16(kM, 2 * COUT, 0, 0);
     constexpr uint32_t ID1 = tc::idesc_bf16(kM, COUT, 0, 0);
+    constexpr int EPI0 = 1 + kIssuers;           // first epilogue warp
 
     extern __shared__ unsigned char smem_raw[];
-    unsigned char *smem = align128(smem_raw);
+    unsigned char *smem = align1024(smem_raw);   // swizzle patterns follow address bits
     unsigned char *wsm = smem;
     unsigned char *ring = smem + L::WB;
     uint64_t *bars = reinterpret_cast<uint64_t *>(ring + kSlots * L::SLOT);
     uint64_t *full = bars, *empty = bars + kSlots, *tfull = bars + 2 * kSlots, *tempty = tfull + kRing,
              *wbar = tempty + kRing, *drain = wbar + 1;
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(drain + 1);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(drain + kIssuers);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
         for (int i = 0; i < kSlots; ++i) {
             mbar_init(full + i, 1);
-            mbar_init(empty + i, 1);
+            mbar_init(empty + i, kIssuers);
         }
         for (int i = 0; i < kRing; ++i) {
-            mbar_init(tfull + i, 1);
+            mbar_init(tfull + i, kIssuers);
             mbar_init(tempty + i, 8);
         }
         mbar_init(wbar, 1);
-        mbar_init(drain, 1);
+        for (int i = 0; i < kIssuers; ++i) mbar_init(drain + i, 1);
         fence_mbar_init();
     }
     if (warp == 1) tc::tmem_alloc(tslot, TCOLS);
@@ -209,13 +216,13 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
     tc::fence_after();
     const uint32_t tbase = *tslot;
     const int q = warp & 3;                      // epilogue: TMEM sub-partition (lanes 32q..32q+31)
-    const int c0 = ((warp - 2) >> 2) * NC;       // epilogue: first column of this warp's half
-    if (warp >= 2) {
+    const int c0 = ((warp - EPI0) >> 2) * NC;    // epilogue: first column of this warp's half
+    if (warp >= EPI0) {
         // every accumulator starts at zero: all MMAs accumulate
         float zero[NC];
 #pragma unroll
         for (int c = 0; c < NC; ++c) zero[c] = 0.0f;
-        for (int sl = 0; sl < kRing; ++sl) {
+        for (int sl = 0; sl < kIssuers * kRing; ++sl) {
             const uint32_t ta = tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)(sl * COUT + c0);
             if constexpr (NC == 16) tc::tmem_st16(ta, zero);
             else tc::tmem_st8(ta, zero);
@@ -228,7 +235,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
     bool ok = true;
     float bias[NC];                              // epilogue: this warp's bias columns
 #pragma unroll
-    for (int c = 0; c < NC; ++c) bias[c] = (EPI != kEpiDGelu && warp >= 2) ? __ldg(a.bias + c0 + c) : 0.0f;
+    for (int c = 0; c < NC; ++c) bias[c] = (EPI != kEpiDGelu && warp >= EPI0) ? __ldg(a.bias + c0 + c) : 0.0f;
 
     if (warp == 0) {
         if (lane == 0) {
@@ -239,7 +246,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
                 const int xc = unit % a.nxc, r = unit / a.nxc;
                 const int pt = r % a.tpp, b = r / a.tpp;
                 const int x0 = xc * a.xchunk, len = min(a.xchunk, a.xo - x0);
-                const int pair0 = pt * (kM / 2);
+                const int p0 = pt * kM;
                 for (int k = 0; k < len + 2; ++k, ++g) {
                     const int slot = (int)(g % kSlots);
                     const long long use = g / kSlots;
@@ -247,12 +254,10 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
                         ok = false;
                         break;
                     }
-                    mbar_expect_tx(full + slot, L::SLOT);
+                    mbar_expect_tx(full + slot, 3 * kWz * ROW);
                     unsigned char *dst = ring + slot * L::SLOT;
-                    for (int cg = 0; cg < CG; ++cg)
-                        for (int dy = 0; dy < 3; ++dy)
-                            tc::tma_load_5d(dst + (cg * 3 + dy) * kPlaneRow, &in_map, 0, pair0 + dy * (a.zi / 2), cg,
-                                            x0 + k, b, full + slot);
+                    for (int dy = 0; dy < 3; ++dy)
+                        tma_load_4d(dst + dy * L::WIN, &in_map, 0, p0 + dy * a.zi, x0 + k, b, full + slot);
                 }
             }
             // copies still in flight must land before the block exits
@@ -260,11 +265,13 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
                 ok &= tc::mbar_sleep_wait(full + (int)(j % kSlots), (uint32_t)((j / kSlots) & 1), kWaitBudget);
             ok &= tc::mbar_sleep_wait(wbar, 0, kWaitBudget);
         }
-    } else if (warp == 1) {
+    } else if (warp <= kIssuers) {
         if (lane == 0) {
+            const int me = warp - 1;              // issuer index: its half of the MMAs, its ring
             ok = tc::mbar_sleep_wait(wbar, 0, kWaitBudget);
             long long g = 0;                      // input planes consumed = output slots completed
-            const uint64_t b0 = tc::sdesc(smem_u32(wsm), NB * 16, 128);
+            const uint64_t b0 = tc::sdesc_sw(smem_u32(wsm), ROW);
+            const uint32_t rbase = tbase + (uint32_t)(me * RING);
             for (int unit = blockIdx.x; ok && unit < a.nunits; unit += gridDim.x) {
                 const int xc = unit % a.nxc;
                 const int len = min(a.xchunk, a.xo - xc * a.xchunk);
@@ -277,40 +284,54 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
                     // the third block writes output slot g+2 first: its previous
                     // occupant must have been drained and zeroed
                     const long long w2 = g + 2;
-                    if (w2 >= kRing &&
-                        !tc::mbar_sleep_wait(tempty + (int)(w2 % kRing), (uint32_t)((w2 / kRing - 1) & 1), kWaitBudget)) {
+                    if (w2 >= kRing && !tc::mbar_sleep_wait(tempty + (int)(w2 % kRing),
+                                                            (uint32_t)((w2 / kRing - 1) & 1), kWaitBudget)) {
                         ok = false;
                         break;
                     }
                     tc::fence_after();
                     const int s0 = (int)(g % kRing);
-                    const int n1 = kRing - s0 < 3 ? kRing - s0 : 3;     // blocks before the ring wraps
-                    const uint32_t d0 = tbase + (uint32_t)(s0 * COUT);
+                    const uint32_t d0 = rbase + (uint32_t)(s0 * COUT);
                     // descriptors advance by (byte offset >> 4) in their 14-bit address field;
                     // every address stays below 256 KB, so no carry leaves the field
-                    const uint64_t a0 = tc::sdesc(smem_u32(ring + ps * L::SLOT), 3 * kPlaneRow, 128);
+                    const uint64_t a0 = tc::sdesc_sw(smem_u32(ring + ps * L::SLOT), ROW);
+                    // this issuer's MMAs: channel half kc = me (CIN 32) or taps 0-4 / 5-8 (CIN 16)
+                    constexpr int T9N = KC == 2 ? 9 : 5;
+                    const int t9lo = KC == 2 ? 0 : me * 5;
+                    const int t9hi = KC == 2 ? 9 : (me ? 9 : 5);
+                    const int kc = KC == 2 ? me : 0;
+                    if (s0 <= kRing - 3) {
 #pragma unroll
-                    for (int t9 = 0; t9 < 9; ++t9) {
-                        const int dy = t9 / 3, dz = t9 % 3;
+                        for (int j = 0; j < T9N; ++j) {
+                            const int t9 = t9lo + j;
+                            if (t9 >= t9hi) break;
+                            const int dy = t9 / 3, dz = t9 % 3;
+                            const uint64_t ad = a0 + (uint32_t)((dy * L::WIN + dz * ROW + kc * 32) >> 4);
+                            const uint64_t bd = b0 + (uint32_t)((t9 * NB * ROW + kc * 32) >> 4);
+                            tc::mma_bf16(d0, ad, bd, ID3, 1u);
+                        }
+                    } else {
+                        // the three blocks would wrap the ring: two MMAs each
+                        const int n1 = kRing - s0;
+                        const uint32_t i1 = n1 == 2 ? ID2 : ID1, i2 = n1 == 2 ? ID1 : ID2;
+                        const uint32_t bo2 = (uint32_t)((n1 * COUT * ROW) >> 4);
 #pragma unroll
-                        for (int kc = 0; kc < KC; ++kc) {
-                            const uint64_t ad = a0 + (uint32_t)(((2 * kc * 3 + dy) * kPlaneRow + dz * 16) >> 4);
-                            const uint64_t bd = b0 + (uint32_t)(((t9 * CG + 2 * kc) * NB * 16) >> 4);
-                            if (n1 == 3) {
-                                tc::mma_bf16(d0, ad, bd, ID3, 1u);
-                            } else {
-                                tc::mma_bf16(d0, ad, bd, n1 == 2 ? ID2 : ID1, 1u);
-                                tc::mma_bf16(tbase, ad, bd + (uint32_t)((n1 * COUT * 16) >> 4), n1 == 2 ? ID1 : ID2,
-                                             1u);
-                            }
+                        for (int j = 0; j < T9N; ++j) {
+                            const int t9 = t9lo + j;
+                            if (t9 >= t9hi) break;
+                            const int dy = t9 / 3, dz = t9 % 3;
+                            const uint64_t ad = a0 + (uint32_t)((dy * L::WIN + dz * ROW + kc * 32) >> 4);
+                            const uint64_t bd = b0 + (uint32_t)((t9 * NB * ROW + kc * 32) >> 4);
+                            tc::mma_bf16(d0, ad, bd, i1, 1u);
+                            tc::mma_bf16(rbase, ad, bd + bo2, i2, 1u);
                         }
                     }
                     tc::commit(empty + ps);               // input plane g is not needed again
                     tc::commit(tfull + s0);               // output slot g is complete
                 }
             }
-            tc::commit(drain);
-            ok &= tc::mbar_sleep_wait(drain, 0, kWaitBudget);
+            tc::commit(drain + me);
+            ok &= tc::mbar_sleep_wait(drain + me, 0, kWaitBudget);
         }
     } else {
         long long g = 0;
@@ -328,18 +349,22 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
                     break;
                 }
                 tc::fence_after();
-                float v[NC], zero[NC];
+                float v[NC], v2[NC], zero[NC];
 #pragma unroll
                 for (int c = 0; c < NC; ++c) zero[c] = 0.0f;
                 const uint32_t ta = tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)(sl * COUT + c0);
                 if constexpr (NC == 16) {
                     tc::tmem_ld16(ta, v);
+                    tc::tmem_ld16(ta + RING, v2);
                     tc::tmem_wait_ld();
                     tc::tmem_st16(ta, zero);
+                    tc::tmem_st16(ta + RING, zero);
                 } else {
                     tc::tmem_ld8(ta, v);
+                    tc::tmem_ld8(ta + RING, v2);
                     tc::tmem_wait_ld();
                     tc::tmem_st8(ta, zero);
+                    tc::tmem_st8(ta + RING, zero);
                 }
                 tc::tmem_wait_st();
                 tc::fence_before();
@@ -348,46 +373,32 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
                 // slot g holds output plane x0 + k - 2 of this chunk when k >= 2;
                 // the first two slots of a chunk mix planes of two chunks
                 if (k < 2 || !valid) continue;
+#pragma unroll
+                for (int c = 0; c < NC; ++c) v[c] += v2[c];
 
                 const int x = x0 + k - 2;
-                constexpr int G = COUT / 8;            // channel groups of the output
-                // blocked offsets of channel group g: ((row + g) * plane + yz) * 8
-                const long long orow = ((long long)b * a.ox + x + a.off) * G + c0 / 8;
-                const long long oplane = (long long)a.oy * a.oz;
-                const long long oyz = (long long)(y + a.off) * a.oz + z + a.off;
-                const long long drow = ((long long)b * a.xo + x) * G + c0 / 8;
-                const long long dplane = (long long)a.yo * a.zo;
-                const long long dyz = (long long)y * a.zo + z;
+                const long long o =
+                    ((((long long)b * a.ox + x + a.off) * a.oy + y + a.off) * a.oz + z + a.off) * COUT + c0;
+                const long long dn = ((((long long)b * a.xo + x) * a.yo + y) * a.zo + z) * COUT + c0;
                 if constexpr (EPI == kEpiGelu) {
 #pragma unroll
                     for (int c = 0; c < NC; ++c) v[c] += bias[c];
-                    if (a.out_z)
-#pragma unroll
-                        for (int gg = 0; gg < NC / 8; ++gg)
-                            store_bf16(a.out_z + ((drow + gg) * dplane + dyz) * 8, v + 8 * gg, 8);
+                    if (a.out_z) store_bf16(a.out_z + dn, v, NC);
 #pragma unroll
                     for (int c = 0; c < NC; ++c) v[c] = gelu(v[c]);
-#pragma unroll
-                    for (int gg = 0; gg < NC / 8; ++gg)
-                        store_bf16(a.out_a + ((orow + gg) * oplane + oyz) * 8, v + 8 * gg, 8);
+                    store_bf16(a.out_a + o, v, NC);
                 } else if constexpr (EPI == kEpiLinear) {
-                    float *dst = a.out_f + ((((long long)b * a.ox + x) * a.oy + y) * a.oz + z) * COUT + c0;
 #pragma unroll
-                    for (int c = 0; c < NC; c += 4) {
-                        float4 w = make_float4(v[c] + bias[c], v[c + 1] + bias[c + 1], v[c + 2] + bias[c + 2],
-                                               v[c + 3] + bias[c + 3]);
-                        *reinterpret_cast<float4 *>(dst + c) = w;
-                    }
+                    for (int c = 0; c < NC; c += 4)
+                        *reinterpret_cast<float4 *>(a.out_f + o + c) =
+                            make_float4(v[c] + bias[c], v[c + 1] + bias[c + 1], v[c + 2] + bias[c + 2],
+                                        v[c + 3] + bias[c + 3]);
                 } else {
                     float zv[NC];
-#pragma unroll
-                    for (int gg = 0; gg < NC / 8; ++gg)
-                        load_bf16(a.zsrc + ((drow + gg) * dplane + dyz) * 8, zv + 8 * gg, 8);
+                    load_bf16(a.zsrc + dn, zv, NC);
 #pragma unroll
                     for (int c = 0; c < NC; ++c) v[c] *= gelu_grad(zv[c]);
-#pragma unroll
-                    for (int gg = 0; gg < NC / 8; ++gg)
-                        store_bf16(a.out_a + ((orow + gg) * oplane + oyz) * 8, v + 8 * gg, 8);
+                    store_bf16(a.out_a + o, v, NC);
                 }
             }
         }
@@ -468,15 +479,15 @@ __global__ void __launch_bounds__(kConvThreads, 1)
                 const int z0 = seg * kM;
                 mbar_expect_tx(full + s, TX);
                 unsigned char *xd = xs + s * L::XSTAGE;
-                // maps: (8 ch, z, y, channel group, x + n * extent_x); the
+                // maps: (C, z, y, x + n * extent_x), boxes of 8 channels; the
                 // x + dx planes stay inside this batch entry
                 for (int dx = 0; dx < 3; ++dx)
                     for (int cg = 0; cg < CG; ++cg)
-                        tc::tma_load_5d(xd + (dx * CG + cg) * kBox, &x_map, 0, z0, y, cg, b * (a.xo + 2) + x + dx,
-                                        full + s);
+                        tma_load_4d(xd + (dx * CG + cg) * kBox, &x_map, cg * 8, z0, y, b * (a.xo + 2) + x + dx,
+                                    full + s);
                 unsigned char *gd = gs + s * L::GSTAGE;
                 for (int g = 0; g < GG; ++g)
-                    tc::tma_load_5d(gd + g * kM * 16, &g_map, 0, z0 + 2, y + 2, g, b * (a.xo + 4) + x + 2, full + s);
+                    tma_load_4d(gd + g * kM * 16, &g_map, g * 8, z0 + 2, y + 2, b * (a.xo + 4) + x + 2, full + s);
             }
             for (int j = it - 2 < 0 ? 0 : it - 2; j < it; ++j) ok &= mbar_wait(full + (j & 1), (j >> 1) & 1, kWaitBudget);
         }

@@ -106,11 +106,9 @@ __global__ void features_kernel(View b, View a, NormDev nm, float inv_vol, float
                                                      (f[c + 1] - nm.in_mean[c + 1]) * nm.in_inv_std[c + 1]);
             u[c >> 1] = *reinterpret_cast<uint32_t *>(&h);
         }
-        // channel-blocked [x][2][y][z][8]
-        const long long plane = (long long)ext * ext;
-        const long long yz = (long long)cy * ext + cz;
-        reinterpret_cast<uint4 *>(out)[((long long)cx * 2 + 0) * plane + yz] = w[0];
-        reinterpret_cast<uint4 *>(out)[((long long)cx * 2 + 1) * plane + yz] = w[1];
+        uint4 *dst = reinterpret_cast<uint4 *>(out + v * 16);
+        dst[0] = w[0];
+        dst[1] = w[1];
     }
 }
 

@@ -87,34 +87,34 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
-// Channel-blocked BF16 tensors [n][x][c/8][y][z][8] seen by TMA.
-// Forward / input-gradient operand: 5-D view (16 = 2 positions x 8 ch,
-// y*z/2 position pairs, c/8, x, n), box (16, kWz/2, 1, 1, 1): one window of
-// one x-plane, rows of 32 bytes (one sector each).  Needs z even.
+// Channels-last BF16 tensors [n][x][y][z][c] seen by TMA.
+// Forward / input-gradient operand: 4-D view (c, y*z, x, n), box (c, kWz,
+// 1, 1) -- one window of one x-plane -- written with the 64-byte (c = 32)
+// or 32-byte (c = 16) swizzle the tensor cores read.
 bool map_conv_input(CUtensorMap *m, const void *base, int c, int n, int x, int y, int z) {
     auto fn = encode_fn();
     if (!fn) return false;
-    const cuuint64_t plane = (cuuint64_t)y * z * 16, g = (cuuint64_t)(c / 8);
-    cuuint64_t dims[5] = {16, (cuuint64_t)y * z / 2, g, (cuuint64_t)x, (cuuint64_t)n};
-    cuuint64_t strides[4] = {32, plane, g * plane, (cuuint64_t)x * g * plane};
-    cuuint32_t box[5] = {16, (cuuint32_t)(kWz / 2), 1, 1, 1};
-    cuuint32_t estr[5] = {1, 1, 1, 1, 1};
-    return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void *>(base), dims, strides, box, estr,
-              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+    const cuuint64_t e = 2;
+    cuuint64_t dims[4] = {(cuuint64_t)c, (cuuint64_t)y * z, (cuuint64_t)x, (cuuint64_t)n};
+    cuuint64_t strides[3] = {c * e, (cuuint64_t)y * z * c * e, (cuuint64_t)x * y * z * c * e};
+    cuuint32_t box[4] = {(cuuint32_t)c, (cuuint32_t)kWz, 1, 1};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void *>(base), dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, c == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// Weight-gradient operands: 5-D view (8 ch, z, y, c/8, x + n * x_extent),
-// box (8, bz, by, 1, 1).
-bool map_5d(CUtensorMap *m, const void *base, int c, int n, int x, int y, int z, int bz, int by) {
+// Weight-gradient operands: 4-D view (c, z, y, x + n * x_extent), box (8,
+// bz, by, 1): 8 channels of each position, no swizzle.
+bool map_wgrad(CUtensorMap *m, const void *base, int c, int n, int x, int y, int z, int bz, int by) {
     auto fn = encode_fn();
     if (!fn) return false;
-    const cuuint64_t row = 16, g = (cuuint64_t)(c / 8);
-    cuuint64_t dims[5] = {8, (cuuint64_t)z, (cuuint64_t)y, g, (cuuint64_t)x * n};
-    cuuint64_t strides[4] = {row, (cuuint64_t)z * row, (cuuint64_t)y * z * row, g * y * z * row};
-    cuuint32_t box[5] = {8, (cuuint32_t)bz, (cuuint32_t)by, 1, 1};
-    cuuint32_t estr[5] = {1, 1, 1, 1, 1};
-    return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void *>(base), dims, strides, box, estr,
+    const cuuint64_t e = 2;
+    cuuint64_t dims[4] = {(cuuint64_t)c, (cuuint64_t)z, (cuuint64_t)y, (cuuint64_t)x * n};
+    cuuint64_t strides[3] = {c * e, (cuuint64_t)z * c * e, (cuuint64_t)y * z * c * e};
+    cuuint32_t box[4] = {8, (cuuint32_t)bz, (cuuint32_t)by, 1};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void *>(base), dims, strides, box, estr,
               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
@@ -123,24 +123,25 @@ bool map_5d(CUtensorMap *m, const void *base, int c, int n, int x, int y, int z,
 // Element-wise kernels
 // ---------------------------------------------------------------------------
 
-// Weight operand of the forward kernel: [dy, dz][ci/8][dx' = 2 - dx][co][8]
-// of a convolution W[co][ci][tap] (tap = 9 dx + 3 dy + dz); `flip` packs
-// the input-gradient convolution instead, with cin' = cout, cout' = cin and
-// W'_t[co'][ci'] = W_{26-t}[ci'][co'] (taps flipped, channels transposed).
+// Weight operand of the forward kernel: rows r = ((dy, dz), dx' = 2 - dx, co)
+// of kin channels (2 kin bytes), in the tensor cores' swizzled K-major layout:
+// the 16-byte chunk c of row r is stored at chunk c ^ ((r * row >> 7) &
+// (row/16 - 1)) (the shared-memory copy starts 1024-byte aligned).  `flip`
+// packs the input-gradient convolution instead, with cin' = cout, cout' =
+// cin and W'_t[co'][ci'] = W_{26-t}[ci'][co'] (taps flipped, channels
+// transposed).
 __global__ void pack_kernel(const float *__restrict__ w, __nv_bfloat16 *__restrict__ out, int cin, int cout,
                             int flip) {
     const int kin = flip ? cout : cin, kout = flip ? cin : cout;   // channels of the packed convolution
+    const int row = 2 * kin;
     const int total = 27 * kin * kout;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
-        const int e = i & 7;
-        int r = i >> 3;
-        const int n = r % (3 * kout);
-        r /= 3 * kout;
-        const int cg = r % (kin / 8);
-        const int t9 = r / (kin / 8);
+        const int r = i / kin, pos = i % kin;
+        const int mask = ((r * row) >> 7) & (row / 16 - 1);
+        const int ci = (((pos >> 3) ^ mask) << 3) | (pos & 7);     // logical channel stored here
+        const int n = r % (3 * kout), t9 = r / (3 * kout);
         const int dx = 2 - n / kout, co = n % kout;
         const int t = dx * 9 + t9;
-        const int ci = cg * 8 + e;
         const float v = flip ? w[((size_t)ci * cin + co) * 27 + (26 - t)] : w[((size_t)co * cin + ci) * 27 + t];
         out[i] = __float2bfloat16_rn(v);
     }
@@ -181,12 +182,8 @@ __global__ void loss_kernel(const float *__restrict__ out, const float *__restri
             acc += (double)d * d;
             g[c] = scale * d;
         }
-        // channel-blocked, padded by 2: [n][x+4][2][y+4][z+4][8]
-        const long long plane = (long long)(y + 4) * (z + 4);
-        const long long yz = (long long)(iy + 2) * (z + 4) + iz + 2;
-        const long long row = ((long long)b * (x + 4) + ix + 2) * (kIO / 8);
-#pragma unroll
-        for (int q = 0; q < kIO / 8; ++q) store_bf16(dz + ((row + q) * plane + yz) * 8, g + 8 * q, 8);
+        const long long o = ((((long long)b * (x + 4) + ix + 2) * (y + 4) + iy + 2) * (z + 4) + iz + 2) * kIO;
+        store_bf16(dz + o, g, kIO);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -212,12 +209,10 @@ __global__ void adam_kernel(float *__restrict__ p, const float *__restrict__ g, 
     }
 }
 
-// Channels-last dense copy [n][x][y][z][c] of a channel-blocked BF16 tensor
-// whose region of extents (x, y, z) sits at offset `pad` (test access).
-__global__ void unblock_kernel(const __nv_bfloat16 *__restrict__ src, __nv_bfloat16 *__restrict__ dst, int n, int x,
-                               int y, int z, int c, int pad) {
+// Unpadded copy of the interior of a BF16 tensor padded by 2 (test access).
+__global__ void unpad_kernel(const __nv_bfloat16 *__restrict__ src, __nv_bfloat16 *__restrict__ dst, int n, int x,
+                             int y, int z, int c) {
     const long long total = (long long)n * x * y * z * c;
-    const int X = x + 2 * pad, Y = y + 2 * pad, Z = z + 2 * pad;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
          i += (long long)gridDim.x * blockDim.x) {
         long long r = i;
@@ -226,8 +221,7 @@ __global__ void unblock_kernel(const __nv_bfloat16 *__restrict__ src, __nv_bfloa
         const int iy = r % y; r /= y;
         const int ix = r % x;
         const int b = (int)(r / x);
-        dst[i] = src[((((long long)b * X + ix + pad) * (c / 8) + ic / 8) * Y + iy + pad) * Z * 8 +
-                     (long long)(iz + pad) * 8 + (ic & 7)];
+        dst[i] = src[((((long long)b * (x + 4) + ix + 2) * (y + 4) + iy + 2) * (z + 4) + iz + 2) * c + ic];
     }
 }
 
@@ -248,14 +242,15 @@ cudaError_t launch_conv(dg_net *net, const void *in, int nb, int xi, int yi, int
             attr_err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kFwdThreads, L::BYTES);
     });
     if (attr_err != cudaSuccess) return attr_err;
-    if (zi & 1) return cudaErrorInvalidValue;   // windows are read as pairs of positions
     CUtensorMap m;
     if (!map_conv_input(&m, in, CIN, nb, xi, yi, zi)) return cudaErrorInvalidValue;
     a.nb = nb;
     a.xi = xi; a.yi = yi; a.zi = zi;
     a.xo = xi - 2; a.yo = yi - 2; a.zo = zi - 2;
     a.tpp = (a.yo * zi + kM - 1) / kM;
-    const int slots = std::max(1, occ) * net->nsm;
+    // blocks holding all 512 TMEM columns cannot share an SM
+    const int per_sm = kIssuers * kRing * COUT > 256 ? 1 : std::max(1, occ);
+    const int slots = per_sm * net->nsm;
     // longest x chunk (fewest re-loaded planes) that still gives every block
     // a few work units
     a.xchunk = 8;
@@ -286,8 +281,8 @@ cudaError_t launch_wgrad(dg_net *net, const void *x_in, const void *g_pad, int n
     });
     if (attr_err != cudaSuccess) return attr_err;
     CUtensorMap mx, mg;
-    if (!map_5d(&mx, x_in, CIN, nb, xo + 2, yo + 2, zo + 2, kWz, 3)) return cudaErrorInvalidValue;
-    if (!map_5d(&mg, g_pad, COUT, nb, xo + 4, yo + 4, zo + 4, kM, 1)) return cudaErrorInvalidValue;
+    if (!map_wgrad(&mx, x_in, CIN, nb, xo + 2, yo + 2, zo + 2, kWz, 3)) return cudaErrorInvalidValue;
+    if (!map_wgrad(&mg, g_pad, COUT, nb, xo + 4, yo + 4, zo + 4, kM, 1)) return cudaErrorInvalidValue;
     WgradArgs a;
     a.nb = nb; a.xo = xo; a.yo = yo; a.zo = zo;
     a.nseg = (zo + kM - 1) / kM;
@@ -373,9 +368,8 @@ uint64_t splitmix(uint64_t &s) {
 }
 
 int check_extents(dg_net *net, int n, int x, int y, int z) {
-    if (n < 1 || x < 9 || y < 9 || z < 10)
-        return fail(net, DG_ERR_INVALID, "input extents must be at least 9 per axis (z 10) and n >= 1");
-    if (z & 1) return fail(net, DG_ERR_INVALID, "the z extent must be even");
+    if (n < 1 || x < 9 || y < 9 || z < 9)
+        return fail(net, DG_ERR_INVALID, "input extents must be at least 9 per axis and n >= 1");
     if ((long long)(y - 2) * z >= (1LL << 31) / 2 || (long long)n * x * y * z >= (1LL << 40))
         return fail(net, DG_ERR_INVALID, "input too large");
     return DG_OK;
@@ -656,24 +650,25 @@ int32_t dg_net_get_tensor(dg_net *net, int32_t layer, int32_t which, void *host,
     const int k = 2 * (layer + 1);
     const int ex = ws.x - k, ey = ws.y - k, ez = ws.z - k;
     const size_t count = (size_t)ws.n * ex * ey * ez * kCout[layer];
-    if (which == 2) {
+    if (which == 0 || which == 1) {
+        if (layer == 3) return fail(net, DG_ERR_INVALID, "layer 3 has no activation; use which = 2");
+        if (bytes < count * 2) return fail(net, DG_ERR_INVALID, "host buffer too small");
+        NET_CUDA(net, cudaMemcpy(host, which == 0 ? ws.act[layer] : ws.pre[layer], count * 2, cudaMemcpyDeviceToHost));
+    } else if (which == 2) {
         if (layer != 3) return fail(net, DG_ERR_INVALID, "the output belongs to layer 3");
         if (bytes < count * 4) return fail(net, DG_ERR_INVALID, "host buffer too small");
         NET_CUDA(net, cudaMemcpy(host, ws.out, count * 4, cudaMemcpyDeviceToHost));
-        return DG_OK;
+    } else {
+        if (bytes < count * 2) return fail(net, DG_ERR_INVALID, "host buffer too small");
+        __nv_bfloat16 *tmp = nullptr;
+        NET_CUDA(net, cudaMalloc(&tmp, count * 2));
+        unpad_kernel<<<256, 256, 0, net->stream>>>(ws.dz[layer], tmp, ws.n, ex, ey, ez, kCout[layer]);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(host, tmp, count * 2, cudaMemcpyDeviceToHost, net->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(net->stream);
+        cudaFree(tmp);
+        if (e != cudaSuccess) return fail(net, DG_ERR_CUDA, std::string("get_tensor: ") + cudaGetErrorString(e));
     }
-    if ((which == 0 || which == 1) && layer == 3)
-        return fail(net, DG_ERR_INVALID, "layer 3 has no activation; use which = 2");
-    if (bytes < count * 2) return fail(net, DG_ERR_INVALID, "host buffer too small");
-    const __nv_bfloat16 *src = which == 0 ? ws.act[layer] : which == 1 ? ws.pre[layer] : ws.dz[layer];
-    __nv_bfloat16 *tmp = nullptr;
-    NET_CUDA(net, cudaMalloc(&tmp, count * 2));
-    unblock_kernel<<<256, 256, 0, net->stream>>>(src, tmp, ws.n, ex, ey, ez, kCout[layer], which == 3 ? 2 : 0);
-    cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaMemcpyAsync(host, tmp, count * 2, cudaMemcpyDeviceToHost, net->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(net->stream);
-    cudaFree(tmp);
-    if (e != cudaSuccess) return fail(net, DG_ERR_CUDA, std::string("get_tensor: ") + cudaGetErrorString(e));
     return DG_OK;
 }
 

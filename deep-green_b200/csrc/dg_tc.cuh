@@ -28,6 +28,19 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t
            ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
+// Descriptor of a K-major operand in one of the swizzled layouts: rows of
+// `row` bytes (32 or 64), 8-row atoms of 8*row bytes whose 16-byte chunks are
+// permuted by address bits (chunk ^= (address >> 7) & (row/16 - 1)); SBO =
+// stride between atoms.  Layout codes: 6 = 32-byte swizzle, 4 = 64-byte.
+// The K step of 16 elements (32 bytes) advances the start address inside a
+// row; the permutation follows the absolute address, so starts that are
+// not atom-aligned address the same bytes the TMA swizzle wrote.
+__device__ __forceinline__ uint64_t sdesc_sw(uint32_t saddr, uint32_t row) {
+    const uint64_t layout = row == 64 ? 4ull : 6ull;
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | (1ull << 16) | ((uint64_t)(((8 * row) >> 4) & 0x3FFFu) << 32) |
+           (1ull << 46) | (layout << 61);
+}
+
 // 32-bit instruction descriptor of kind::f16: BF16 x BF16 -> FP32.
 // a_mn / b_mn: 1 when that operand is MN-major.
 __host__ __device__ constexpr uint32_t idesc_bf16(int m, int n, int a_mn, int b_mn) {

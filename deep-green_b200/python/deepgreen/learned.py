@@ -234,8 +234,7 @@ class Batcher:
         self.ps, self.batch, self.crop = ps, batch, crop
         self.ext = crop + 8
         dev = torch.device("cuda", device)
-        self.feat = torch.zeros((batch, self.ext, IO_CHANNELS // 8, self.ext, self.ext, 8), dtype=torch.bfloat16,
-                                device=dev)
+        self.feat = torch.zeros((batch, self.ext, self.ext, self.ext, IO_CHANNELS), dtype=torch.bfloat16, device=dev)
         self.tgt = torch.zeros((batch, crop, crop, crop, IO_CHANNELS), dtype=torch.float32, device=dev)
         self.rng = np.random.default_rng(seed)
 
@@ -260,8 +259,7 @@ def fit_norm(ps: PairSet, samples: int = 16, crop: int = 48, seed: int = 0) -> N
     b = Batcher(ps, samples, crop, seed)
     b.fill(ident)
     torch.cuda.synchronize()
-    from .net import unblock
-    f = unblock(b.feat.float()).reshape(-1, IO_CHANNELS).cpu().numpy().astype(np.float64)
+    f = b.feat.float().reshape(-1, IO_CHANNELS).cpu().numpy().astype(np.float64)
     t = b.tgt.reshape(-1, IO_CHANNELS).cpu().numpy().astype(np.float64)
     norm = Norm.identity()
     for c in range(16):

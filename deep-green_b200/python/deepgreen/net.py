@@ -2,8 +2,8 @@
 
 Device tensors are passed as torch CUDA tensors (torch provides the device
 memory); all arithmetic runs in libdeepgreen.so's kernels.  Layouts:
-features BF16 channel-blocked [n][x][2][y][z][8] (see `block`), outputs and
-targets FP32 channels-last [n][x-8][y-8][z-8][16].
+features BF16 [n][x][y][z][16], outputs and targets FP32
+[n][x-8][y-8][z-8][16], channels last.
 """
 from __future__ import annotations
 
@@ -23,18 +23,6 @@ class NetInfo(ctypes.Structure):
         ("inputs", ctypes.c_int32), ("outputs", ctypes.c_int32), ("device", ctypes.c_int32),
         ("pad", ctypes.c_int32), ("seed", ctypes.c_uint64), ("out_scale", ctypes.c_double),
     ]
-
-
-def block(t):
-    """[n][x][y][z][C] -> channel-blocked [n][x][C/8][y][z][8] (a copy)."""
-    n, x, y, z, c = t.shape
-    return t.reshape(n, x, y, z, c // 8, 8).permute(0, 1, 4, 2, 3, 5).contiguous()
-
-
-def unblock(t):
-    """Channel-blocked [n][x][C/8][y][z][8] -> [n][x][y][z][C] (a copy)."""
-    n, x, g, y, z, e = t.shape
-    return t.permute(0, 1, 3, 4, 2, 5).reshape(n, x, y, z, g * e).contiguous()
 
 
 def layer_shape(layer: int, inputs: int, outputs: int):
@@ -106,11 +94,9 @@ class Net:
     @staticmethod
     def _dims(feat):
         import torch
-        if (feat.dtype != torch.bfloat16 or feat.dim() != 6 or tuple(feat.shape[-1:]) != (8,)
-                or feat.shape[2] != IO_CHANNELS // 8 or not feat.is_contiguous()):
-            raise ValueError("features must be a contiguous BF16 tensor [n][x][2][y][z][8] (see block())")
-        n, x, _, y, z, _ = feat.shape
-        return int(n), int(x), int(y), int(z)
+        if feat.dtype != torch.bfloat16 or feat.dim() != 5 or feat.shape[-1] != IO_CHANNELS or not feat.is_contiguous():
+            raise ValueError("features must be a contiguous BF16 tensor [n][x][y][z][16]")
+        return tuple(int(s) for s in feat.shape[:4])
 
     def forward(self, feat, out=None):
         import torch

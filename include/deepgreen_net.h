@@ -11,11 +11,9 @@
  * cores; master weights, gradients and Adam moments FP32.  Channels are padded
  * to DG_NET_IO_CHANNELS at the input and output (padding channels are zero).
  *
- * Device tensors, z fastest: the BF16 network input is channel-blocked,
- * [n][x][C/8][y][z][8] with C = 16 (for each x-plane, two planes of 8
- * channels); FP32 outputs and targets are channels-last [n][x][y][z][16].  A
- * forward pass over an input of extents (X, Y, Z) produces (X-8, Y-8, Z-8);
- * Z must be even (the kernels read pairs of positions).
+ * Device tensors are channels-last, [n][x][y][z][C] with C = 16, z fastest
+ * (BF16 inputs, FP32 outputs and targets).  A forward pass over an input of
+ * extents (X, Y, Z) produces (X-8, Y-8, Z-8).
  *
  * Layouts of parameters exchanged with the host: weights of layer l as FP32
  * [cout][cin][3][3][3] over the REAL channel counts (the layout of
@@ -58,11 +56,11 @@ int32_t dg_net_set_layer(dg_net *net, int32_t layer, const float *w, const float
 int32_t dg_net_get_layer(dg_net *net, int32_t layer, float *w, float *b);
 int32_t dg_net_get_grad(dg_net *net, int32_t layer, float *gw, float *gb);
 
-/* Inference.  feat: device BF16 [n][x][2][y][z][8]; out: device FP32
+/* Inference.  feat: device BF16 [n][x][y][z][16]; out: device FP32
  * [n][x-8][y-8][z-8][16].  Asynchronous on the network's stream. */
 int32_t dg_net_forward(dg_net *net, const void *feat, int32_t n, int32_t x, int32_t y, int32_t z, float *out);
 
-/* One forward + backward pass.  feat: device BF16 [n][x][2][y][z][8]; target:
+/* One forward + backward pass.  feat: device BF16 [n][x][y][z][16]; target:
  * device FP32 [n][x-8][y-8][z-8][16] (first `outputs` channels used).  Loss
  * = mean over positions and real outputs of (out - target)^2, returned in
  * *loss (synchronises).  Gradients are kept in the network (replacing the
@@ -77,8 +75,8 @@ int32_t dg_net_adam_step(dg_net *net, float lr, float beta1, float beta2, float 
 /* Copy of an intermediate tensor of the last forward_backward, for tests:
  * which = 0 activation (after GELU, BF16 bits), 1 pre-activation (BF16
  * bits), 2 network output (FP32), 3 gradient w.r.t. the pre-activation (BF16
- * bits, unpadded); BF16 ones are returned channels-last [n][x][y][z][C].
- * Layer 0..3; host buffer sized by the caller. */
+ * bits, unpadded), channels-last [n][x][y][z][C].  Layer 0..3; host
+ * buffer sized by the caller. */
 int32_t dg_net_get_tensor(dg_net *net, int32_t layer, int32_t which, void *host, uint64_t bytes);
 
 /* ---- Learned coarse step -------------------------------------------------
@@ -113,8 +111,8 @@ int32_t dg_coarsen(dg_ctx *fine, dg_ctx *coarse);
 
 /* Network inputs of a crop of a periodic cubic grid with n interior cells per
  * axis, from state packs `before` and `after`: ext^3 cells starting at
- * interior cell (ox, oy, oz) (wrapped), written as BF16 [ext][2][ext][ext][8]
- * (channel-blocked) to feat.  Asynchronous on `stream` (cudaStream_t or NULL). */
+ * interior cell (ox, oy, oz) (wrapped), written as BF16 [ext][ext][ext][16]
+ * to feat.  Asynchronous on `stream` (cudaStream_t or NULL). */
 int32_t dg_learned_features(const dg_learned_norm *norm, const float *before, const float *after, int32_t n, double ds,
                             double gamma, int32_t ox, int32_t oy, int32_t oz, int32_t ext, void *feat, void *stream);
 

@@ -72,7 +72,7 @@ def test_features_and_targets_match_numpy():
     for c in range(5):
         norm.out_std[c] = float(rng.uniform(0.5, 2))
     ext, origin = 9, (-4, 7, 10)
-    feat = torch.zeros((1, ext, 2, ext, ext, 8), dtype=torch.bfloat16, device="cuda")
+    feat = torch.zeros((ext, ext, ext, 16), dtype=torch.bfloat16, device="cuda")
     learned.features(norm, pool.ptr(0), pool.ptr(1), n, origin, ext, feat.data_ptr())
     tgt = torch.zeros((ext, ext, ext, 16), dtype=torch.float32, device="cuda")
     learned.targets(norm, pool.ptr(1), pool.ptr(2), n, origin, ext, tgt.data_ptr())
@@ -93,7 +93,7 @@ def test_features_and_targets_match_numpy():
     inv = np.array(norm.in_inv_std)
     inv[14:] = 0.0
     exp = (raw - mean) * inv
-    got = dnet.unblock(feat.float())[0].cpu().numpy()
+    got = feat.float().cpu().numpy()
     np.testing.assert_allclose(got, exp, rtol=1e-2, atol=2e-2 * np.abs(exp).max())
     et = np.zeros((ext, ext, ext, 16))
     et[..., :5] = (tr - u1) / np.array(norm.out_std)[:5]
