@@ -211,7 +211,8 @@ __device__ bool block_sum(double v[K], double *part, unsigned *counter) {
     return last != 0;
 }
 
-// pass 1: raw correction (totals), positivity mask, sums for the mean
+// pass 1: raw correction (totals) = divergence of the network's face fluxes,
+// positivity mask, sums for the mean
 __global__ void __launch_bounds__(kLearnThreads) correct_kernel(View u1, const float *__restrict__ out, NormDev nm,
                                                                 float vol, float inv_vol, float gm1,
                                                                 float *__restrict__ delta, uint8_t *__restrict__ mask,
@@ -223,9 +224,19 @@ __global__ void __launch_bounds__(kLearnThreads) correct_kernel(View u1, const f
          v += (long long)gridDim.x * blockDim.x) {
         const int z = (int)(v % n), y = (int)((v / n) % n), x = (int)(v / ((long long)n * n));
         const long long i = vidx(u1, x, y, z);
-        const float4 o0 = *reinterpret_cast<const float4 *>(out + v * 16);
-        const float o4 = out[v * 16 + 4];
-        const float o[5] = {o0.x, o0.y, o0.z, o0.w, o4};
+        // divergence of the face fluxes (channel 5 d + c), periodic
+        const long long nn = (long long)n * n;
+        const long long lo[3] = {(long long)(x == 0 ? n - 1 : x - 1) * nn + (long long)y * n + z,
+                                 (long long)x * nn + (long long)(y == 0 ? n - 1 : y - 1) * n + z,
+                                 (long long)x * nn + (long long)y * n + (z == 0 ? n - 1 : z - 1)};
+        float o[5];
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+            float s = 0.0f;
+#pragma unroll
+            for (int dd = 0; dd < 3; ++dd) s += out[v * 16 + 5 * dd + c] - out[lo[dd] * 16 + 5 * dd + c];
+            o[c] = s;
+        }
         float d[5], u[5];
         bool ok = true;
 #pragma unroll
@@ -451,7 +462,7 @@ int32_t dg_corrector_create(dg_ctx *coarse, dg_net *net, const dg_learned_norm *
     if (coarse->elem != 4 || coarse->exact) return lfail(DG_ERR_INVALID, "the corrector needs the FP32 fast step");
     if (!periodic_cube(coarse)) return lfail(DG_ERR_INVALID, "the corrector needs a cubic, periodic grid");
     if (net_inputs(net) != DG_LEARNED_INPUTS || net_outputs(net) != DG_LEARNED_OUTPUTS)
-        return lfail(DG_ERR_INVALID, "the network must have 14 inputs and 5 outputs");
+        return lfail(DG_ERR_INVALID, "the network must have 14 inputs and 15 (flux) outputs");
     if (net_device(net) != coarse->info.device) return lfail(DG_ERR_INVALID, "network and grid on different devices");
     for (int c = 0; c < DG_LEARNED_OUTPUTS; ++c)
         if (!(norm->out_std[c] > 0)) return lfail(DG_ERR_INVALID, "out_std must be positive");

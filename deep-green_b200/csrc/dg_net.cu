@@ -32,6 +32,8 @@ struct Workspace {
     float *out = nullptr;              // network output (training)
     __nv_bfloat16 *dz[4] = {};         // gradients w.r.t. Z1..Z3 and the output, padded by 2
     size_t act_bytes[3] = {}, dz_bytes[4] = {}, out_bytes = 0;
+    float *gbuf = nullptr;             // flux-form loss: gradient w.r.t. the corrections
+    long long gbuf_elems = 0;
 };
 
 }  // namespace
@@ -196,6 +198,78 @@ __global__ void loss_kernel(const float *__restrict__ out, const float *__restri
     }
 }
 
+// Flux-form loss, pass 1: the correction of target cell t is the divergence
+// of the network's face fluxes, dU_c(t) = sum_d F_{d,c}(t+1) - F_{d,c}(t+1-e_d)
+// (output channel 5 d + c, output cell t+1 in an output one cell larger than
+// the target on each axis); residual r = dU - target, squared-error partials
+// per block, and g = scale * r into gbuf [n][s^3][5].
+__global__ void flux_residual_kernel(const float *__restrict__ out, const float *__restrict__ tgt, int n, int s,
+                                     float scale, float *__restrict__ gbuf, double *part) {
+    __shared__ double red[32];
+    const long long total = (long long)n * s * s * s;
+    const int o = s + 1;
+    double acc = 0.0;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < total;
+         v += (long long)gridDim.x * blockDim.x) {
+        long long r = v;
+        const int iz = r % s; r /= s;
+        const int iy = r % s; r /= s;
+        const int ix = r % s;
+        const int b = (int)(r / s);
+        const long long c0 = ((((long long)b * o + ix + 1) * o + iy + 1) * o + iz + 1) * kIO;
+        const long long lo[3] = {c0 - (long long)o * o * kIO, c0 - (long long)o * kIO, c0 - kIO};
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+            float du = 0.0f;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) du += out[c0 + 5 * d + c] - out[lo[d] + 5 * d + c];
+            const float res = du - tgt[v * kIO + c];
+            acc += (double)res * res;
+            gbuf[v * 5 + c] = scale * res;
+        }
+    }
+#pragma unroll
+    for (int sh = 16; sh > 0; sh >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, sh);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double sum = 0.0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) sum += red[i];
+        part[blockIdx.x] = sum;
+    }
+}
+
+// Flux-form loss, pass 2: dL/dF_{d,c}(q) = g_c(q-1) - g_c(q-1+e_d) (terms whose
+// target cell lies outside the target are absent), as BF16 into the interior
+// of the output-gradient buffer padded by 2; channel 15 is zero.
+__global__ void flux_grad_kernel(const float *__restrict__ gbuf, int n, int s, __nv_bfloat16 *__restrict__ dz) {
+    const int o = s + 1;
+    const long long total = (long long)n * o * o * o;
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < total;
+         v += (long long)gridDim.x * blockDim.x) {
+        long long r = v;
+        const int qz = r % o; r /= o;
+        const int qy = r % o; r /= o;
+        const int qx = r % o;
+        const int b = (int)(r / o);
+        auto gat = [&](int tx, int ty, int tz, int c) -> float {
+            if (tx < 0 || ty < 0 || tz < 0 || tx >= s || ty >= s || tz >= s) return 0.0f;
+            return gbuf[((((long long)b * s + tx) * s + ty) * s + tz) * 5 + c];
+        };
+        float g[kIO];
+#pragma unroll
+        for (int c = 0; c < 5; ++c) {
+            const float self = gat(qx - 1, qy - 1, qz - 1, c);
+            g[c] = self - gat(qx, qy - 1, qz - 1, c);
+            g[5 + c] = self - gat(qx - 1, qy, qz - 1, c);
+            g[10 + c] = self - gat(qx - 1, qy - 1, qz, c);
+        }
+        g[15] = 0.0f;
+        const long long d = ((((long long)b * (o + 4) + qx + 2) * (o + 4) + qy + 2) * (o + 4) + qz + 2) * kIO;
+        store_bf16(dz + d, g, kIO);
+    }
+}
+
 __global__ void adam_kernel(float *__restrict__ p, const float *__restrict__ g, float *__restrict__ m,
                             float *__restrict__ v, int count, float lr, float b1, float b2, float eps, float c1,
                             float c2) {
@@ -318,6 +392,9 @@ void free_ws(Workspace &ws) {
     }
     cudaFree(ws.out);
     ws.out = nullptr;
+    cudaFree(ws.gbuf);
+    ws.gbuf = nullptr;
+    ws.gbuf_elems = 0;
     ws.n = 0;
 }
 
@@ -399,6 +476,34 @@ int forward(dg_net *net, const void *feat, int n, int x, int y, int z, float *ou
     a.out_f = out;
     e = launch_conv<kH, kIO, kEpiLinear>(net, in, n, xi, yi, zi, net->wf[3], a, st);
     if (e != cudaSuccess) return fail(net, DG_ERR_CUDA, std::string("conv launch: ") + cudaGetErrorString(e));
+    return DG_OK;
+}
+
+// Backward pass from the output gradient in ws.dz[3] down to the weights of
+// layer 0 (weight gradients of every layer, input gradients of layers 1-3).
+int backward(dg_net *net, const void *feat, int n, int x, int y, int z) {
+    Workspace &ws = net->ws;
+    cudaError_t e;
+    for (int l = 3; l >= 0; --l) {
+        const int k = 2 * (l + 1);
+        const int ex = x - k, ey = y - k, ez = z - k;        // extents of layer l's output
+        const void *xin = l == 0 ? feat : ws.act[l - 1];
+        if (l == 3) e = launch_wgrad<kH, kIO>(net, xin, ws.dz[l], n, ex, ey, ez, net->gw[l], net->gb[l]);
+        else if (l == 0) e = launch_wgrad<kIO, kH>(net, xin, ws.dz[l], n, ex, ey, ez, net->gw[l], net->gb[l]);
+        else e = launch_wgrad<kH, kH>(net, xin, ws.dz[l], n, ex, ey, ez, net->gw[l], net->gb[l]);
+        if (e != cudaSuccess) return fail(net, DG_ERR_CUDA, std::string("wgrad launch: ") + cudaGetErrorString(e));
+        if (l == 0) break;
+        // gradient w.r.t. the pre-activation of layer l-1 (extent ex+2), into its padded buffer
+        ConvArgs a{};
+        a.ox = ex + 2 + 4; a.oy = ey + 2 + 4; a.oz = ez + 2 + 4; a.off = 2;
+        a.out_a = ws.dz[l - 1];
+        a.zsrc = ws.pre[l - 1];
+        if (l == 3) e = launch_conv<kIO, kH, kEpiDGelu>(net, ws.dz[l], n, ex + 4, ey + 4, ez + 4, net->wd[l], a,
+                                                        net->stream);
+        else e = launch_conv<kH, kH, kEpiDGelu>(net, ws.dz[l], n, ex + 4, ey + 4, ez + 4, net->wd[l], a,
+                                                net->stream);
+        if (e != cudaSuccess) return fail(net, DG_ERR_CUDA, std::string("dgrad launch: ") + cudaGetErrorString(e));
+    }
     return DG_OK;
 }
 
@@ -590,28 +695,7 @@ int32_t dg_net_forward_backward(dg_net *net, const void *feat, const float *targ
     loss_kernel<<<lblocks, 256, 0, net->stream>>>(ws.out, target, n, xo, yo, zo, net->outputs, scale, ws.dz[3],
                                                   net->loss_part);
     NET_CUDA(net, cudaGetLastError());
-    // backward, layer 3 down to layer 0
-    cudaError_t e;
-    for (int l = 3; l >= 0; --l) {
-        const int k = 2 * (l + 1);
-        const int ex = x - k, ey = y - k, ez = z - k;        // extents of layer l's output
-        const void *xin = l == 0 ? feat : ws.act[l - 1];
-        if (l == 3) e = launch_wgrad<kH, kIO>(net, xin, ws.dz[l], n, ex, ey, ez, net->gw[l], net->gb[l]);
-        else if (l == 0) e = launch_wgrad<kIO, kH>(net, xin, ws.dz[l], n, ex, ey, ez, net->gw[l], net->gb[l]);
-        else e = launch_wgrad<kH, kH>(net, xin, ws.dz[l], n, ex, ey, ez, net->gw[l], net->gb[l]);
-        if (e != cudaSuccess) return fail(net, DG_ERR_CUDA, std::string("wgrad launch: ") + cudaGetErrorString(e));
-        if (l == 0) break;
-        // gradient w.r.t. the pre-activation of layer l-1 (extent ex+2), into its padded buffer
-        ConvArgs a{};
-        a.ox = ex + 2 + 4; a.oy = ey + 2 + 4; a.oz = ez + 2 + 4; a.off = 2;
-        a.out_a = ws.dz[l - 1];
-        a.zsrc = ws.pre[l - 1];
-        if (l == 3) e = launch_conv<kIO, kH, kEpiDGelu>(net, ws.dz[l], n, ex + 4, ey + 4, ez + 4, net->wd[l], a,
-                                                        net->stream);
-        else e = launch_conv<kH, kH, kEpiDGelu>(net, ws.dz[l], n, ex + 4, ey + 4, ez + 4, net->wd[l], a,
-                                                net->stream);
-        if (e != cudaSuccess) return fail(net, DG_ERR_CUDA, std::string("dgrad launch: ") + cudaGetErrorString(e));
-    }
+    if (int r = backward(net, feat, n, x, y, z)) return r;
     if (int r = check_status(net)) return r;
     if (loss) {
         std::vector<double> part(lblocks);
@@ -619,6 +703,46 @@ int32_t dg_net_forward_backward(dg_net *net, const void *feat, const float *targ
         double s = 0.0;
         for (double v : part) s += v;
         *loss = s / ((double)nvox * net->outputs);
+    }
+    return DG_OK;
+}
+
+int32_t dg_net_forward_backward_flux(dg_net *net, const void *feat, const float *target, int32_t n, int32_t x,
+                                     int32_t y, int32_t z, double *loss) {
+    if (!net || !feat || !target) return fail(net, DG_ERR_INVALID, "null argument");
+    if (net->outputs != 15) return fail(net, DG_ERR_INVALID, "the flux form needs a network with 15 outputs");
+    if (x != y || y != z) return fail(net, DG_ERR_INVALID, "the flux form takes cubic crops");
+    if (int r = check_extents(net, n, x, y, z)) return r;
+    if (x < 10) return fail(net, DG_ERR_INVALID, "the flux form needs extents of at least 10");
+    if ((reinterpret_cast<uintptr_t>(feat) | reinterpret_cast<uintptr_t>(target)) & 15)
+        return fail(net, DG_ERR_INVALID, "device pointers must be 16-byte aligned");
+    NET_CUDA(net, cudaSetDevice(net->device));
+    if (int r = ensure_ws(net, n, x, y, z, true)) return r;
+    Workspace &ws = net->ws;
+    const int s = x - 9;                                   // target extent
+    const long long ntgt = (long long)n * s * s * s;
+    if (ws.gbuf_elems < ntgt * 5) {
+        NET_CUDA(net, cudaStreamSynchronize(net->stream));
+        cudaFree(ws.gbuf);
+        ws.gbuf = nullptr;
+        ws.gbuf_elems = 0;
+        NET_CUDA(net, cudaMalloc(&ws.gbuf, ntgt * 5 * sizeof(float)));
+        ws.gbuf_elems = ntgt * 5;
+    }
+    if (int r = forward(net, feat, n, x, y, z, ws.out, true, net->stream)) return r;
+    const float scale = (float)(2.0 / ((double)ntgt * 5));
+    const int lblocks = (int)std::min<long long>(4096, (ntgt + 255) / 256);
+    flux_residual_kernel<<<lblocks, 256, 0, net->stream>>>(ws.out, target, n, s, scale, ws.gbuf, net->loss_part);
+    flux_grad_kernel<<<1024, 256, 0, net->stream>>>(ws.gbuf, n, s, ws.dz[3]);
+    NET_CUDA(net, cudaGetLastError());
+    if (int r = backward(net, feat, n, x, y, z)) return r;
+    if (int r = check_status(net)) return r;
+    if (loss) {
+        std::vector<double> part(lblocks);
+        NET_CUDA(net, cudaMemcpy(part.data(), net->loss_part, lblocks * sizeof(double), cudaMemcpyDeviceToHost));
+        double sum = 0.0;
+        for (double v : part) sum += v;
+        *loss = sum / ((double)ntgt * 5);
     }
     return DG_OK;
 }

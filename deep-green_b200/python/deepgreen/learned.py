@@ -9,7 +9,9 @@ Pairs (one per coarse step): a fine periodic grid F (2n cells per axis) and
 a coarse grid C (n) that starts as the 2x2x2 sums of F.  F takes two steps
 (dt1, dt2, its own CFL dts); C takes one plain step of dt1 + dt2.  The pair
 is (C before, C after, truth = coarsened F after): the network learns
-truth - C_after from (C_before, C_after).
+truth - C_after from (C_before, C_after), in flux form -- it predicts face
+fluxes whose divergence is the correction, so the correction conserves the
+totals exactly and vanishes for uniform states.
 """
 from __future__ import annotations
 
@@ -25,7 +27,7 @@ from . import capi, setups
 from .net import IO_CHANNELS, Net
 
 INPUTS = 14
-OUTPUTS = 5
+OUTPUTS = 15          # face fluxes: the correction is their divergence
 GAMMA = 1.4
 CFL = 0.4
 
@@ -232,7 +234,7 @@ class Batcher:
     def __init__(self, ps: PairSet, batch: int, crop: int, seed: int, device: int = 0):
         import torch
         self.ps, self.batch, self.crop = ps, batch, crop
-        self.ext = crop + 8
+        self.ext = crop + 9        # network output crop + 1: the divergence needs the lower faces
         dev = torch.device("cuda", device)
         self.feat = torch.zeros((batch, self.ext, self.ext, self.ext, IO_CHANNELS), dtype=torch.bfloat16, device=dev)
         self.tgt = torch.zeros((batch, crop, crop, crop, IO_CHANNELS), dtype=torch.float32, device=dev)
@@ -245,7 +247,7 @@ class Batcher:
         for i in range(self.batch):
             slot = int(self.rng.integers(0, self.ps.count))
             o = self.rng.integers(0, n, 3)
-            features(norm, self.ps.before.ptr(slot), self.ps.after.ptr(slot), n, o - 4, self.ext,
+            features(norm, self.ps.before.ptr(slot), self.ps.after.ptr(slot), n, o - 5, self.ext,
                      self.feat.data_ptr() + i * fstride, stream)
             targets(norm, self.ps.after.ptr(slot), self.ps.truth.ptr(slot), n, o, self.crop,
                     self.tgt.data_ptr() + i * tstride, stream)
@@ -283,7 +285,7 @@ def train(net: Net, ps: PairSet, norm: Norm, steps: int, batch: int = 8, crop: i
     t0 = time.time()
     for it in range(steps):
         b.fill(norm)
-        loss = net.forward_backward(b.feat, b.tgt)
+        loss = net.forward_backward_flux(b.feat, b.tgt)
         rate = lr_min + 0.5 * (lr - lr_min) * (1.0 + math.cos(math.pi * it / max(steps, 1)))
         net.adam_step(rate)
         hist.append(loss)

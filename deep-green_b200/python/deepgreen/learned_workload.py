@@ -2,8 +2,9 @@
 
 Training (fine 256^3 vs coarse 128^3): pairs generated by the solver from
 seeded KH layers (shear in [0.2, 0.8], density ratio in [1, 4]) and smooth
-8-mode Fourier states; a 4-layer, 32-channel 3x3x3 CNN with GELU, trained by
-the library's tensor-core kernels with Adam, batch 8 crops of 64^3.
+8-mode Fourier states; a 4-layer, 32-channel 3x3x3 CNN with GELU predicting
+face fluxes (the correction is their divergence), trained by the library's
+tensor-core kernels with Adam, batch 8 crops of 64^3.
 
 Evaluation (coarse 256^3 corrected every step vs fine 512^3 plain): held-out
 KH (shear 0.5, density ratio 2) and Fourier states, to the time the fine
@@ -53,8 +54,8 @@ def validation_loss(net, ps, norm, batches=8, batch=8, crop=64, seed=123):
     lt, lz = [], []
     for _ in range(batches):
         b.fill(norm)
-        lt.append(net.forward_backward(b.feat, b.tgt))
-        lz.append(zero.forward_backward(b.feat, b.tgt))
+        lt.append(net.forward_backward_flux(b.feat, b.tgt))
+        lz.append(zero.forward_backward_flux(b.feat, b.tgt))
     return float(np.mean(lt)), float(np.mean(lz))
 
 

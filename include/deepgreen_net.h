@@ -68,6 +68,17 @@ int32_t dg_net_forward(dg_net *net, const void *feat, int32_t n, int32_t x, int3
 int32_t dg_net_forward_backward(dg_net *net, const void *feat, const float *target, int32_t n, int32_t x,
                                 int32_t y, int32_t z, double *loss);
 
+/* The same in flux form, for a network with 15 outputs: output channel
+ * 5 d + c is the flux of conserved field c through the upper face of a cell
+ * along axis d (x, y, z), and the correction of cell t is the divergence
+ * dU_c(t) = sum_d F_{d,c}(t) - F_{d,c}(t - e_d) -- exactly conservative, and
+ * zero wherever the fluxes are uniform.  Cubic crops: feat of extents x^3,
+ * network output (x-8)^3, target FP32 [n][x-9][x-9][x-9][16] (first 5
+ * channels: the corrections of the cells whose lower faces the output also
+ * covers).  Loss = mean over cells and the 5 fields of (dU - target)^2. */
+int32_t dg_net_forward_backward_flux(dg_net *net, const void *feat, const float *target, int32_t n, int32_t x,
+                                     int32_t y, int32_t z, double *loss);
+
 /* Adam update of all parameters from the stored gradients (bias-corrected,
  * step counter kept by the network). */
 int32_t dg_net_adam_step(dg_net *net, float lr, float beta1, float beta2, float eps);
@@ -87,16 +98,17 @@ int32_t dg_net_get_tensor(dg_net *net, int32_t layer, int32_t which, void *host,
  *   0 rho1, 1-3 (rho v)1, 4 E1,  5-9 U1 - U0 (same order),
  *   10-12 v1 = (rho v)1 / rho1,  13 p1 = (gamma-1)(E1 - |(rho v)1|^2 / (2 rho1)),
  * each normalised as (raw - in_mean[c]) * in_inv_std[c] (channels 14, 15 are
- * zero).  Output channel c < 5 is the correction of conserved density c in
- * units of out_std[c].  Grids must be cubic and periodic: the network's
- * 4-cell halo wraps around the domain.
+ * zero).  The network has 15 outputs, face fluxes in flux form (see
+ * dg_net_forward_backward_flux); their divergence is the correction of
+ * conserved density c in units of out_std[c].  Grids must be cubic and
+ * periodic: the network's 4-cell halo and the divergence wrap around.
  *
  * "State packs" are dense device copies of a grid's conserved state: 5
  * fields (mass, mom_x, mom_y, mom_z, energy) of (n+4)^3 FP32 values each, C
  * order with ghosts, consecutive -- what dg_get_conserved_device writes when
  * given pointers 1, 2, ... fields apart. */
 #define DG_LEARNED_INPUTS 14
-#define DG_LEARNED_OUTPUTS 5
+#define DG_LEARNED_OUTPUTS 15
 
 typedef struct dg_learned_norm {
     float in_mean[16];
@@ -135,7 +147,7 @@ typedef struct dg_learned_stats {
 } dg_learned_stats;
 
 /* A corrector couples a coarse FP32 context (cubic, periodic) and a network
- * (14 inputs, 5 outputs).  Each step: one plain step; the network's
+ * (14 inputs, 15 flux outputs).  Each step: one plain step; the network's
  * correction, zero in cells where rho or p of the corrected state would not
  * be positive, minus its mean over the other cells; the whole step falls back
  * to the plain state if a cell still loses positivity or the correction

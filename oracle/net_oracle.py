@@ -60,7 +60,15 @@ def pad_params(params, inputs, outputs):
     return out
 
 
-def forward_backward(params, feat, target, inputs, outputs, round_bf16=True):
+def flux_divergence(F):
+    """dU_c(t) = sum_d F[5d+c](t+1) - F[5d+c](t+1-e_d) over the target cells
+    t, for F of shape (n, 16, s+1, s+1, s+1); returns (n, 5, s, s, s)."""
+    hi = F[:, :, 1:, 1:, 1:]
+    lo = [F[:, :, :-1, 1:, 1:], F[:, :, 1:, :-1, 1:], F[:, :, 1:, 1:, :-1]]
+    return sum(hi[:, 5 * d:5 * d + 5] - lo[d][:, 5 * d:5 * d + 5] for d in range(3))
+
+
+def forward_backward(params, feat, target, inputs, outputs, round_bf16=True, flux=False):
     """params: real-channel (w, b) per layer (FP32 master values); feat:
     (n, x, y, z, 16) array of BF16-representable values; target: (n, x-8,
     y-8, z-8, 16).  Returns dict with loss, out, act[l], pre[l], dz[l]
@@ -74,6 +82,7 @@ def forward_backward(params, feat, target, inputs, outputs, round_bf16=True):
     B = [b for _, b in P]
     x = torch.as_tensor(np.asarray(feat, dtype=np.float64)).permute(0, 4, 1, 2, 3).contiguous()
     t = torch.as_tensor(np.asarray(target, dtype=np.float64)).permute(0, 4, 1, 2, 3).contiguous()
+    # flux form: target extent is one less than the output's
     acts, pres = [x], []
     a = x
     for l in range(3):
@@ -82,10 +91,26 @@ def forward_backward(params, feat, target, inputs, outputs, round_bf16=True):
         a = rnd(gelu(z))
         acts.append(a)
     out = F.conv3d(a, W[3]) + B[3].view(1, -1, 1, 1, 1)
-    d = out[:, :outputs] - t[:, :outputs]
-    loss = float((d * d).mean())
-    g = torch.zeros_like(out)
-    g[:, :outputs] = 2.0 * d / d.numel()
+    if flux:
+        # the divergence is linear: its adjoint comes from autograd, exactly
+        o = out.detach().requires_grad_(True)
+        d = flux_divergence(o) - t[:, :5]
+        lsum = (d * d).sum()
+        loss = float(lsum) / d.numel()
+        (gr,) = torch.autograd.grad(lsum, o)
+        g = (gr / d.numel()).detach()
+        # the GPU stores the per-cell residual gradient in FP32 first
+        if round_bf16:
+            res = (2.0 * d.detach() / d.numel()).to(torch.float32).to(torch.float64)
+            ores = torch.zeros_like(o)
+            ores.requires_grad_(True)
+            g = torch.autograd.grad((flux_divergence(ores) * res).sum(), ores)[0]
+    else:
+        d = out[:, :outputs] - t[:, :outputs]
+        loss = float((d * d).mean())
+        g = torch.zeros_like(out)
+        g[:, :outputs] = 2.0 * d / d.numel()
+    g[:, 15:] = 0.0
     dz = rnd(g.to(torch.float32).to(torch.float64)) if round_bf16 else g
     dzs = [None] * 4
     dzs[3] = dz

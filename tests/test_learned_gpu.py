@@ -127,20 +127,53 @@ def test_zero_correction_is_the_plain_step_bit_for_bit():
     assert st["steps"] == 3 and st["fallback_steps"] == 0 and st["masked_cells"] == 0
 
 
-def test_cells_that_would_lose_positivity_keep_the_plain_value():
-    n = 16
-    plain, corr = _grid(n, 6), _grid(n, 6)
+def _flux_of_density_net(lam):
+    """A network whose x-flux of mass is exactly lam * rho1 (input channel 0):
+    hidden channel 0 carries rho1 + 10 through the GELUs' linear range."""
     net = _net(0.0)
-    w, b = net.get_layer(3)
-    b[0] = -1e9                       # every density correction hugely negative
-    net.set_layer(3, w, b)
-    cor = learned.Corrector(corr, net, _norm(1.0))
+    w0 = np.zeros((32, 14, 3, 3, 3), np.float32)
+    w0[0, 0, 1, 1, 1] = 1.0
+    b0 = np.zeros(32, np.float32)
+    b0[0] = 10.0
+    net.set_layer(0, w0, b0)
+    for l in (1, 2):
+        w = np.zeros((32, 32, 3, 3, 3), np.float32)
+        w[0, 0, 1, 1, 1] = 1.0
+        net.set_layer(l, w, np.zeros(32, np.float32))
+    w3 = np.zeros((15, 32, 3, 3, 3), np.float32)
+    w3[0, 0, 1, 1, 1] = lam
+    b3 = np.zeros(15, np.float32)
+    b3[0] = -10.0 * lam
+    net.set_layer(3, w3, b3)
+    return net
+
+
+def test_cells_that_would_lose_positivity_keep_the_plain_value():
+    # uniform gas with one low-density cell: the plain step's dissipation turns it
+    # into a bump (rho1 ~ 1.18 against 0.82 around it); the correction
+    # d(rho) = -4 (rho1(i) - rho1(i - e_x)) drives that cell negative (masked)
+    # and raises its +x neighbour
+    n = 16
+    shape = (n + 4,) * 3
+    prim = [np.ones(shape), np.zeros(shape), np.zeros(shape), np.zeros(shape), np.ones(shape)]
+    prim[0][10, 10, 10] = 0.1
+    plain, corr = learned.grid(n), learned.grid(n)
+    plain.set_primitives(prim)
+    corr.set_primitives(prim)
+    # 16^3 is too small for the 1e-10 conservation bound (FP32 rounding alone
+    # moves the totals by ~5e-10 here): this test is about the mask
+    cor = learned.Corrector(corr, _flux_of_density_net(-4.0), _norm(1.0), tolerance=1e-6)
     plain.compute_step(1)
     cor.step(1)
-    for x, y in zip(plain.get_conserved(), corr.get_conserved()):
-        assert np.array_equal(x, y)
     st = cor.stats()
-    assert st["masked_cells"] == n ** 3 and st["fallback_steps"] == 0
+    assert st["fallback_steps"] == 0 and st["masked_cells"] >= 1, st
+    p = plain.get_conserved()
+    c = corr.get_conserved()
+    hole = (10, 10, 10)
+    for f in range(5):
+        assert p[f][hole] == c[f][hole]                      # masked: the plain value
+    assert c[0][11, 10, 10] > p[0][11, 10, 10]               # the neighbour took the mass
+    assert np.all(_interior(c[0]) > 0)
 
 
 def test_correction_conserves_totals():

@@ -107,3 +107,37 @@ def test_adam_step_matches_reference_update():
             v = (1 - b2) * g.astype(np.float64) ** 2
             exp = p0 - lr * (m / (1 - b1)) / (np.sqrt(v / (1 - b2)) + eps)
             np.testing.assert_allclose(p1, exp, rtol=1e-5, atol=1e-7)
+
+
+@pytest.mark.parametrize("n,ext", [(2, 14), (1, 19)])
+def test_flux_form_loss_and_gradients_match_cpu_oracle(n, ext):
+    import torch
+    import net_oracle
+
+    inputs, outputs = 14, 15
+    net = dnet.Net(inputs, outputs, seed=13, out_scale=1.0)
+    params = net.params()
+    rng = np.random.default_rng(8)
+    feat = np.zeros((n, ext, ext, ext, 16), np.float32)
+    feat[..., :inputs] = bf16_round(rng.standard_normal((n, ext, ext, ext, inputs)))
+    s = ext - 9
+    tgt = np.zeros((n, s, s, s, 16), np.float32)
+    tgt[..., :5] = rng.standard_normal((n, s, s, s, 5)).astype(np.float32)
+    dev = torch.device("cuda", 0)
+    f = torch.from_numpy(feat).to(dev).to(torch.bfloat16).contiguous()
+    loss = net.forward_backward_flux(f, torch.from_numpy(tgt).to(dev).contiguous())
+    ref = net_oracle.forward_backward(params, feat, tgt, inputs, outputs, flux=True)
+    assert abs(loss - ref["loss"]) <= 1e-4 * abs(ref["loss"])
+    o = ext - 8
+    assert rel_l2(net.get_tensor(3, 3, (n, o, o, o, 16)), ref["dz"][3]) < TOL
+    for l in range(4):
+        gw, gb = net.get_grad(l)
+        rw, rb = ref["grads"][l]
+        assert rel_l2(gw, rw) < TOL, ("gw", l, rel_l2(gw, rw))
+        if l < 3:
+            assert rel_l2(gb, rb) < TOL, ("gb", l, rel_l2(gb, rb))
+        else:
+            # the output bias gradient is the sum of the flux gradients, which
+            # telescopes to boundary terms: compare against the summands' size
+            scale = np.abs(ref["dz"][3]).reshape(-1, 16).sum(0)[:15]
+            assert np.all(np.abs(gb - rb) <= TOL * scale), ("gb", l, np.abs(gb - rb) / scale)
