@@ -34,6 +34,7 @@ struct Workspace {
     size_t act_bytes[3] = {}, dz_bytes[4] = {}, out_bytes = 0;
     float *gbuf = nullptr;             // flux-form loss: gradient w.r.t. the corrections
     long long gbuf_elems = 0;
+    float *wsample = nullptr;          // flux-form loss: per-entry weights (after gbuf)
 };
 
 }  // namespace
@@ -203,8 +204,43 @@ __global__ void loss_kernel(const float *__restrict__ out, const float *__restri
 // (output channel 5 d + c, output cell t+1 in an output one cell larger than
 // the target on each axis); residual r = dU - target, squared-error partials
 // per block, and g = scale * r into gbuf [n][s^3][5].
+// Per batch entry b: w[b] = 1 when not balancing, else mean power of all
+// targets / (power of entry b's target + floor * mean power), so that every
+// crop counts alike whatever the size of its corrections.
+__global__ void sample_weight_kernel(const float *__restrict__ tgt, int n, int s, int balance, float floor_frac,
+                                     float *__restrict__ w) {
+    __shared__ double red[32];
+    __shared__ double pw[64];
+    const long long per = (long long)s * s * s;
+    for (int b = 0; b < n; ++b) {
+        double acc = 0.0;
+        for (long long v = threadIdx.x; v < per; v += blockDim.x)
+            for (int c = 0; c < 5; ++c) {
+                const double t = tgt[((long long)b * per + v) * 16 + c];
+                acc += t * t;
+            }
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double sum = 0.0;
+            for (int i = 0; i < (int)(blockDim.x >> 5); ++i) sum += red[i];
+            pw[b] = sum / (per * 5.0);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double mean = 0.0;
+        for (int b = 0; b < n; ++b) mean += pw[b];
+        mean /= n;
+        for (int b = 0; b < n; ++b)
+            w[b] = balance && mean > 0.0 ? (float)(mean / (pw[b] + floor_frac * mean)) : 1.0f;
+    }
+}
+
 __global__ void flux_residual_kernel(const float *__restrict__ out, const float *__restrict__ tgt, int n, int s,
-                                     float scale, float *__restrict__ gbuf, double *part) {
+                                     float scale, const float *__restrict__ wsample, float *__restrict__ gbuf,
+                                     double *part) {
     __shared__ double red[32];
     const long long total = (long long)n * s * s * s;
     const int o = s + 1;
@@ -224,8 +260,9 @@ __global__ void flux_residual_kernel(const float *__restrict__ out, const float 
 #pragma unroll
             for (int d = 0; d < 3; ++d) du += out[c0 + 5 * d + c] - out[lo[d] + 5 * d + c];
             const float res = du - tgt[v * kIO + c];
-            acc += (double)res * res;
-            gbuf[v * 5 + c] = scale * res;
+            const float wb = wsample[b];
+            acc += (double)wb * res * res;
+            gbuf[v * 5 + c] = scale * wb * res;
         }
     }
 #pragma unroll
@@ -708,8 +745,9 @@ int32_t dg_net_forward_backward(dg_net *net, const void *feat, const float *targ
 }
 
 int32_t dg_net_forward_backward_flux(dg_net *net, const void *feat, const float *target, int32_t n, int32_t x,
-                                     int32_t y, int32_t z, double *loss) {
+                                     int32_t y, int32_t z, int32_t balance, double *loss) {
     if (!net || !feat || !target) return fail(net, DG_ERR_INVALID, "null argument");
+    if (n > 64) return fail(net, DG_ERR_INVALID, "at most 64 batch entries");
     if (net->outputs != 15) return fail(net, DG_ERR_INVALID, "the flux form needs a network with 15 outputs");
     if (x != y || y != z) return fail(net, DG_ERR_INVALID, "the flux form takes cubic crops");
     if (int r = check_extents(net, n, x, y, z)) return r;
@@ -726,13 +764,16 @@ int32_t dg_net_forward_backward_flux(dg_net *net, const void *feat, const float 
         cudaFree(ws.gbuf);
         ws.gbuf = nullptr;
         ws.gbuf_elems = 0;
-        NET_CUDA(net, cudaMalloc(&ws.gbuf, ntgt * 5 * sizeof(float)));
+        NET_CUDA(net, cudaMalloc(&ws.gbuf, ntgt * 5 * sizeof(float) + 64 * sizeof(float)));
         ws.gbuf_elems = ntgt * 5;
     }
+    ws.wsample = ws.gbuf + ws.gbuf_elems;
     if (int r = forward(net, feat, n, x, y, z, ws.out, true, net->stream)) return r;
     const float scale = (float)(2.0 / ((double)ntgt * 5));
     const int lblocks = (int)std::min<long long>(4096, (ntgt + 255) / 256);
-    flux_residual_kernel<<<lblocks, 256, 0, net->stream>>>(ws.out, target, n, s, scale, ws.gbuf, net->loss_part);
+    sample_weight_kernel<<<1, 256, 0, net->stream>>>(target, n, s, balance, 0.01f, ws.wsample);
+    flux_residual_kernel<<<lblocks, 256, 0, net->stream>>>(ws.out, target, n, s, scale, ws.wsample, ws.gbuf,
+                                                           net->loss_part);
     flux_grad_kernel<<<1024, 256, 0, net->stream>>>(ws.gbuf, n, s, ws.dz[3]);
     NET_CUDA(net, cudaGetLastError());
     if (int r = backward(net, feat, n, x, y, z)) return r;

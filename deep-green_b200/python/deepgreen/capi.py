@@ -99,7 +99,7 @@ SIGNATURES = {
     "dg_net_get_grad": [_P, _I, _P, _P],
     "dg_net_forward": [_P, _P, _I, _I, _I, _I, _P],
     "dg_net_forward_backward": [_P, _P, _P, _I, _I, _I, _I, ctypes.POINTER(ctypes.c_double)],
-    "dg_net_forward_backward_flux": [_P, _P, _P, _I, _I, _I, _I, ctypes.POINTER(ctypes.c_double)],
+    "dg_net_forward_backward_flux": [_P, _P, _P, _I, _I, _I, _I, _I, ctypes.POINTER(ctypes.c_double)],
     "dg_net_adam_step": [_P, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float],
     "dg_net_get_tensor": [_P, _I, _I, _P, ctypes.c_uint64],
     "dg_coarsen": [_P, _P],

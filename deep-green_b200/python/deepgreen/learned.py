@@ -277,15 +277,17 @@ def fit_norm(ps: PairSet, samples: int = 16, crop: int = 48, seed: int = 0) -> N
 
 
 def train(net: Net, ps: PairSet, norm: Norm, steps: int, batch: int = 8, crop: int = 64, lr: float = 1e-3,
-          lr_min: float = 1e-5, seed: int = 0, log_every: int = 100, log=print):
-    """Adam on the MSE of the normalised correction; cosine learning-rate
-    decay from lr to lr_min.  Returns the loss history."""
+          lr_min: float = 1e-5, seed: int = 0, log_every: int = 100, log=print, balance: bool = True):
+    """Adam on the MSE of the normalised correction, each crop weighted by the
+    inverse power of its target when `balance` (so that crops of smooth flow,
+    whose corrections are small, count as much as crops of shear layers);
+    cosine learning-rate decay from lr to lr_min.  Returns the loss history."""
     b = Batcher(ps, batch, crop, seed)
     hist = []
     t0 = time.time()
     for it in range(steps):
         b.fill(norm)
-        loss = net.forward_backward_flux(b.feat, b.tgt)
+        loss = net.forward_backward_flux(b.feat, b.tgt, balance)
         rate = lr_min + 0.5 * (lr - lr_min) * (1.0 + math.cos(math.pi * it / max(steps, 1)))
         net.adam_step(rate)
         hist.append(loss)

@@ -32,14 +32,15 @@ def rel_l1_density(coarse_ctx, truth_ctx):
     return float(np.abs(a - b).sum() / np.abs(b).sum())
 
 
-def training(n_coarse, trajectories, pairs_per_traj, spacing, warmup_max, steps, batch, crop, lr, seed, log=print):
+def training(n_coarse, trajectories, pairs_per_traj, spacing, warmup_max, steps, batch, crop, lr, seed, log=print,
+             balance=True):
     t0 = time.time()
     ps = learned.make_pairs(n_coarse, trajectories, pairs_per_traj, spacing, warmup_max, seed, log=log)
     t_pairs = time.time() - t0
     norm = learned.fit_norm(ps, samples=16, crop=min(48, n_coarse), seed=seed)
     net = Net(learned.INPUTS, learned.OUTPUTS, seed=seed, out_scale=0.1)
     t1 = time.time()
-    hist = learned.train(net, ps, norm, steps, batch=batch, crop=crop, lr=lr, seed=seed, log=log)
+    hist = learned.train(net, ps, norm, steps, batch=batch, crop=crop, lr=lr, seed=seed, log=log, balance=balance)
     t_train = time.time() - t1
     return net, norm, ps, {"pairs": ps.count, "pair_seconds": t_pairs, "train_seconds": t_train,
                            "loss_first": float(np.mean(hist[:20])), "loss_last": float(np.mean(hist[-20:])),
@@ -118,6 +119,10 @@ def main(argv=None):
     ap.add_argument("--save", default=None, help="write the trained network here (JSON)")
     ap.add_argument("--load", default=None, help="skip training, load a network")
     ap.add_argument("--no-eval", action="store_true")
+    ap.add_argument("--no-balance", dest="balance", action="store_false",
+                    help="plain MSE instead of weighing every training crop by its inverse target power")
+    ap.add_argument("--eval-train-res", action="store_true",
+                    help="also evaluate at the training resolution (coarse = the pairs' coarse grid)")
     args = ap.parse_args(argv)
     if args.small:
         cfg = dict(n_coarse=32, traj=[("kh", 11), ("fourier", 12)], ppt=4, spacing=4, warm=8, steps=args.steps or 20,
@@ -126,12 +131,13 @@ def main(argv=None):
         traj = [("kh", 100 + i) for i in range(8)] + [("fourier", 200 + i) for i in range(8)]
         cfg = dict(n_coarse=128, traj=traj, ppt=8, spacing=20, warm=40, steps=args.steps or 2000, batch=8, crop=64,
                    eval_n=256, fine_steps=400)
-    out = {"config": {k: v for k, v in cfg.items() if k != "traj"}, "trajectories": cfg["traj"]}
+    out = {"config": {k: v for k, v in cfg.items() if k != "traj"} | {"balance": args.balance},
+           "trajectories": cfg["traj"]}
     if args.load:
         net, norm, _ = learned.load(args.load)
     else:
         net, norm, ps, tr = training(cfg["n_coarse"], cfg["traj"], cfg["ppt"], cfg["spacing"], cfg["warm"],
-                                     cfg["steps"], cfg["batch"], cfg["crop"], 1e-3, 0)
+                                     cfg["steps"], cfg["batch"], cfg["crop"], 1e-3, 0, balance=args.balance)
         out["training"] = tr
         lt, lz = validation_loss(net, ps, norm, batch=cfg["batch"], crop=cfg["crop"])
         out["training"]["crop_loss_trained"] = lt
@@ -144,6 +150,11 @@ def main(argv=None):
             evaluate_case(net, norm, "kh", 9001, cfg["eval_n"], cfg["fine_steps"], shear=0.5, ratio=2.0),
             evaluate_case(net, norm, "fourier", 9002, cfg["eval_n"], cfg["fine_steps"]),
         ]
+        if args.eval_train_res:
+            out["evaluation_training_resolution"] = [
+                evaluate_case(net, norm, "kh", 9001, cfg["n_coarse"], cfg["fine_steps"] // 2, shear=0.5, ratio=2.0),
+                evaluate_case(net, norm, "fourier", 9002, cfg["n_coarse"], cfg["fine_steps"] // 2),
+            ]
     with open(args.out, "w") as fh:
         json.dump(out, fh, indent=1)
     print(json.dumps({k: v for k, v in out.items() if k != "training"} | {

@@ -116,16 +116,17 @@ class Net:
                                                      ctypes.byref(loss)))
         return loss.value
 
-    def forward_backward_flux(self, feat, target):
+    def forward_backward_flux(self, feat, target, balance=False):
         """Flux-form loss (dg_net_forward_backward_flux): cubic feat of
-        extent x, target FP32 [n][x-9]^3[16]."""
+        extent x, target FP32 [n][x-9]^3[16]; `balance` weighs every batch
+        entry by the inverse power of its target."""
         import torch
         n, x, y, z = self._dims(feat)
         if target.dtype != torch.float32 or tuple(target.shape) != (n, x - 9, y - 9, z - 9, IO_CHANNELS):
             raise ValueError("target must be FP32 [n][x-9][y-9][z-9][16]")
         loss = ctypes.c_double()
         self._check(self.lib.dg_net_forward_backward_flux(self.h, feat.data_ptr(), target.data_ptr(), n, x, y, z,
-                                                          ctypes.byref(loss)))
+                                                          int(bool(balance)), ctypes.byref(loss)))
         return loss.value
 
     def adam_step(self, lr, beta1=0.9, beta2=0.999, eps=1e-8):

@@ -75,9 +75,12 @@ int32_t dg_net_forward_backward(dg_net *net, const void *feat, const float *targ
  * zero wherever the fluxes are uniform.  Cubic crops: feat of extents x^3,
  * network output (x-8)^3, target FP32 [n][x-9][x-9][x-9][16] (first 5
  * channels: the corrections of the cells whose lower faces the output also
- * covers).  Loss = mean over cells and the 5 fields of (dU - target)^2. */
+ * covers).  Loss = mean over cells and the 5 fields of w_b (dU - target)^2,
+ * w_b = 1, or with `balance` = mean target power of the batch / (target power
+ * of entry b + 0.01 x that mean): every crop counts alike, whether its
+ * corrections are large (shear layers) or small (smooth flow). */
 int32_t dg_net_forward_backward_flux(dg_net *net, const void *feat, const float *target, int32_t n, int32_t x,
-                                     int32_t y, int32_t z, double *loss);
+                                     int32_t y, int32_t z, int32_t balance, double *loss);
 
 /* Adam update of all parameters from the stored gradients (bias-corrected,
  * step counter kept by the network). */
