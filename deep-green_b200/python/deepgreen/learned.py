@@ -253,9 +253,18 @@ class Batcher:
                     self.tgt.data_ptr() + i * tstride, stream)
 
 
+# Input channels holding the three components of one vector (momentum, its
+# change over the step, velocity) and the target channels of the momentum.
+VECTOR_INPUTS = ((1, 2, 3), (6, 7, 8), (10, 11, 12))
+VECTOR_TARGETS = ((1, 2, 3),)
+
+
 def fit_norm(ps: PairSet, samples: int = 16, crop: int = 48, seed: int = 0) -> Norm:
     """Per-channel mean / std of the inputs and std of the targets over random
-    crops of the pair set (host statistics of device-made crops)."""
+    crops of the pair set (host statistics of device-made crops).  The three
+    components of a vector share one scale, the largest: a flow whose
+    training states move along x only (a shear layer) still gets a sensible
+    scale for the y and z components, which grow once it rolls up."""
     import torch
     ident = Norm.identity()
     b = Batcher(ps, samples, crop, seed)
@@ -263,16 +272,21 @@ def fit_norm(ps: PairSet, samples: int = 16, crop: int = 48, seed: int = 0) -> N
     torch.cuda.synchronize()
     f = b.feat.float().reshape(-1, IO_CHANNELS).cpu().numpy().astype(np.float64)
     t = b.tgt.reshape(-1, IO_CHANNELS).cpu().numpy().astype(np.float64)
+    in_sd = f.std(axis=0)
+    out_sd = t.std(axis=0)
+    for grp in VECTOR_INPUTS:
+        in_sd[list(grp)] = in_sd[list(grp)].max()
+    for grp in VECTOR_TARGETS:
+        out_sd[list(grp)] = out_sd[list(grp)].max()
     norm = Norm.identity()
     for c in range(16):
         if c < INPUTS:
             norm.in_mean[c] = float(f[:, c].mean())
-            sd = float(f[:, c].std())
-            norm.in_inv_std[c] = 1.0 / sd if sd > 0 else 1.0
+            norm.in_inv_std[c] = 1.0 / float(in_sd[c]) if in_sd[c] > 0 else 1.0
         else:
             norm.in_mean[c] = 0.0
             norm.in_inv_std[c] = 0.0
-        norm.out_std[c] = float(t[:, c].std()) if c < OUTPUTS and t[:, c].std() > 0 else 1.0
+        norm.out_std[c] = float(out_sd[c]) if c < 5 and out_sd[c] > 0 else 1.0
     return norm
 
 
