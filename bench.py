@@ -21,6 +21,18 @@ Keys beside the contract's ones:
                 on the host cores, bounded sample of the same workload.
   clocks        nvidia-smi samples during the timed region.
 
+--case learned: the learned coarse-grid correction end to end -- training
+pairs made by the solver (256^3 fine / 128^3 coarse), 2000 Adam steps of the
+tensor-core network, then held-out KH and Fourier states solved at 256^3 with
+the correction every step against the 512^3 plain solve (400 steps).  Metric:
+time-to-solution ratio (512^3 plain / corrected 256^3), with the L1 density
+errors, fallback rates and the network's forward throughput against the
+measured BF16 peak beside it.  Takes about two minutes.
+
+--case netfwd: the correction network's forward pass alone (4 tcgen05 BF16
+convolutions, random weights) on an (n+8)^3 input, as the corrector runs it
+on an n^3 grid; TFLOP/s against the measured BF16 peak.
+
 --impl reference times the reference's CPU algorithm (the oracle port; the
 Rust crate cannot be built on this image) on the same workload and metric.
 Multi-GPU (torchrun): independent replicas, one 512^3 grid per rank
@@ -57,7 +69,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=512, help="interior cells per axis")
-    ap.add_argument("--case", default="sod", choices=["sod", "vortex", "batch64"])
+    ap.add_argument("--case", default="sod", choices=["sod", "vortex", "batch64", "learned", "netfwd"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -401,6 +413,102 @@ def run_batch(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def run_learned(args, world, rank, local):
+    """Learned coarse-grid correction: train, then time corrected 256^3 solves
+    against the 512^3 plain solve (rank 0; other ranks idle)."""
+    import torch
+    from deepgreen import learned, learned_workload as lw
+    from deepgreen.net import Net
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    quiet = lambda *a: None  # noqa: E731
+    traj = [("kh", 100 + i) for i in range(8)] + [("fourier", 200 + i) for i in range(8)]
+    net, norm, ps, tr = lw.training(128, traj, 8, 20, 40, 2000, 8, 64, 1e-3, 0, log=quiet)
+    del ps
+    cases = [lw.evaluate_case(net, norm, "kh", 9001, 256, 400, log=quiet, shear=0.5, ratio=2.0),
+             lw.evaluate_case(net, norm, "fourier", 9002, 256, 400, log=quiet)]
+    # the network alone at the corrector's shape: 264^3 input -> 256^3 fluxes
+    dev = torch.device("cuda", local)
+    feat = torch.zeros((1, 264, 264, 264, 16), dtype=torch.bfloat16, device=dev)
+    feat[..., :learned.INPUTS] = torch.randn((1, 264, 264, 264, learned.INPUTS), device=dev).to(torch.bfloat16)
+    out = net.forward(feat)
+    net.synchronize()
+    stream = torch.cuda.ExternalStream(net.stream(), device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(5):
+        net.forward(feat, out)
+    e1.record(stream)
+    net.synchronize()
+    fwd_ms = e0.elapsed_time(e1) / 5
+    flop = 2 * 27 * (learned.INPUTS * 32 + 32 * 32 * 2 + 32 * learned.OUTPUTS) * 256 ** 3
+    pk = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = float(pk.get("bf16_tflops", 1590.0))
+    achieved = flop / (fwd_ms * 1e-3) / 1e12
+    ratios = [c["time_ratio_fine_over_learned"] for c in cases]
+    line = {
+        "metric": "time-to-solution ratio (512^3 plain / learned 256^3)", "value": float(np.mean(ratios)),
+        "unit": "x", "n_gpus": 1, "steps": 400, "warmup": 2, "higher_is_better": True, "scaling": "none",
+        "vs_baseline": None, "dtype": "bf16 network, f32 state", "data": "synthetic",
+        "config": {"workload": "learned_correction_256_vs_512", "train": "128^3/256^3 pairs, 2000 x 8 crops of 64^3",
+                   "horizon": "time of 400 steps of the 512^3 grid"},
+        "learned": {"training": {k: v for k, v in tr.items() if k != "loss_history"},
+                    "cases": [{k: c[k] for k in ("kind", "l1_density_plain_coarse", "l1_density_learned_coarse",
+                                                  "fallback_step_rate", "masked_cell_rate", "max_drift",
+                                                  "fine_seconds", "learned_coarse_seconds", "plain_coarse_seconds",
+                                                  "time_ratio_fine_over_learned")} for c in cases]},
+        "e2e": {"value": float(np.mean(ratios)), "unit": "x", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 8},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "kernel": "network forward at 264^3 (4 tcgen05 convolutions), algorithmic FLOP"},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_netfwd(args, world, rank, local):
+    """The correction network's forward pass alone at the corrector's shape."""
+    import torch
+    from deepgreen import learned
+    from deepgreen.net import Net
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n = args.n
+    net = Net(learned.INPUTS, learned.OUTPUTS, seed=1, out_scale=0.1)
+    feat = torch.zeros((1, n + 8, n + 8, n + 8, 16), dtype=torch.bfloat16, device=dev)
+    feat[..., :learned.INPUTS] = torch.randn((1, n + 8, n + 8, n + 8, learned.INPUTS), device=dev).to(torch.bfloat16)
+    out = net.forward(feat)
+    for _ in range(max(args.warmup - 1, 0)):
+        net.forward(feat, out)
+    net.synchronize()
+    stream = torch.cuda.ExternalStream(net.stream(), device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            net.forward(feat, out)
+        e1.record(stream)
+        net.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    flop = 2 * 27 * (learned.INPUTS * 32 + 32 * 32 * 2 + 32 * learned.OUTPUTS) * n ** 3
+    pk = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = float(pk.get("bf16_tflops", 1590.0))
+    achieved = flop / (ms * 1e-3) / 1e12
+    line = {
+        "metric": "network forward TFLOP/s", "value": achieved, "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "none", "vs_baseline": None,
+        "dtype": "bf16", "data": "synthetic",
+        "config": {"workload": f"correction_network_forward_{n}^3", "input": f"{n + 8}^3 x 16 ch",
+                   "layers": "15-32-32-32-15, 3x3x3", "flop_per_cell": flop // n ** 3},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "traffic": None, "peak_source": "measured" if pk else "fallback"},
+        "clocks": clk.summary(), "gpu_launches": 4 * args.steps,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup()
@@ -409,6 +517,10 @@ def main():
             run_reference(args, world, rank)
         elif args.case == "batch64":
             run_batch(args, world, rank, local)
+        elif args.case == "learned":
+            run_learned(args, world, rank, local)
+        elif args.case == "netfwd":
+            run_netfwd(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:
