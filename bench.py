@@ -65,7 +65,7 @@ BYTES_PER_CELL = {"f32": 40, "f64": 80}
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=512, help="interior cells per axis")
@@ -145,24 +145,40 @@ class ClockSampler:
         self.proc = None
 
     def __enter__(self):
+        # start sampling and wait for the first sample, so that the whole
+        # timed region is covered (nvidia-smi takes ~0.1-0.5 s to start)
+        self.lines = []
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
                                           "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
+            return self
+        self.reader = threading.Thread(target=self._read, daemon=True)
+        self.reader.start()
+        t0 = time.time()
+        while not self.lines and time.time() - t0 < 3.0 and self.proc.poll() is None:
+            time.sleep(0.01)
+        self.skip = len(self.lines)          # samples taken before the timed region
         return self
 
+    def _read(self):
+        for l in self.proc.stdout:
+            if l.strip():
+                self.lines.append(l)
+
     def __exit__(self, *a):
-        self.lines = []
         if self.proc:
             self.proc.terminate()
             try:
-                out, _ = self.proc.communicate(timeout=5)
+                self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
-                out, _ = self.proc.communicate()
-            self.lines = [l for l in out.splitlines() if l.strip()]
+                self.proc.wait()
+            self.reader.join(timeout=5)
+            # keep the last pre-region sample (taken within 20 ms of the start) and all later ones
+            self.lines = self.lines[max(self.skip - 1, 0):]
 
     def summary(self):
         sm, mx, reasons = [], None, set()
