@@ -90,11 +90,9 @@ __device__ __forceinline__ void raw_features(const View &b, const View &a, long 
 __global__ void features_kernel(View b, View a, NormDev nm, float inv_vol, float gm1, int ox, int oy, int oz, int ext,
                                 __nv_bfloat16 *__restrict__ out) {
     const long long total = (long long)ext * ext * ext;
-    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < total;
-         v += (long long)gridDim.x * blockDim.x) {
-        const int cz = (int)(v % ext);
-        const int cy = (int)((v / ext) % ext);
-        const int cx = (int)(v / ((long long)ext * ext));
+    for (unsigned v = blockIdx.x * blockDim.x + threadIdx.x; v < (unsigned)total; v += gridDim.x * blockDim.x) {
+        const unsigned row = v / (unsigned)ext;
+        const int cz = (int)(v - row * (unsigned)ext), cy = (int)(row % (unsigned)ext), cx = (int)(row / (unsigned)ext);
         const int x = wrapi(ox + cx, a.n), y = wrapi(oy + cy, a.n), z = wrapi(oz + cz, a.n);
         float f[16];
         raw_features(b, a, vidx(a, x, y, z), inv_vol, gm1, f);
@@ -106,7 +104,7 @@ __global__ void features_kernel(View b, View a, NormDev nm, float inv_vol, float
                                                      (f[c + 1] - nm.in_mean[c + 1]) * nm.in_inv_std[c + 1]);
             u[c >> 1] = *reinterpret_cast<uint32_t *>(&h);
         }
-        uint4 *dst = reinterpret_cast<uint4 *>(out + v * 16);
+        uint4 *dst = reinterpret_cast<uint4 *>(out + (size_t)v * 16);
         dst[0] = w[0];
         dst[1] = w[1];
     }
@@ -115,14 +113,12 @@ __global__ void features_kernel(View b, View a, NormDev nm, float inv_vol, float
 __global__ void targets_kernel(View a, View t, NormDev nm, float inv_vol, int ox, int oy, int oz, int ext,
                                float *__restrict__ out) {
     const long long total = (long long)ext * ext * ext;
-    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < total;
-         v += (long long)gridDim.x * blockDim.x) {
-        const int cz = (int)(v % ext);
-        const int cy = (int)((v / ext) % ext);
-        const int cx = (int)(v / ((long long)ext * ext));
+    for (unsigned v = blockIdx.x * blockDim.x + threadIdx.x; v < (unsigned)total; v += gridDim.x * blockDim.x) {
+        const unsigned row = v / (unsigned)ext;
+        const int cz = (int)(v - row * (unsigned)ext), cy = (int)(row % (unsigned)ext), cx = (int)(row / (unsigned)ext);
         const int x = wrapi(ox + cx, a.n), y = wrapi(oy + cy, a.n), z = wrapi(oz + cz, a.n);
         const long long ia = vidx(a, x, y, z), it = vidx(t, x, y, z);
-        float4 *dst = reinterpret_cast<float4 *>(out + v * 16);
+        float4 *dst = reinterpret_cast<float4 *>(out + (size_t)v * 16);
         float o[8];
 #pragma unroll
         for (int c = 0; c < 5; ++c)
@@ -138,9 +134,9 @@ __global__ void targets_kernel(View a, View t, NormDev nm, float inv_vol, int ox
 // coarse interior cell = sum of its 8 fine cells, per field
 __global__ void coarsen_kernel(View f, float *__restrict__ dst, int pitch, int nyg, long long fstride, int n) {
     const long long total = (long long)n * n * n;
-    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < total;
-         v += (long long)gridDim.x * blockDim.x) {
-        const int z = (int)(v % n), y = (int)((v / n) % n), x = (int)(v / ((long long)n * n));
+    for (unsigned v = blockIdx.x * blockDim.x + threadIdx.x; v < (unsigned)total; v += gridDim.x * blockDim.x) {
+        const unsigned row = v / (unsigned)n;
+        const int z = (int)(v - row * (unsigned)n), y = (int)(row % (unsigned)n), x = (int)(row / (unsigned)n);
         const long long o = ((long long)(x + 2) * nyg + (y + 2)) * pitch + (z + 2);
 #pragma unroll
         for (int c = 0; c < 5; ++c) {
@@ -220,23 +216,33 @@ __global__ void __launch_bounds__(kLearnThreads) correct_kernel(View u1, const f
     const int n = u1.n;
     const long long total = (long long)n * n * n;
     double acc[kCorrVals] = {0, 0, 0, 0, 0, 0};
-    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < total;
-         v += (long long)gridDim.x * blockDim.x) {
-        const int z = (int)(v % n), y = (int)((v / n) % n), x = (int)(v / ((long long)n * n));
+    for (unsigned v = blockIdx.x * blockDim.x + threadIdx.x; v < (unsigned)total; v += gridDim.x * blockDim.x) {
+        const unsigned row = v / (unsigned)n;
+        const int z = (int)(v - row * (unsigned)n), y = (int)(row % (unsigned)n), x = (int)(row / (unsigned)n);
         const long long i = vidx(u1, x, y, z);
-        // divergence of the face fluxes (channel 5 d + c), periodic
-        const long long nn = (long long)n * n;
-        const long long lo[3] = {(long long)(x == 0 ? n - 1 : x - 1) * nn + (long long)y * n + z,
-                                 (long long)x * nn + (long long)(y == 0 ? n - 1 : y - 1) * n + z,
-                                 (long long)x * nn + (long long)y * n + (z == 0 ? n - 1 : z - 1)};
+        // divergence of the face fluxes (channel 5 d + c), periodic; rows of
+        // 16 floats read as float4 / float2 pieces
+        const unsigned nn = (unsigned)n * n;
+        const unsigned lx = (unsigned)(x == 0 ? n - 1 : x - 1) * nn + (unsigned)y * n + z;
+        const unsigned ly = (unsigned)x * nn + (unsigned)(y == 0 ? n - 1 : y - 1) * n + z;
+        const unsigned lz = (unsigned)x * nn + (unsigned)y * n + (z == 0 ? n - 1 : z - 1);
+        const float4 *own = reinterpret_cast<const float4 *>(out) + (size_t)v * 4;
+        const float4 f0 = own[0], f1 = own[1], f2 = own[2], f3 = own[3];
+        const float hi[15] = {f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, f1.z, f1.w,
+                              f2.x, f2.y, f2.z, f2.w, f3.x, f3.y, f3.z};
+        const float4 ax = reinterpret_cast<const float4 *>(out)[(size_t)lx * 4];
+        const float ax4 = out[(size_t)lx * 16 + 4];
+        const float4 ay = reinterpret_cast<const float4 *>(out)[(size_t)ly * 4 + 1];
+        const float2 ay8 = reinterpret_cast<const float2 *>(out)[(size_t)ly * 8 + 4];
+        const float2 az10 = reinterpret_cast<const float2 *>(out)[(size_t)lz * 8 + 5];
+        const float4 az12 = reinterpret_cast<const float4 *>(out)[(size_t)lz * 4 + 3];
+        const float lo_x[5] = {ax.x, ax.y, ax.z, ax.w, ax4};
+        const float lo_y[5] = {ay.y, ay.z, ay.w, ay8.x, ay8.y};
+        const float lo_z[5] = {az10.x, az10.y, az12.x, az12.y, az12.z};
         float o[5];
 #pragma unroll
-        for (int c = 0; c < 5; ++c) {
-            float s = 0.0f;
-#pragma unroll
-            for (int dd = 0; dd < 3; ++dd) s += out[v * 16 + 5 * dd + c] - out[lo[dd] * 16 + 5 * dd + c];
-            o[c] = s;
-        }
+        for (int c = 0; c < 5; ++c)
+            o[c] = ((hi[c] - lo_x[c]) + (hi[5 + c] - lo_y[c])) + (hi[10 + c] - lo_z[c]);
         float d[5], u[5];
         bool ok = true;
 #pragma unroll
@@ -268,15 +274,19 @@ __global__ void __launch_bounds__(kLearnThreads) correct_kernel(View u1, const f
     }
 }
 
-// Uniform in [-1/2, 1/2) from (step, cell, field): SplitMix64 finaliser of a
-// counter (Steele, Lea & Flood 2014).
-__device__ __forceinline__ double dither(unsigned long long step, long long cell, int field) {
-    unsigned long long z = step * 0x9E3779B97F4A7C15ull + (unsigned long long)cell * 8ull + (unsigned long long)field;
+// 64 random bits per (step, cell): SplitMix64 finaliser of a counter
+// (Steele, Lea & Flood 2014); field c takes bits 12c .. 12c+11 as its dither,
+// uniform on 4096 centred levels in (-1/2, 1/2).
+__device__ __forceinline__ unsigned long long cell_bits(unsigned long long step, unsigned long long cell) {
+    unsigned long long z = step * 0x9E3779B97F4A7C15ull + cell;
     z += 0x9E3779B97F4A7C15ull;
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
     z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-    z ^= z >> 31;
-    return (double)(z >> 11) * (1.0 / 9007199254740992.0) - 0.5;
+    return z ^ (z >> 31);
+}
+
+__device__ __forceinline__ double dither(unsigned long long bits, int field) {
+    return ((double)((bits >> (12 * field)) & 4095u) + 0.5) * (1.0 / 4096.0) - 0.5;
 }
 
 // x rounded to FP32 with a dither of one unit in the last place (stochastic
@@ -306,17 +316,18 @@ __global__ void __launch_bounds__(kLearnThreads) apply_kernel(View u1, float *__
     for (int c = 0; c < 5; ++c) mean[c] = ctl->mean[c];
     const unsigned long long step = ctl->steps;
     double acc[kApplyVals] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < total;
-         v += (long long)gridDim.x * blockDim.x) {
-        const int z = (int)(v % n), y = (int)((v / n) % n), x = (int)(v / ((long long)n * n));
+    for (unsigned v = blockIdx.x * blockDim.x + threadIdx.x; v < (unsigned)total; v += gridDim.x * blockDim.x) {
+        const unsigned row = v / (unsigned)n;
+        const int z = (int)(v - row * (unsigned)n), y = (int)(row % (unsigned)n), x = (int)(row / (unsigned)n);
         const long long i = vidx(u1, x, y, z);
         const bool keep = mask[v] != 0;
+        const unsigned long long bits = cell_bits(step, v);
         float u[5];
 #pragma unroll
         for (int c = 0; c < 5; ++c) {
             const float old = u1.p[i + c * u1.fstride];
             u[c] = keep ? old
-                        : round_dithered((double)old + ((double)delta[c * total + v] - mean[c]), dither(step, v, c));
+                        : round_dithered((double)old + ((double)delta[c * total + v] - mean[c]), dither(bits, c));
             dst[i + c * u1.fstride] = u[c];
             acc[c] += (double)u[c] - (double)old;
             acc[5 + c] += fabs((double)old);
@@ -355,9 +366,9 @@ __global__ void fallback_kernel(View u1, float *__restrict__ dst, const CorrCtl 
     if (ctl->fallback == 0) return;
     const int n = u1.n;
     const long long total = (long long)n * n * n;
-    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < total;
-         v += (long long)gridDim.x * blockDim.x) {
-        const int z = (int)(v % n), y = (int)((v / n) % n), x = (int)(v / ((long long)n * n));
+    for (unsigned v = blockIdx.x * blockDim.x + threadIdx.x; v < (unsigned)total; v += gridDim.x * blockDim.x) {
+        const unsigned row = v / (unsigned)n;
+        const int z = (int)(v - row * (unsigned)n), y = (int)(row % (unsigned)n), x = (int)(row / (unsigned)n);
         const long long i = vidx(u1, x, y, z);
 #pragma unroll
         for (int c = 0; c < 5; ++c) dst[i + c * u1.fstride] = u1.p[i + c * u1.fstride];
@@ -433,6 +444,7 @@ int32_t dg_learned_features(const dg_learned_norm *norm, const float *before, co
                             double gamma, int32_t ox, int32_t oy, int32_t oz, int32_t ext, void *feat, void *stream) {
     if (!norm || !before || !after || !feat) return lfail(DG_ERR_INVALID, "null argument");
     if (n < 1 || ext < 1 || !(ds > 0) || !(gamma > 1)) return lfail(DG_ERR_INVALID, "bad extents or constants");
+    if (ext > 1600 || n > 1600) return lfail(DG_ERR_INVALID, "extents above 1600 cells per axis");
     if (reinterpret_cast<uintptr_t>(feat) & 15) return lfail(DG_ERR_INVALID, "feat must be 16-byte aligned");
     const float vol = (float)(ds * ds * ds);
     features_kernel<<<kLearnBlocks, kLearnThreads, 0, static_cast<cudaStream_t>(stream)>>>(
@@ -446,6 +458,7 @@ int32_t dg_learned_targets(const dg_learned_norm *norm, const float *after, cons
                            int32_t ox, int32_t oy, int32_t oz, int32_t ext, float *out, void *stream) {
     if (!norm || !after || !truth || !out) return lfail(DG_ERR_INVALID, "null argument");
     if (n < 1 || ext < 1 || !(ds > 0)) return lfail(DG_ERR_INVALID, "bad extents or constants");
+    if (ext > 1600 || n > 1600) return lfail(DG_ERR_INVALID, "extents above 1600 cells per axis");
     if (reinterpret_cast<uintptr_t>(out) & 15) return lfail(DG_ERR_INVALID, "out must be 16-byte aligned");
     for (int c = 0; c < DG_LEARNED_OUTPUTS; ++c)
         if (!(norm->out_std[c] > 0)) return lfail(DG_ERR_INVALID, "out_std must be positive");
@@ -461,6 +474,7 @@ int32_t dg_corrector_create(dg_ctx *coarse, dg_net *net, const dg_learned_norm *
     *out = nullptr;
     if (coarse->elem != 4 || coarse->exact) return lfail(DG_ERR_INVALID, "the corrector needs the FP32 fast step");
     if (!periodic_cube(coarse)) return lfail(DG_ERR_INVALID, "the corrector needs a cubic, periodic grid");
+    if (coarse->info.nx > 1024) return lfail(DG_ERR_INVALID, "the corrector takes grids of at most 1024^3 cells");
     if (net_inputs(net) != DG_LEARNED_INPUTS || net_outputs(net) != DG_LEARNED_OUTPUTS)
         return lfail(DG_ERR_INVALID, "the network must have 14 inputs and 15 (flux) outputs");
     if (net_device(net) != coarse->info.device) return lfail(DG_ERR_INVALID, "network and grid on different devices");
