@@ -207,6 +207,35 @@ __device__ bool block_sum(double v[K], double *part, unsigned *counter) {
     return last != 0;
 }
 
+// In every thread of the last block: the fixed-order sum of all blocks'
+// partials, thread t taking blocks t, t + blockDim.x, ..., then a shuffle
+// tree and the warps in order; the result is valid in thread 0.
+template <int K>
+__device__ void final_sum(const double *part, double s[K]) {
+    __shared__ double red[kLearnThreads / 32][K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) s[k] = 0.0;
+    const volatile double *vp = part;       // other blocks' partials: not through L1
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+#pragma unroll
+        for (int k = 0; k < K; ++k) s[k] += vp[(size_t)b * K + k];
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s[k] += __shfl_xor_sync(0xffffffffu, s[k], o);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < K; ++k) red[warp][k] = s[k];
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int k = 0; k < K; ++k) {
+            double t = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w][k];
+            s[k] = t;
+        }
+}
+
 // pass 1: raw correction (totals) = divergence of the network's face fluxes,
 // positivity mask, sums for the mean
 __global__ void __launch_bounds__(kLearnThreads) correct_kernel(View u1, const float *__restrict__ out, NormDev nm,
@@ -261,11 +290,10 @@ __global__ void __launch_bounds__(kLearnThreads) correct_kernel(View u1, const f
         }
         acc[5] += ok ? 0.0 : 1.0;
     }
-    if (block_sum<kCorrVals>(acc, part, &ctl->counter) && threadIdx.x == 0) {
-        double s[kCorrVals] = {0, 0, 0, 0, 0, 0};
-        const volatile double *vp = part;   // other blocks' partials: not through L1
-        for (unsigned b = 0; b < gridDim.x; ++b)
-            for (int k = 0; k < kCorrVals; ++k) s[k] += vp[(size_t)b * kCorrVals + k];
+    if (!block_sum<kCorrVals>(acc, part, &ctl->counter)) return;
+    double s[kCorrVals];
+    final_sum<kCorrVals>(part, s);
+    if (threadIdx.x == 0) {
         const double kept = (double)total - s[5];
         for (int c = 0; c < 5; ++c) ctl->mean[c] = kept > 0 ? s[c] / kept : 0.0;
         ctl->masked = (unsigned long long)s[5];
@@ -334,12 +362,10 @@ __global__ void __launch_bounds__(kLearnThreads) apply_kernel(View u1, float *__
         }
         acc[10] += (keep || positive(u, gm1, inv_vol)) ? 0.0 : 1.0;
     }
-    if (block_sum<kApplyVals>(acc, part, &ctl->counter) && threadIdx.x == 0) {
-        double s[kApplyVals];
-        for (int k = 0; k < kApplyVals; ++k) s[k] = 0.0;
-        const volatile double *vp = part;
-        for (unsigned b = 0; b < gridDim.x; ++b)
-            for (int k = 0; k < kApplyVals; ++k) s[k] += vp[(size_t)b * kApplyVals + k];
+    if (!block_sum<kApplyVals>(acc, part, &ctl->counter)) return;
+    double s[kApplyVals];
+    final_sum<kApplyVals>(part, s);
+    if (threadIdx.x == 0) {
         double drift = 0.0;
         for (int c = 0; c < 5; ++c) {
             const double d = s[5 + c] > 0 ? fabs(s[c]) / s[5 + c] : fabs(s[c]);
