@@ -67,7 +67,9 @@ constexpr int kStages = 2;
 constexpr int kConvThreads = 192;          // weight gradient: 6 warps (TMA, MMA, 4 x epilogue)
 constexpr int kIssuers = 2;                // forward: MMA-issuing warps, each with its own accumulators
 constexpr int kFwdThreads = 32 * (1 + kIssuers + 8);   // forward: TMA, issuers, 8 x epilogue
-constexpr int kRing = 8;                   // TMEM accumulator slots (output planes) of the forward kernel
+// Forward kernel: TMEM accumulator slots (output planes) of one issuer's ring;
+// the rings of all issuers fill the 512 TMEM columns.
+template <int COUT> constexpr int fwd_ring() { return 512 / (kIssuers * COUT); }
 constexpr int kSlots = 4;                  // input-plane slots of the forward kernel's shared-memory ring
 constexpr unsigned kNetTimeout = 0x2u;     // status bit: a wait ran out
 
@@ -167,21 +169,23 @@ struct ConvSmem {
     static constexpr int WB = 27 * COUT * ROW;                // weights
     static constexpr int WIN = (kWz * ROW + 1023) / 1024 * 1024;   // one window, 1024-byte aligned
     static constexpr int SLOT = 3 * WIN;                      // the dy windows of one x-plane
-    static constexpr int BYTES = WB + kSlots * SLOT + 512 /*barriers*/ + 1024 /*alignment*/;
+    static constexpr int BYTES = WB + kSlots * SLOT + 1024 /*barriers*/ + 1024 /*alignment*/;
 };
 
 template <int CIN, int COUT, int EPI>
 __global__ void __launch_bounds__(kFwdThreads, 1)
     conv_fwd_kernel(const __grid_constant__ CUtensorMap in_map, const __nv_bfloat16 *__restrict__ wpack, ConvArgs a) {
     static_assert((CIN == 16 || CIN == 32) && (COUT == 16 || COUT == 32), "unsupported channel counts");
-    static_assert(kIssuers == 2, "the MMA split below is written for two issuers");
+    static_assert(kIssuers == 1 || kIssuers == 2, "one or two issuing warps");
     using L = ConvSmem<CIN, COUT>;
     constexpr int KC = CIN / 16;
     constexpr int ROW = L::ROW;
     constexpr int NC = COUT / 2;                 // columns per epilogue warp
     constexpr int NB = 3 * COUT;                 // rows of the weight operand (three dx blocks)
-    constexpr int RING = kRing * COUT;           // TMEM columns of one issuer's ring
-    constexpr uint32_t TCOLS = kIssuers * RING;  // 512 or 256
+    constexpr int R = fwd_ring<COUT>();          // slots of one issuer's ring
+    constexpr int RING = R * COUT;               // TMEM columns of one issuer's ring
+    constexpr uint32_t TCOLS = kIssuers * RING;  // 512
+    static_assert(TCOLS == 512 && R >= 8, "ring layout");
     constexpr uint32_t ID3 = tc::idesc_bf16(kM, 3 * COUT, 0, 0);
     constexpr uint32_t ID2 = tc::idesc_bf16(kM, 2 * COUT, 0, 0);
     constexpr uint32_t ID1 = tc::idesc_bf16(kM, COUT, 0, 0);
@@ -192,8 +196,8 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
     unsigned char *wsm = smem;
     unsigned char *ring = smem + L::WB;
     uint64_t *bars = reinterpret_cast<uint64_t *>(ring + kSlots * L::SLOT);
-    uint64_t *full = bars, *empty = bars + kSlots, *tfull = bars + 2 * kSlots, *tempty = tfull + kRing,
-             *wbar = tempty + kRing, *drain = wbar + 1;
+    uint64_t *full = bars, *empty = bars + kSlots, *tfull = bars + 2 * kSlots, *tempty = tfull + R,
+             *wbar = tempty + R, *drain = wbar + 1;
     uint32_t *tslot = reinterpret_cast<uint32_t *>(drain + kIssuers);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -202,7 +206,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
             mbar_init(full + i, 1);
             mbar_init(empty + i, kIssuers);
         }
-        for (int i = 0; i < kRing; ++i) {
+        for (int i = 0; i < R; ++i) {
             mbar_init(tfull + i, kIssuers);
             mbar_init(tempty + i, 8);
         }
@@ -222,7 +226,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
         float zero[NC];
 #pragma unroll
         for (int c = 0; c < NC; ++c) zero[c] = 0.0f;
-        for (int sl = 0; sl < kIssuers * kRing; ++sl) {
+        for (int sl = 0; sl < kIssuers * R; ++sl) {
             const uint32_t ta = tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)(sl * COUT + c0);
             if constexpr (NC == 16) tc::tmem_st16(ta, zero);
             else tc::tmem_st8(ta, zero);
@@ -266,44 +270,45 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
             ok &= tc::mbar_sleep_wait(wbar, 0, kWaitBudget);
         }
     } else if (warp <= kIssuers) {
-        if (lane == 0) {
-            const int me = warp - 1;              // issuer index: its half of the MMAs, its ring
-            ok = tc::mbar_sleep_wait(wbar, 0, kWaitBudget);
-            long long g = 0;                      // input planes consumed = output slots completed
-            const uint64_t b0 = tc::sdesc_sw(smem_u32(wsm), ROW);
-            const uint32_t rbase = tbase + (uint32_t)(me * RING);
-            for (int unit = blockIdx.x; ok && unit < a.nunits; unit += gridDim.x) {
-                const int xc = unit % a.nxc;
-                const int len = min(a.xchunk, a.xo - xc * a.xchunk);
-                for (int k = 0; k < len + 2; ++k, ++g) {
-                    const int ps = (int)(g % kSlots);
-                    if (!tc::mbar_sleep_wait(full + ps, (uint32_t)((g / kSlots) & 1), kWaitBudget)) {
-                        ok = false;
-                        break;
-                    }
-                    // the third block writes output slot g+2 first: its previous
-                    // occupant must have been drained and zeroed
-                    const long long w2 = g + 2;
-                    if (w2 >= kRing && !tc::mbar_sleep_wait(tempty + (int)(w2 % kRing),
-                                                            (uint32_t)((w2 / kRing - 1) & 1), kWaitBudget)) {
-                        ok = false;
-                        break;
-                    }
-                    tc::fence_after();
-                    const int s0 = (int)(g % kRing);
-                    const uint32_t d0 = rbase + (uint32_t)(s0 * COUT);
-                    // descriptors advance by (byte offset >> 4) in their 14-bit address field;
-                    // every address stays below 256 KB, so no carry leaves the field
-                    const uint64_t a0 = tc::sdesc_sw(smem_u32(ring + ps * L::SLOT), ROW);
-                    // this issuer's MMAs: channel half kc = me (CIN 32) or taps 0-4 / 5-8 (CIN 16)
-                    constexpr int T9N = KC == 2 ? 9 : 5;
-                    const int t9lo = KC == 2 ? 0 : me * 5;
-                    const int t9hi = KC == 2 ? 9 : (me ? 9 : 5);
-                    const int kc = KC == 2 ? me : 0;
-                    if (s0 <= kRing - 3) {
+        // The whole warp runs the issue loop and one elected lane issues each
+        // plane's MMAs and commits (see elect_one).
+        const int me = warp - 1;              // issuer index: its half of the MMAs, its ring
+        ok = warp_wait(wbar, 0);
+        long long g = 0;                      // input planes consumed = output slots completed
+        const uint64_t b0 = tc::sdesc_sw(smem_u32(wsm), ROW);
+        const uint32_t rbase = tbase + (uint32_t)(me * RING);
+        for (int unit = blockIdx.x; ok && unit < a.nunits; unit += gridDim.x) {
+            const int xc = unit % a.nxc;
+            const int len = min(a.xchunk, a.xo - xc * a.xchunk);
+            for (int k = 0; k < len + 2; ++k, ++g) {
+                const int ps = (int)(g % kSlots);
+                bool got = tc::mbar_sleep_wait(full + ps, (uint32_t)((g / kSlots) & 1), kWaitBudget);
+                // the third block writes output slot g+2 first: its previous
+                // occupant must have been drained and zeroed
+                const long long w2 = g + 2;
+                if (got && w2 >= R)
+                    got = tc::mbar_sleep_wait(tempty + (int)(w2 % R), (uint32_t)((w2 / R - 1) & 1), kWaitBudget);
+                if (!__all_sync(0xffffffffu, got)) {
+                    ok = false;
+                    break;
+                }
+                tc::fence_after();
+                const int s0 = (int)(g % R);
+                const uint32_t d0 = rbase + (uint32_t)(s0 * COUT);
+                // descriptors advance by (byte offset >> 4) in their 14-bit address field;
+                // every address stays below 256 KB, so no carry leaves the field
+                const uint64_t a0 = tc::sdesc_sw(smem_u32(ring + ps * L::SLOT), ROW);
+                // this issuer's MMAs: every (tap, channel half) with one issuer; with
+                // two, channel half kc = me (CIN 32) or taps 0-4 / 5-8 (CIN 16)
+                constexpr int NT = kIssuers == 1 ? 9 * KC : (KC == 2 ? 9 : 5);
+                const int t9lo = (kIssuers == 2 && KC == 1) ? me * 5 : 0;
+                const int t9hi = (kIssuers == 2 && KC == 1) ? (me ? 9 : 5) : 9;
+                const int kc0 = (kIssuers == 2 && KC == 2) ? me : 0;
+                if (tc::elect_one()) {
+                    if (s0 <= R - 3) {
 #pragma unroll
-                        for (int j = 0; j < T9N; ++j) {
-                            const int t9 = t9lo + j;
+                        for (int j = 0; j < NT; ++j) {
+                            const int t9 = t9lo + j % 9, kc = kc0 + j / 9;
                             if (t9 >= t9hi) break;
                             const int dy = t9 / 3, dz = t9 % 3;
                             const uint64_t ad = a0 + (uint32_t)((dy * L::WIN + dz * ROW + kc * 32) >> 4);
@@ -312,12 +317,12 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
                         }
                     } else {
                         // the three blocks would wrap the ring: two MMAs each
-                        const int n1 = kRing - s0;
+                        const int n1 = R - s0;
                         const uint32_t i1 = n1 == 2 ? ID2 : ID1, i2 = n1 == 2 ? ID1 : ID2;
                         const uint32_t bo2 = (uint32_t)((n1 * COUT * ROW) >> 4);
 #pragma unroll
-                        for (int j = 0; j < T9N; ++j) {
-                            const int t9 = t9lo + j;
+                        for (int j = 0; j < NT; ++j) {
+                            const int t9 = t9lo + j % 9, kc = kc0 + j / 9;
                             if (t9 >= t9hi) break;
                             const int dy = t9 / 3, dz = t9 % 3;
                             const uint64_t ad = a0 + (uint32_t)((dy * L::WIN + dz * ROW + kc * 32) >> 4);
@@ -326,13 +331,15 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
                             tc::mma_bf16(rbase, ad, bd + bo2, i2, 1u);
                         }
                     }
-                    tc::commit(empty + ps);               // input plane g is not needed again
-                    tc::commit(tfull + s0);               // output slot g is complete
+                    tc::commit(empty + ps);           // input plane g is not needed again
+                    tc::commit(tfull + s0);           // output slot g is complete
                 }
+                __syncwarp();
             }
-            tc::commit(drain + me);
-            ok &= tc::mbar_sleep_wait(drain + me, 0, kWaitBudget);
         }
+        if (tc::elect_one()) tc::commit(drain + me);
+        __syncwarp();
+        ok &= warp_wait(drain + me, 0);
     } else {
         long long g = 0;
         for (int unit = blockIdx.x; ok && unit < a.nunits; unit += gridDim.x) {
@@ -343,8 +350,8 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
             const int y = p / a.zi, z = p - y * a.zi;
             const bool valid = y < a.yo && z < a.zo;
             for (int k = 0; k < len + 2; ++k, ++g) {
-                const int sl = (int)(g % kRing);
-                if (!warp_wait(tfull + sl, (uint32_t)((g / kRing) & 1))) {
+                const int sl = (int)(g % R);
+                if (!warp_wait(tfull + sl, (uint32_t)((g / R) & 1))) {
                     ok = false;
                     break;
                 }
@@ -355,16 +362,16 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
                 const uint32_t ta = tbase + ((uint32_t)(32 * q) << 16) + (uint32_t)(sl * COUT + c0);
                 if constexpr (NC == 16) {
                     tc::tmem_ld16(ta, v);
-                    tc::tmem_ld16(ta + RING, v2);
+                    if constexpr (kIssuers == 2) tc::tmem_ld16(ta + RING, v2);
                     tc::tmem_wait_ld();
                     tc::tmem_st16(ta, zero);
-                    tc::tmem_st16(ta + RING, zero);
+                    if constexpr (kIssuers == 2) tc::tmem_st16(ta + RING, zero);
                 } else {
                     tc::tmem_ld8(ta, v);
-                    tc::tmem_ld8(ta + RING, v2);
+                    if constexpr (kIssuers == 2) tc::tmem_ld8(ta + RING, v2);
                     tc::tmem_wait_ld();
                     tc::tmem_st8(ta, zero);
-                    tc::tmem_st8(ta + RING, zero);
+                    if constexpr (kIssuers == 2) tc::tmem_st8(ta + RING, zero);
                 }
                 tc::tmem_wait_st();
                 tc::fence_before();
@@ -373,8 +380,9 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
                 // slot g holds output plane x0 + k - 2 of this chunk when k >= 2;
                 // the first two slots of a chunk mix planes of two chunks
                 if (k < 2 || !valid) continue;
+                if constexpr (kIssuers == 2)
 #pragma unroll
-                for (int c = 0; c < NC; ++c) v[c] += v2[c];
+                    for (int c = 0; c < NC; ++c) v[c] += v2[c];
 
                 const int x = x0 + k - 2;
                 const long long o =

@@ -346,11 +346,8 @@ cudaError_t launch_conv(dg_net *net, const void *in, int nb, int xi, int yi, int
     auto kern = conv_fwd_kernel<CIN, COUT, EPI>;
     static std::once_flag once;
     static cudaError_t attr_err = cudaSuccess;
-    static int occ = 1;
     std::call_once(once, [&] {
         attr_err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::BYTES);
-        if (attr_err == cudaSuccess)
-            attr_err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kFwdThreads, L::BYTES);
     });
     if (attr_err != cudaSuccess) return attr_err;
     CUtensorMap m;
@@ -360,7 +357,7 @@ cudaError_t launch_conv(dg_net *net, const void *in, int nb, int xi, int yi, int
     a.xo = xi - 2; a.yo = yi - 2; a.zo = zi - 2;
     a.tpp = (a.yo * zi + kM - 1) / kM;
     // blocks holding all 512 TMEM columns cannot share an SM
-    const int per_sm = kIssuers * kRing * COUT > 256 ? 1 : std::max(1, occ);
+    const int per_sm = 1;
     const int slots = per_sm * net->nsm;
     // longest x chunk (fewest re-loaded planes) that still gives every block
     // a few work units

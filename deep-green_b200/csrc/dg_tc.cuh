@@ -58,6 +58,19 @@ __device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b
         : "memory");
 }
 
+// One lane of a converged warp (the lowest active one) gets true.  Issuing
+// tcgen05 work under this predicate keeps the issue loop on the warp's
+// uniform datapath; under `lane == 0` the same loop issues ~25% slower.
+__device__ __forceinline__ bool elect_one() {
+    uint32_t pred = 0;
+    asm volatile(
+        "{\n\t.reg .pred P;\n\t"
+        "elect.sync _|P, 0xffffffff;\n\t"
+        "selp.b32 %0, 1, 0, P;\n\t}"
+        : "=r"(pred));
+    return pred != 0;
+}
+
 // Arrive (once) on an mbarrier when all tcgen05 operations issued so far by
 // this thread have completed.
 __device__ __forceinline__ void commit(uint64_t *bar) {
@@ -134,6 +147,18 @@ __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.
 // after ~`budget` SM clocks.
 __device__ __forceinline__ bool mbar_sleep_wait(uint64_t *bar, uint32_t parity, long long budget) {
     const uint32_t addr = smem_u32(bar);
+    {
+        // fast path: a phase that already completed costs one non-blocking test
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(addr), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
     const long long t0 = clock64();
     while (true) {
         uint32_t ok;
