@@ -11,6 +11,7 @@
 #include <string>
 
 #include "../../include/deepgreen_net.h"
+#include "dg_common.cuh"
 #include "dg_ctx.h"
 #include "dg_net_impl.h"
 
@@ -169,7 +170,6 @@ struct CorrCtl {
 };
 
 constexpr int kCorrVals = 6;   // per-block partials of the correction pass
-constexpr int kApplyVals = 11; // per-block partials of the apply pass
 
 __device__ __forceinline__ bool positive(const float u[5], float gm1, float inv_vol) {
     const float r = u[0] * inv_vol;
@@ -208,17 +208,18 @@ __device__ bool block_sum(double v[K], double *part, unsigned *counter) {
 }
 
 // In every thread of the last block: the fixed-order sum of all blocks'
-// partials, thread t taking blocks t, t + blockDim.x, ..., then a shuffle
-// tree and the warps in order; the result is valid in thread 0.
-template <int K>
-__device__ void final_sum(const double *part, double s[K]) {
+// partials (the first K of each block's KP values), thread t taking blocks
+// t, t + blockDim.x, ..., then a shuffle tree and the warps in order; the
+// result is valid in thread 0.
+template <int K, int KP>
+__device__ void final_sum_strided(const double *part, double s[K]) {
     __shared__ double red[kLearnThreads / 32][K];
 #pragma unroll
     for (int k = 0; k < K; ++k) s[k] = 0.0;
-    const volatile double *vp = part;       // other blocks' partials: not through L1
+    const volatile double *vp = part;
     for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
 #pragma unroll
-        for (int k = 0; k < K; ++k) s[k] += vp[(size_t)b * K + k];
+        for (int k = 0; k < K; ++k) s[k] += vp[(size_t)b * KP + k];
 #pragma unroll
     for (int k = 0; k < K; ++k)
 #pragma unroll
@@ -292,7 +293,7 @@ __global__ void __launch_bounds__(kLearnThreads) correct_kernel(View u1, const f
     }
     if (!block_sum<kCorrVals>(acc, part, &ctl->counter)) return;
     double s[kCorrVals];
-    final_sum<kCorrVals>(part, s);
+    final_sum_strided<kCorrVals, kCorrVals>(part, s);
     if (threadIdx.x == 0) {
         const double kept = (double)total - s[5];
         for (int c = 0; c < 5; ++c) ctl->mean[c] = kept > 0 ? s[c] / kept : 0.0;
@@ -332,73 +333,180 @@ __device__ __forceinline__ float round_dithered(double x, double h) {
     return (float)(x + h * ulp);
 }
 
-// pass 2: corrected state into dst, conservation and positivity check
+constexpr int kApplyVals = 16;  // per-block partials of the apply pass (+ the wave-speed maximum)
+
+// Ghosted coordinate of the periodic image of interior coordinate c
+// (0..n-1), or -1: cells 0, 1 reappear as ghosts n+2, n+3 and cells n-2,
+// n-1 as ghosts 0, 1 (the copies fill_ghosts makes on a periodic axis).
+__device__ __forceinline__ int periodic_image(int c, int n) {
+    return c < 2 ? c + 2 + n : (c >= n - 2 ? c + 2 - n : -1);
+}
+
+// Stores of one corrected z-quad (4 cells, z0 % 4 == 0) of field c at
+// interior row (x, y), with the periodic ghost images of cells next to a face.
+__device__ __forceinline__ void store_quad(float *dst, const View &v, int x, int y, int z0, int c, float q0,
+                                           float q1, float q2, float q3) {
+    const int n = v.n;
+    float *f = dst + c * v.fstride;
+    const int xi = periodic_image(x, n), yi = periodic_image(y, n);
+    const bool zlo = z0 == 0, zhi = z0 == n - 4;
+    if (xi < 0 && yi < 0 && !zlo && !zhi) {
+        float *row = f + ((long long)(x + 2) * v.nyg + (y + 2)) * v.pitch;
+        *reinterpret_cast<float2 *>(row + z0 + 2) = make_float2(q0, q1);
+        *reinterpret_cast<float2 *>(row + z0 + 4) = make_float2(q2, q3);
+        return;
+    }
+    for (int a = 0; a < 2; ++a) {
+        const int gx = a ? xi : x + 2;
+        if (gx < 0) continue;
+        for (int b = 0; b < 2; ++b) {
+            const int gy = b ? yi : y + 2;
+            if (gy < 0) continue;
+            float *row = f + ((long long)gx * v.nyg + gy) * v.pitch;
+            *reinterpret_cast<float2 *>(row + z0 + 2) = make_float2(q0, q1);
+            *reinterpret_cast<float2 *>(row + z0 + 4) = make_float2(q2, q3);
+            if (zlo) {
+                row[n + 2] = q0;
+                row[n + 3] = q1;
+            }
+            if (zhi) {
+                row[0] = q2;
+                row[1] = q3;
+            }
+        }
+    }
+}
+
+// pass 2: the corrected state into dst (interior and periodic ghosts),
+// conservation and positivity check, and the corrected state's dt (the
+// fast policy's CFL * ds / max(c_s + |v|), as the plain step's own
+// reduction computes it).  One thread per z-quad; n % 4 == 0.
 __global__ void __launch_bounds__(kLearnThreads) apply_kernel(View u1, float *__restrict__ dst,
                                                               const float *__restrict__ delta,
-                                                              const uint8_t *__restrict__ mask, float gm1,
-                                                              float inv_vol, double tol, double *part, CorrCtl *ctl) {
+                                                              const uint8_t *__restrict__ mask, GridArgs<float> g,
+                                                              double tol, double *part, CorrCtl *ctl) {
     const int n = u1.n;
-    const long long total = (long long)n * n * n;
+    const unsigned nq = (unsigned)n / 4, total = (unsigned)n * n * n, quads = total / 4;
     double mean[5];
 #pragma unroll
     for (int c = 0; c < 5; ++c) mean[c] = ctl->mean[c];
     const unsigned long long step = ctl->steps;
-    double acc[kApplyVals] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (unsigned v = blockIdx.x * blockDim.x + threadIdx.x; v < (unsigned)total; v += gridDim.x * blockDim.x) {
-        const unsigned row = v / (unsigned)n;
-        const int z = (int)(v - row * (unsigned)n), y = (int)(row % (unsigned)n), x = (int)(row / (unsigned)n);
-        const long long i = vidx(u1, x, y, z);
-        const bool keep = mask[v] != 0;
-        const unsigned long long bits = cell_bits(step, v);
-        float u[5];
+    // acc: 0-4 sum of u - old, 5-9 sum |old|, 10 positivity violations, 11-15 sum old
+    double acc[kApplyVals];
+#pragma unroll
+    for (int k = 0; k < kApplyVals; ++k) acc[k] = 0.0;
+    float smax = 0.0f;
+    for (unsigned qd = blockIdx.x * blockDim.x + threadIdx.x; qd < quads; qd += gridDim.x * blockDim.x) {
+        const unsigned row = qd / nq;
+        const int z0 = (int)(qd - row * nq) * 4, y = (int)(row % (unsigned)n), x = (int)(row / (unsigned)n);
+        const unsigned v = row * (unsigned)n + (unsigned)z0;
+        const long long i = vidx(u1, x, y, z0);
+        const uchar4 mk = *reinterpret_cast<const uchar4 *>(mask + v);
+        const bool keep[4] = {mk.x != 0, mk.y != 0, mk.z != 0, mk.w != 0};
+        float old[5][4], d[5][4], u[5][4];
 #pragma unroll
         for (int c = 0; c < 5; ++c) {
-            const float old = u1.p[i + c * u1.fstride];
-            u[c] = keep ? old
-                        : round_dithered((double)old + ((double)delta[c * total + v] - mean[c]), dither(bits, c));
-            dst[i + c * u1.fstride] = u[c];
-            acc[c] += (double)u[c] - (double)old;
-            acc[5 + c] += fabs((double)old);
+            const float2 a0 = *reinterpret_cast<const float2 *>(u1.p + i + c * u1.fstride);
+            const float2 a1 = *reinterpret_cast<const float2 *>(u1.p + i + c * u1.fstride + 2);
+            const float4 dd = *reinterpret_cast<const float4 *>(delta + (size_t)c * total + v);
+            old[c][0] = a0.x; old[c][1] = a0.y; old[c][2] = a1.x; old[c][3] = a1.y;
+            d[c][0] = dd.x; d[c][1] = dd.y; d[c][2] = dd.z; d[c][3] = dd.w;
         }
-        acc[10] += (keep || positive(u, gm1, inv_vol)) ? 0.0 : 1.0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const unsigned long long bits = cell_bits(step, v + j);
+            float w[5], cu[5];
+#pragma unroll
+            for (int c = 0; c < 5; ++c) {
+                const double o = (double)old[c][j];
+                u[c][j] = keep[j] ? old[c][j] : round_dithered(o + ((double)d[c][j] - mean[c]), dither(bits, c));
+                cu[c] = u[c][j];
+                acc[c] += (double)u[c][j] - o;
+                acc[5 + c] += fabs(o);
+                acc[11 + c] += o;
+            }
+            acc[10] += (keep[j] || positive(cu, g.k.gm1, g.k.inv_vol)) ? 0.0 : 1.0;
+            Phys<float, false>::prim(cu, w, g.k);
+            smax = max_nan(smax, fast_speed(w[0], w[1], w[2], w[3], w[4], g.k.gamma));
+        }
+#pragma unroll
+        for (int c = 0; c < 5; ++c) store_quad(dst, u1, x, y, z0, c, u[c][0], u[c][1], u[c][2], u[c][3]);
     }
-    if (!block_sum<kApplyVals>(acc, part, &ctl->counter)) return;
-    double s[kApplyVals];
-    final_sum<kApplyVals>(part, s);
+    // block partials: the sums, then the wave-speed maximum (NaN-propagating)
+    __shared__ double red[kLearnThreads / 32][kApplyVals + 1];
+    __shared__ int last;
+#pragma unroll
+    for (int k = 0; k < kApplyVals; ++k)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) smax = max_nan(smax, __shfl_xor_sync(0xffffffffu, smax, o));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < kApplyVals; ++k) red[warp][k] = acc[k];
+        red[warp][kApplyVals] = (double)smax;
+    }
+    __syncthreads();
+    constexpr int KP = kApplyVals + 1;
     if (threadIdx.x == 0) {
-        double drift = 0.0;
-        for (int c = 0; c < 5; ++c) {
-            const double d = s[5 + c] > 0 ? fabs(s[c]) / s[5 + c] : fabs(s[c]);
-            ctl->last_field_drift[c] = d;
-            drift = fmax(drift, d);
+        for (int k = 0; k < KP; ++k) {
+            double t = k < kApplyVals ? 0.0 : red[0][k];
+            for (int w = k < kApplyVals ? 0 : 1; w < (int)(blockDim.x >> 5); ++w)
+                t = k < kApplyVals ? t + red[w][k] : (double)max_nan((float)t, (float)red[w][k]);
+            part[(size_t)blockIdx.x * KP + k] = t;
         }
-        ctl->last_drift = drift;
-        ctl->violations += (unsigned long long)s[10];
-        const bool fb = s[10] > 0.0 || !(drift <= tol);
-        ctl->fallback = fb ? 1u : 0u;
-        ctl->steps += 1;
-        if (fb) ctl->fallbacks += 1;
-        else {
-            ctl->masked_total += ctl->masked;
-            ctl->max_drift = fmax(ctl->max_drift, drift);
-        }
-        ctl->counter = 0;
         __threadfence();
+        last = atomicAdd(&ctl->counter, 1u) == gridDim.x - 1;
     }
+    __syncthreads();
+    if (!last) return;
+    double s[kApplyVals];
+    final_sum_strided<kApplyVals, KP>(part, s);
+    __shared__ float smw[kLearnThreads / 32];
+    const volatile double *vp = part;
+    float sm = 0.0f;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) sm = max_nan(sm, (float)vp[(size_t)b * KP + kApplyVals]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sm = max_nan(sm, __shfl_xor_sync(0xffffffffu, sm, o));
+    if (lane == 0) smw[warp] = sm;
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) sm = max_nan(sm, smw[w]);
+    double drift = 0.0;
+    for (int c = 0; c < 5; ++c) {
+        const double dr = s[5 + c] > 0 ? fabs(s[c]) / s[5 + c] : fabs(s[c]);
+        ctl->last_field_drift[c] = dr;
+        drift = fmax(drift, dr);
+    }
+    ctl->last_drift = drift;
+    ctl->violations += (unsigned long long)s[10];
+    const bool fb = s[10] > 0.0 || !(drift <= tol);
+    ctl->fallback = fb ? 1u : 0u;
+    ctl->steps += 1;
+    if (fb) {
+        ctl->fallbacks += 1;     // the plain step's dt stays
+    } else {
+        ctl->masked_total += ctl->masked;
+        ctl->max_drift = fmax(ctl->max_drift, drift);
+        // dt of the coming step from the kept state (kSetDt of the state reduction)
+        DevCtl *dc = g.ctl;
+        const bool nn = sm != sm;
+        const float w = __fdiv_rn(g.k.ds, sm);
+        dc->dt[dc->step & 1] = (double)(nn ? g.k.cfl * 1.0f : g.k.cfl * w);
+        if (nn) dc->flags |= kStatusNonFinite;
+    }
+    ctl->counter = 0;
+    __threadfence();
 }
 
-// pass 3 (only when the step falls back): dst := plain state
-__global__ void fallback_kernel(View u1, float *__restrict__ dst, const CorrCtl *ctl) {
+// pass 3 (only when the step falls back): dst := the plain state, ghosts included
+__global__ void fallback_kernel(const float *__restrict__ src, float *__restrict__ dst, long long count,
+                                const CorrCtl *ctl) {
     if (ctl->fallback == 0) return;
-    const int n = u1.n;
-    const long long total = (long long)n * n * n;
-    for (unsigned v = blockIdx.x * blockDim.x + threadIdx.x; v < (unsigned)total; v += gridDim.x * blockDim.x) {
-        const unsigned row = v / (unsigned)n;
-        const int z = (int)(v - row * (unsigned)n), y = (int)(row % (unsigned)n), x = (int)(row / (unsigned)n);
-        const long long i = vidx(u1, x, y, z);
-#pragma unroll
-        for (int c = 0; c < 5; ++c) dst[i + c * u1.fstride] = u1.p[i + c * u1.fstride];
-    }
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < count;
+         e += (long long)gridDim.x * blockDim.x)
+        dst[e] = src[e];
 }
 
 NormDev to_dev(const dg_learned_norm *n) {
@@ -501,6 +609,7 @@ int32_t dg_corrector_create(dg_ctx *coarse, dg_net *net, const dg_learned_norm *
     if (coarse->elem != 4 || coarse->exact) return lfail(DG_ERR_INVALID, "the corrector needs the FP32 fast step");
     if (!periodic_cube(coarse)) return lfail(DG_ERR_INVALID, "the corrector needs a cubic, periodic grid");
     if (coarse->info.nx > 1024) return lfail(DG_ERR_INVALID, "the corrector takes grids of at most 1024^3 cells");
+    if (coarse->info.nx % 4 != 0) return lfail(DG_ERR_INVALID, "the corrector needs n divisible by 4");
     if (net_inputs(net) != DG_LEARNED_INPUTS || net_outputs(net) != DG_LEARNED_OUTPUTS)
         return lfail(DG_ERR_INVALID, "the network must have 14 inputs and 15 (flux) outputs");
     if (net_device(net) != coarse->info.device) return lfail(DG_ERR_INVALID, "network and grid on different devices");
@@ -518,7 +627,7 @@ int32_t dg_corrector_create(dg_ctx *coarse, dg_net *net, const dg_learned_norm *
     if (e == cudaSuccess) e = cudaMalloc(&k->out, (size_t)cells * 16 * 4);
     if (e == cudaSuccess) e = cudaMalloc(&k->delta, (size_t)cells * 5 * 4);
     if (e == cudaSuccess) e = cudaMalloc(&k->mask, (size_t)cells);
-    if (e == cudaSuccess) e = cudaMalloc(&k->part, (size_t)kLearnBlocks * kApplyVals * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&k->part, (size_t)kLearnBlocks * (kApplyVals + 1) * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&k->ctl, sizeof(CorrCtl));
     if (e == cudaSuccess) e = cudaMemset(k->ctl, 0, sizeof(CorrCtl));
     if (e != cudaSuccess) {
@@ -571,14 +680,12 @@ int32_t dg_corrector_step(dg_corrector *k, int32_t nsteps) {
         correct_kernel<<<kLearnBlocks, kLearnThreads, 0, c->stream>>>(u1, k->out, k->norm, vol, 1.0f / vol, gm1,
                                                                        k->delta, k->mask, k->part, k->ctl);
         float *dst = static_cast<float *>(c->buf[other]);
-        apply_kernel<<<kLearnBlocks, kLearnThreads, 0, c->stream>>>(u1, dst, k->delta, k->mask, gm1, 1.0f / vol,
-                                                                     k->tol, k->part, k->ctl);
-        fallback_kernel<<<kLearnBlocks, kLearnThreads, 0, c->stream>>>(u1, dst, k->ctl);
+        apply_kernel<<<kLearnBlocks, kLearnThreads, 0, c->stream>>>(u1, dst, k->delta, k->mask,
+                                                                     grid_args<float>(c, dst, dst), k->tol, k->part,
+                                                                     k->ctl);
+        fallback_kernel<<<kLearnBlocks, kLearnThreads, 0, c->stream>>>(static_cast<const float *>(c->buf[cur]), dst,
+                                                                        5 * c->fstride, k->ctl);
         DG_CUDA(c, cudaGetLastError());
-        auto a = grid_args<float>(c, dst, dst);
-        cudaError_t e = launch_fill_ghosts<float>(a, dst, c->stream);
-        if (e == cudaSuccess) e = launch_reduce_policy<float, false>(a, 1 /* dt of the coming step */, c->stream);
-        if (e != cudaSuccess) return cuda_fail(c, e, "corrector ghosts / dt");
         c->cur = other;
     }
     return DG_OK;

@@ -469,9 +469,19 @@ __global__ void __launch_bounds__(256) reduce_kernel(const GridArgs<T> a, int se
     double wm = INFINITY;
     unsigned nanf = 0;
     float smax = 0.0f;   // fast policy: max wave speed (NaN-propagating)
-    for (long long c = blockIdx.x * 256LL + tid; c < total; c += (long long)gridDim.x * 256) {
-        const long long x = c / (nyi * nzi) + 2, y = (c / nzi) % nyi + 2, z = c % nzi + 2;
-        const long long o = (x * a.ny + y) * a.pitch + z;
+    // the cells c = blockIdx.x * 256 + tid + k * stride, with (x, y, z)
+    // advanced by the stride's own decomposition (no division per cell)
+    const long long stride = (long long)gridDim.x * 256;
+    long long c = blockIdx.x * 256LL + tid;
+    int x = (int)(c / (nyi * nzi)), y = (int)((c / nzi) % nyi), z = (int)(c % nzi);
+    const int sx = (int)(stride / (nyi * nzi)), sy = (int)((stride / nzi) % nyi), sz = (int)(stride % nzi);
+    for (; c < total; c += stride) {
+        const long long o = ((long long)(x + 2) * a.ny + (y + 2)) * a.pitch + (z + 2);
+        z += sz;
+        if (z >= nzi) { z -= (int)nzi; ++y; }
+        y += sy;
+        if (y >= nyi) { y -= (int)nyi; ++x; }
+        x += sx;
         T u[5], w[5];
         for (int f = 0; f < 5; ++f) u[f] = a.src[f * a.fstride + o];
         Phys<T, EXACT>::prim(u, w, a.k);
@@ -521,15 +531,42 @@ __global__ void __launch_bounds__(256) reduce_kernel(const GridArgs<T> a, int se
 }
 
 // Copy every ghost cell of buf from its interior source (boundary rules).
+// Ghost cell e (0 .. ghost_cells - 1) as ghosted coordinates: the two
+// layers of each x face (4 ny nz cells), then those of each y face over the
+// interior x (4 (nx-4) nz), then those of each z face over the interior x, y
+// (4 (nx-4)(ny-4)).
+__device__ __forceinline__ void ghost_cell(long long e, int nx, int ny, int nz, int &x, int &y, int &z) {
+    const long long fx = 4LL * ny * nz, fy = 4LL * (nx - 4) * nz;
+    if (e < fx) {
+        const int s = (int)(e / ((long long)ny * nz));
+        const long long r = e - (long long)s * ny * nz;
+        x = s < 2 ? s : nx - 4 + s;
+        y = (int)(r / nz);
+        z = (int)(r - (long long)y * nz);
+    } else if (e < fx + fy) {
+        e -= fx;
+        const int xi = (int)(e / (4LL * nz));
+        const int r = (int)(e - (long long)xi * 4 * nz);
+        const int s = r / nz;
+        x = xi + 2;
+        y = s < 2 ? s : ny - 4 + s;
+        z = r - s * nz;
+    } else {
+        e -= fx + fy;
+        const long long row = e >> 2;
+        const int s = (int)(e & 3);
+        x = (int)(row / (ny - 4)) + 2;
+        y = (int)(row - (long long)(x - 2) * (ny - 4)) + 2;
+        z = s < 2 ? s : nz - 4 + s;
+    }
+}
+
 template <class T> __global__ void fill_ghosts_kernel(const GridArgs<T> a, T *buf) {
-    const long long total = (long long)a.nx * a.ny * a.nz;
+    const long long total = (long long)a.nx * a.ny * a.nz - (long long)(a.nx - 4) * (a.ny - 4) * (a.nz - 4);
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < total;
          c += (long long)gridDim.x * blockDim.x) {
-        const int x = (int)(c / ((long long)a.ny * a.nz));
-        const int y = (int)((c / a.nz) % a.ny);
-        const int z = (int)(c % a.nz);
-        const bool ghost = x < 2 || x > a.nx - 3 || y < 2 || y > a.ny - 3 || z < 2 || z > a.nz - 3;
-        if (!ghost) continue;
+        int x, y, z;
+        ghost_cell(c, a.nx, a.ny, a.nz, x, y, z);
         int fx, fy, fz;
         const int sx = axis_source(x, a.nx, a.bc[0], a.bc[1], &fx);
         const int sy = axis_source(y, a.ny, a.bc[2], a.bc[3], &fy);

@@ -8,7 +8,8 @@
 namespace dg {
 
 template <class T> cudaError_t launch_fill_ghosts(const GridArgs<T> &a, T *buf, cudaStream_t st) {
-    fill_ghosts_kernel<T><<<flat_blocks((long long)a.nx * a.ny * a.nz), 256, 0, st>>>(a, buf);
+    const long long ghosts = (long long)a.nx * a.ny * a.nz - (long long)(a.nx - 4) * (a.ny - 4) * (a.nz - 4);
+    fill_ghosts_kernel<T><<<flat_blocks(ghosts), 256, 0, st>>>(a, buf);
     return cudaGetLastError();
 }
 
