@@ -314,8 +314,12 @@ __device__ __forceinline__ unsigned long long cell_bits(unsigned long long step,
     return z ^ (z >> 31);
 }
 
+// (k + 1/2) / 4096 - 1/2 for the 12-bit k of the field, built without an
+// integer conversion: 1 + k/4096 is the double with exponent 0 and k in the
+// top mantissa bits, and subtracting 3/2 - 1/8192 is exact.
 __device__ __forceinline__ double dither(unsigned long long bits, int field) {
-    return ((double)((bits >> (12 * field)) & 4095u) + 0.5) * (1.0 / 4096.0) - 0.5;
+    const unsigned k = (unsigned)(bits >> (12 * field)) & 4095u;
+    return __hiloint2double((int)(0x3FF00000u | (k << 8)), 0) - (1.5 - 0.5 / 4096.0);
 }
 
 // x rounded to FP32 with a dither of one unit in the last place (stochastic
@@ -329,8 +333,9 @@ __device__ __forceinline__ float round_dithered(double x, double h) {
     const float r = (float)x;
     const float a = fabsf(r);
     if (!isfinite(a)) return r;
-    const double ulp = (double)__uint_as_float(__float_as_uint(a) + 1u) - (double)a;
-    return (float)(x + h * ulp);
+    // the spacing above a: exact in FP32 (adjacent values)
+    const float ulp = __uint_as_float(__float_as_uint(a) + 1u) - a;
+    return (float)(x + h * (double)ulp);
 }
 
 constexpr int kApplyVals = 16;  // per-block partials of the apply pass (+ the wave-speed maximum)
