@@ -151,6 +151,26 @@ __device__ __forceinline__ void store_bf16(__nv_bfloat16 *dst, const float *v, i
     }
 }
 
+// 16 values as BF16 with one 32-byte store (dst 32-byte aligned).
+__device__ __forceinline__ void store16_bf16(__nv_bfloat16 *dst, const float *v) {
+    uint32_t w[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        __nv_bfloat162 h = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+        w[i] = *reinterpret_cast<uint32_t *>(&h);
+    }
+    asm volatile("st.global.v8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(dst), "r"(w[0]), "r"(w[1]),
+                 "r"(w[2]), "r"(w[3]), "r"(w[4]), "r"(w[5]), "r"(w[6]), "r"(w[7])
+                 : "memory");
+}
+
+// 8 FP32 values with one 32-byte store (dst 32-byte aligned).
+__device__ __forceinline__ void store8_f32(float *dst, const float *v) {
+    asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(dst), "f"(v[0]), "f"(v[1]),
+                 "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7])
+                 : "memory");
+}
+
 __device__ __forceinline__ void load_bf16(const __nv_bfloat16 *src, float *v, int n) {
     for (int c = 0; c < n; c += 8) {
         const uint4 w = *reinterpret_cast<const uint4 *>(src + c);
@@ -388,25 +408,36 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
                 const long long o =
                     ((((long long)b * a.ox + x + a.off) * a.oy + y + a.off) * a.oz + z + a.off) * COUT + c0;
                 const long long dn = ((((long long)b * a.xo + x) * a.yo + y) * a.zo + z) * COUT + c0;
+                // one 32-byte store per lane and tensor where the columns allow
+                // (COUT 32: 16 BF16 columns; COUT 16: 8 FP32 columns)
                 if constexpr (EPI == kEpiGelu) {
 #pragma unroll
                     for (int c = 0; c < NC; ++c) v[c] += bias[c];
-                    if (a.out_z) store_bf16(a.out_z + dn, v, NC);
+                    if (a.out_z) {
+                        if constexpr (NC == 16) store16_bf16(a.out_z + dn, v);
+                        else store_bf16(a.out_z + dn, v, NC);
+                    }
 #pragma unroll
                     for (int c = 0; c < NC; ++c) v[c] = gelu(v[c]);
-                    store_bf16(a.out_a + o, v, NC);
+                    if constexpr (NC == 16) store16_bf16(a.out_a + o, v);
+                    else store_bf16(a.out_a + o, v, NC);
                 } else if constexpr (EPI == kEpiLinear) {
 #pragma unroll
-                    for (int c = 0; c < NC; c += 4)
-                        *reinterpret_cast<float4 *>(a.out_f + o + c) =
-                            make_float4(v[c] + bias[c], v[c + 1] + bias[c + 1], v[c + 2] + bias[c + 2],
-                                        v[c + 3] + bias[c + 3]);
+                    for (int c = 0; c < NC; ++c) v[c] += bias[c];
+                    if constexpr (NC == 8) {
+                        store8_f32(a.out_f + o, v);
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < NC; c += 4)
+                            *reinterpret_cast<float4 *>(a.out_f + o + c) = make_float4(v[c], v[c + 1], v[c + 2], v[c + 3]);
+                    }
                 } else {
                     float zv[NC];
                     load_bf16(a.zsrc + dn, zv, NC);
 #pragma unroll
                     for (int c = 0; c < NC; ++c) v[c] *= gelu_grad(zv[c]);
-                    store_bf16(a.out_a + o, v, NC);
+                    if constexpr (NC == 16) store16_bf16(a.out_a + o, v);
+                    else store_bf16(a.out_a + o, v, NC);
                 }
             }
         }

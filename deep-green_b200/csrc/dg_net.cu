@@ -705,8 +705,9 @@ int32_t dg_net_get_grad(dg_net *net, int32_t layer, float *gw, float *gb) {
 int32_t dg_net_forward(dg_net *net, const void *feat, int32_t n, int32_t x, int32_t y, int32_t z, float *out) {
     if (!net || !feat || !out) return fail(net, DG_ERR_INVALID, "null argument");
     if (int r = check_extents(net, n, x, y, z)) return r;
-    if ((reinterpret_cast<uintptr_t>(feat) | reinterpret_cast<uintptr_t>(out)) & 15)
-        return fail(net, DG_ERR_INVALID, "device pointers must be 16-byte aligned");
+    // the output is written with 32-byte stores
+    if ((reinterpret_cast<uintptr_t>(feat) & 15) || (reinterpret_cast<uintptr_t>(out) & 31))
+        return fail(net, DG_ERR_INVALID, "feat must be 16-byte and out 32-byte aligned");
     NET_CUDA(net, cudaSetDevice(net->device));
     if (int r = ensure_ws(net, n, x, y, z, false)) return r;
     return forward(net, feat, n, x, y, z, out, false, net->stream);

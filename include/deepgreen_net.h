@@ -56,8 +56,9 @@ int32_t dg_net_set_layer(dg_net *net, int32_t layer, const float *w, const float
 int32_t dg_net_get_layer(dg_net *net, int32_t layer, float *w, float *b);
 int32_t dg_net_get_grad(dg_net *net, int32_t layer, float *gw, float *gb);
 
-/* Inference.  feat: device BF16 [n][x][y][z][16]; out: device FP32
- * [n][x-8][y-8][z-8][16].  Asynchronous on the network's stream. */
+/* Inference.  feat: device BF16 [n][x][y][z][16] (16-byte aligned); out:
+ * device FP32 [n][x-8][y-8][z-8][16] (32-byte aligned).  Asynchronous on the
+ * network's stream. */
 int32_t dg_net_forward(dg_net *net, const void *feat, int32_t n, int32_t x, int32_t y, int32_t z, float *out);
 
 /* One forward + backward pass.  feat: device BF16 [n][x][y][z][16]; target:
