@@ -33,6 +33,11 @@ measured BF16 peak beside it.  Takes about two minutes.
 convolutions, random weights) on an (n+8)^3 input, as the corrector runs it
 on an n^3 grid; TFLOP/s against the measured BF16 peak.
 
+--case snapshot: the state output of the reference's time loop
+(save_to_disk, io.rs:5-196) for the 512^3 state: capture time on the step
+stream, device->host copy rate, the step time while a copy is in flight,
+and the file write rate.
+
 --impl reference times the reference's CPU algorithm (the oracle port; the
 Rust crate cannot be built on this image) on the same workload and metric.
 Multi-GPU (torchrun): independent replicas, one 512^3 grid per rank
@@ -69,7 +74,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=512, help="interior cells per axis")
-    ap.add_argument("--case", default="sod", choices=["sod", "vortex", "batch64", "learned", "netfwd"])
+    ap.add_argument("--case", default="sod", choices=["sod", "vortex", "batch64", "learned", "netfwd", "snapshot"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -525,6 +530,79 @@ def run_netfwd(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def run_snapshot(args, world, rank, local):
+    """Snapshot output (save_to_disk, io.rs:5-196) of the n^3 Sod state: the
+    capture's cost on the step stream, the device->host copy rate, the step
+    time while a copy is in flight, and the file write rate."""
+    import tempfile
+    import torch
+    from deepgreen import capi, snapshot
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n = args.n
+    cons, ds, bcs = device_initial_state("sod", n, dev)
+    ctx = capi.Context((n, n, n), ds, bcs, gamma=GAMMA, cfl=CFL, limiter=capi.LIMITER_MINMOD,
+                       precision=capi.F32, device=local)
+    ctx.set_conserved_device([c.data_ptr() for c in cons])
+    del cons
+    ctx.enqueue_steps(max(args.warmup, 1))
+    ctx.synchronize()
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    snap = snapshot.Snapshot(ctx)
+    nbytes = 10 * (n + 4) ** 3 * 4
+    snap.begin()
+    snap.wait()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    captures, copies = [], []
+    for _ in range(3):
+        ctx.synchronize()
+        ev[0].record(stream)
+        t0 = time.perf_counter()
+        snap.begin()
+        ev[1].record(stream)
+        snap.wait()
+        copies.append(time.perf_counter() - t0)
+        ev[1].synchronize()
+        captures.append(ev[0].elapsed_time(ev[1]))
+    k = 10
+    ctx.synchronize()
+    ev[0].record(stream)
+    ctx.enqueue_steps(k)
+    ev[1].record(stream)
+    ev[1].synchronize()
+    plain_ms = ev[0].elapsed_time(ev[1]) / k
+    snap.begin()
+    ev[2].record(stream)
+    ctx.enqueue_steps(k)
+    ev[3].record(stream)
+    ev[3].synchronize()
+    snap.wait()
+    overlapped_ms = ev[2].elapsed_time(ev[3]) / k
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "state.00000.dgsnap")
+        t0 = time.perf_counter()
+        snap.write(path)
+        write_s = time.perf_counter() - t0
+        size = os.path.getsize(path)
+    snap.close()
+    cap = statistics.median(captures)
+    line = {
+        "metric": "snapshot capture time on the step stream", "value": cap, "unit": "ms",
+        "n_gpus": 1, "steps": k, "warmup": args.warmup, "higher_is_better": False, "scaling": "none",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"snapshot_sod_{n}^3_fp32", "groups": "primitives + conserved", "bytes": nbytes},
+        # capture traffic: read 2 states (5 fields each), write 10 dense fields
+        "capture_GBps": 2 * nbytes / (cap * 1e-3) / 1e9,
+        "d2h_GBps": nbytes / statistics.median(copies) / 1e9,
+        "step_ms": plain_ms, "step_ms_during_copy": overlapped_ms,
+        "file_write_GBps": size / write_s / 1e9,
+        "gpu_launches": 1,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup()
@@ -537,6 +615,8 @@ def main():
             run_learned(args, world, rank, local)
         elif args.case == "netfwd":
             run_netfwd(args, world, rank, local)
+        elif args.case == "snapshot":
+            run_snapshot(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:

@@ -29,6 +29,7 @@ F32, F64 = 0, 1
 ROUNDING_DEFAULT, ROUNDING_REFERENCE = 0, 1
 STATUS_NONFINITE = 0x1
 STATUS_TIMEOUT = 0x2
+SNAP_PRIMITIVES, SNAP_CONSERVED = 0x1, 0x2
 
 
 class SimInfo(ctypes.Structure):
@@ -79,6 +80,14 @@ SIGNATURES = {
     "dg_compute_step_dt": [_P, ctypes.c_double],
     "dg_next_dt": [_P, ctypes.POINTER(ctypes.c_double)],
     "dg_compute_step_noalloc": [ctypes.POINTER(SimInfo), _P, _P, ctypes.POINTER(ctypes.c_double), _P],
+    "dg_snapshot_create": [_P, ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p)],
+    "dg_snapshot_destroy": [_P],
+    "dg_snapshot_begin": [_P],
+    "dg_snapshot_wait": [_P, ctypes.POINTER(ctypes.c_void_p)],
+    "dg_snapshot_write": [_P, ctypes.c_char_p],
+    "dg_snapshot_write_host": [ctypes.c_char_p, _I, ctypes.POINTER(_I), _I, ctypes.POINTER(ctypes.c_char_p),
+                               ctypes.POINTER(ctypes.c_void_p), ctypes.c_uint64, ctypes.c_char_p],
+    "dg_snapshot_last_error": [_P],
     "dg_batch_create": [_I, ctypes.POINTER(SimInfo), ctypes.POINTER(ctypes.c_void_p)],
     "dg_batch_destroy": [_P],
     "dg_batch_set_primitives": [_P, _I, _PP5],
@@ -121,6 +130,7 @@ _RESTYPES = {
     "dg_batch_last_error": ctypes.c_char_p,
     "dg_net_last_error": ctypes.c_char_p,
     "dg_corrector_last_error": ctypes.c_char_p,
+    "dg_snapshot_last_error": ctypes.c_char_p,
     "dg_net_get_stream": ctypes.c_void_p,
 }
 

@@ -132,3 +132,19 @@ def compute_step(info: Simulation, grid: SimulationGrid) -> float:
     if not grid._has_state:
         raise RuntimeError("calc_conserved must run before compute_step (as in main.rs:50)")
     return float(grid._ctx.compute_step(1)[0])
+
+
+def save_to_disk(grid: SimulationGrid, fname: str) -> None:
+    """io.rs:5-196: the grid's primitive and conserved fields to fname, in
+    the snapshot format of deepgreen.snapshot (HDF5 is not available; the
+    gradient and flux intermediates are not stored by the fused step).  The
+    capture and its copy to the host run on the device; the grid may step
+    again as soon as this returns."""
+    from . import snapshot
+    if not grid._has_state:
+        raise RuntimeError("calc_conserved must run before save_to_disk")
+    snap = getattr(grid, "_snapshot", None)
+    if snap is None:
+        snap = grid._snapshot = snapshot.Snapshot(grid._ctx)
+    snap.begin()
+    snap.write(fname)

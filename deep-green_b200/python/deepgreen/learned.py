@@ -327,11 +327,15 @@ def load(path, device: int = 0):
 # ---------------------------------------------------------------------------
 # Corrected and plain solves to a given time
 # ---------------------------------------------------------------------------
-def solve_to_time(ctx: capi.Context, t_end: float, corrector: Corrector | None = None, max_steps: int = 100000):
+def solve_to_time(ctx: capi.Context, t_end: float, corrector: Corrector | None = None, max_steps: int = 100000,
+                  batch: int = 16, growth: float = 1.1):
     """Advance ctx from time 0 to t_end: CFL steps (plain, or corrected when a
     corrector is given) while they stay short of t_end, then one plain step
-    of the remaining time.  Each step reads the coming dt first, as the
-    reference's loop reads dt every step.  Returns (steps, seconds)."""
+    of the remaining time.  Far from t_end the steps go to the device in
+    batches of up to `batch` without a host round trip: a batch of m steps
+    is enqueued only if m steps whose dt grew by `growth` each step would
+    still end short of t_end, and the dts the steps used are read back after
+    it.  Near t_end every step reads its dt first.  Returns (steps, seconds)."""
     import torch
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -344,11 +348,17 @@ def solve_to_time(ctx: capi.Context, t_end: float, corrector: Corrector | None =
                 ctx.compute_step_dt(t_end - t)
                 steps += 1
             break
+        m, reach, d = 0, 0.0, dt
+        while m < min(batch, max_steps - steps) and t + reach + d < t_end:
+            reach += d
+            d *= growth
+            m += 1
+        m = max(m, 1)
         if corrector is not None:
-            corrector.step(1)
+            corrector.step(m)
         else:
-            ctx.enqueue_steps(1)
-        t += dt
-        steps += 1
+            ctx.enqueue_steps(m)
+        t += float(np.sum(ctx.get_dts(m))) if m > 1 else dt
+        steps += m
     ctx.synchronize()
     return steps, time.perf_counter() - t0

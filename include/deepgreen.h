@@ -188,6 +188,44 @@ int32_t dg_compute_step_dt(dg_ctx *ctx, double dt);
 int32_t dg_compute_step_noalloc(const dg_sim_info *info, void *cons_in, void *cons_out, double *dt_used,
                                 void *stream);
 
+/* ---- Snapshots (save_to_disk, io.rs:5-196) -------------------------------
+ * The groups save_to_disk writes for the state: "primitives" (rho, vx, vy,
+ * vz, pressure: the state at the start of the last step, as
+ * dg_get_primitives) and "conserved" (mass, momentum_x, momentum_y,
+ * momentum_z, energy: the current state), each field the full ghosted
+ * (nx+4, ny+4, nz+4) C-order array in the context's precision.  (The
+ * "gradients" and "fluxes" groups are step intermediates that the fused step
+ * never stores; they are not written.)  HDF5 is not available, so the file is
+ * "DGSNAP01", a little-endian uint64 header length, a JSON header (dtype,
+ * shape, steps, the context's constants as "attrs", and per dataset its
+ * "group/name", byte offset and size), then the datasets, each starting on
+ * a 4096-byte boundary.  deepgreen.snapshot.read (Python) reads it. */
+#define DG_SNAP_PRIMITIVES 0x1u
+#define DG_SNAP_CONSERVED 0x2u
+typedef struct dg_snapshot dg_snapshot;
+/* Device and pinned host buffers for the chosen groups of ctx's state;
+ * reusable for every output of a run.  ctx must outlive the snapshot. */
+int32_t dg_snapshot_create(dg_ctx *ctx, uint32_t groups, dg_snapshot **out);
+int32_t dg_snapshot_destroy(dg_snapshot *snap);
+/* Capture the current state: the fields are packed on the device in order
+ * on ctx's stream, then copied to pinned host memory on a copy stream.
+ * Returns at once; ctx may keep stepping (the capture does not wait for the
+ * steps and the steps do not disturb the capture). */
+int32_t dg_snapshot_begin(dg_snapshot *snap);
+/* Wait for the last capture's copy; *host (if non-NULL) receives the pinned
+ * buffer: the fields, dense, in file order. */
+int32_t dg_snapshot_wait(dg_snapshot *snap, const void **host);
+/* Wait for the last capture and write it to path. */
+int32_t dg_snapshot_write(dg_snapshot *snap, const char *path);
+/* The file writer on host arrays (no device needed): nfields datasets
+ * "group/name" of shape[0]*shape[1]*shape[2] values of dtype (DG_F32 or
+ * DG_F64); attrs is a JSON object or NULL. */
+int32_t dg_snapshot_write_host(const char *path, int32_t dtype, const int32_t shape[3], int32_t nfields,
+                               const char *const names[], const void *const data[], uint64_t steps,
+                               const char *attrs);
+/* Message of the last failed snapshot call (shared by all snapshots). */
+const char *dg_snapshot_last_error(const dg_snapshot *snap);
+
 /* ---- Batches: many independent grids, one persistent launch per step ----
  * No counterpart in the reference, which steps one grid per compute_step
  * call (physics.rs:595-681); a batch is N such grids advanced together.
