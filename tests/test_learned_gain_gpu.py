@@ -5,7 +5,7 @@ the GPU by the library's own kernels: training pairs made by the solver
 (coarse 64^3 against fine 128^3, seeded KH layers), the flux-form network
 trained with Adam, then a held-out KH layer (shear 0.5, density ratio 2)
 solved on the coarse grid with and without the correction to the time the
-fine grid reaches in 100 steps.  The fine solve, coarsened, is the judge: the
+fine grid reaches in 100 steps.  The fine solve, coarsened, is the reference: the
 corrected coarse solve must have a clearly smaller relative L1 density error
 than the plain one, with (almost) no step falling back.
 
