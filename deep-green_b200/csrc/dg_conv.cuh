@@ -531,35 +531,39 @@ __global__ void __launch_bounds__(kConvThreads, 1)
             for (int j = it - 2 < 0 ? 0 : it - 2; j < it; ++j) ok &= mbar_wait(full + (j & 1), (j >> 1) & 1, kWaitBudget);
         }
     } else if (warp == 1) {
-        if (lane == 0) {
-            int it = 0;
-            for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, ++it) {
-                const int s = it & 1, u = it >> 1;
-                if (!mbar_wait(full + s, u & 1, kWaitBudget)) {
-                    ok = false;
-                    break;
-                }
-                tc::fence_after();
-                const int seg = tile % a.nseg;
-                const int len = min(kM, a.zo - seg * kM);
-                const int nk = (len + 15) >> 4;
-                const uint32_t xa = smem_u32(xs + s * L::XSTAGE);
-                const uint32_t ga = smem_u32(gs + s * L::GSTAGE);
+        // the whole warp runs the issue loop; the elected lane issues each
+        // tile's MMAs and its commit (see elect_one)
+        int it = 0;
+        for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, ++it) {
+            const int s = it & 1, u = it >> 1;
+            if (!warp_wait(full + s, u & 1)) {
+                ok = false;
+                break;
+            }
+            tc::fence_after();
+            const int seg = tile % a.nseg;
+            const int len = min(kM, a.zo - seg * kM);
+            const int nk = (len + 15) >> 4;
+            const uint32_t xa = smem_u32(xs + s * L::XSTAGE);
+            const uint32_t ga = smem_u32(gs + s * L::GSTAGE);
+            if (tc::elect_one()) {
 #pragma unroll 1
                 for (int ks = 0; ks < nk; ++ks) {
                     const uint64_t bd = tc::sdesc(ga + (uint32_t)(ks * 256), 128, kM * 16);
+                    const uint32_t acc = (it | ks) != 0;
 #pragma unroll
                     for (int j = 0; j < 9; ++j) {
                         const int dy = j / 3, dz = j % 3;
                         const uint32_t aa = xa + (uint32_t)((dy * kWz + dz + 16 * ks) * 16);
-                        tc::mma_bf16(tbase + (uint32_t)(j * COUT), tc::sdesc(aa, 128, kBox), bd, IDESC,
-                                     (it | ks) != 0);
+                        tc::mma_bf16(tbase + (uint32_t)(j * COUT), tc::sdesc(aa, 128, kBox), bd, IDESC, acc);
                     }
                 }
                 tc::commit(empty + s);
             }
-            tc::commit(done);
+            __syncwarp();
         }
+        if (tc::elect_one()) tc::commit(done);
+        __syncwarp();
     } else {
         const int q = warp & 3;
         const int m = 32 * q + lane;            // TMEM lane = row of D

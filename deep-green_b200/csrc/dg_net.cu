@@ -51,6 +51,7 @@ struct dg_net {
     unsigned *status = nullptr;
     float *wpart = nullptr;            // weight-gradient partials, one row per block
     double *loss_part = nullptr;
+    double *pow_part = nullptr;        // flux-form loss: target power partials [64 entries][kPowBlocks]
     int nsm = 148;
     long long adam_t = 0;
     Workspace ws;
@@ -204,37 +205,53 @@ __global__ void loss_kernel(const float *__restrict__ out, const float *__restri
 // (output channel 5 d + c, output cell t+1 in an output one cell larger than
 // the target on each axis); residual r = dU - target, squared-error partials
 // per block, and g = scale * r into gbuf [n][s^3][5].
+// Target power of each batch entry: block (x, b) sums the squares of the 5
+// target channels over its share of entry b's cells (rows of 16 floats read
+// as one float4 and one float) into part[b][x].
+constexpr int kPowBlocks = 64;
+__global__ void __launch_bounds__(256) sample_power_kernel(const float *__restrict__ tgt, int s,
+                                                           double *__restrict__ part) {
+    __shared__ double red[8];
+    const int b = blockIdx.y;
+    const long long per = (long long)s * s * s;
+    const float *t = tgt + (long long)b * per * 16;
+    double acc = 0.0;
+    for (long long v = blockIdx.x * 256LL + threadIdx.x; v < per; v += kPowBlocks * 256LL) {
+        const float4 a = *reinterpret_cast<const float4 *>(t + v * 16);
+        const float e = t[v * 16 + 4];
+        acc += (double)a.x * a.x + (double)a.y * a.y + (double)a.z * a.z + (double)a.w * a.w + (double)e * e;
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double sum = 0.0;
+        for (int i = 0; i < 8; ++i) sum += red[i];
+        part[b * kPowBlocks + blockIdx.x] = sum;
+    }
+}
+
 // Per batch entry b: w[b] = 1 when not balancing, else mean power of all
 // targets / (power of entry b's target + floor * mean power), so that every
-// crop counts alike whatever the size of its corrections.
-__global__ void sample_weight_kernel(const float *__restrict__ tgt, int n, int s, int balance, float floor_frac,
+// crop counts alike whatever the size of its corrections.  One block of 64
+// threads; thread b sums entry b's partials in order.
+__global__ void sample_weight_kernel(const double *__restrict__ part, int n, int s, int balance, float floor_frac,
                                      float *__restrict__ w) {
-    __shared__ double red[32];
     __shared__ double pw[64];
     const long long per = (long long)s * s * s;
-    for (int b = 0; b < n; ++b) {
-        double acc = 0.0;
-        for (long long v = threadIdx.x; v < per; v += blockDim.x)
-            for (int c = 0; c < 5; ++c) {
-                const double t = tgt[((long long)b * per + v) * 16 + c];
-                acc += t * t;
-            }
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double sum = 0.0;
-            for (int i = 0; i < (int)(blockDim.x >> 5); ++i) sum += red[i];
-            pw[b] = sum / (per * 5.0);
-        }
-        __syncthreads();
+    const int b = threadIdx.x;
+    if (b < n) {
+        double sum = 0.0;
+        for (int x = 0; x < kPowBlocks; ++x) sum += part[b * kPowBlocks + x];
+        pw[b] = sum / (per * 5.0);
     }
+    __syncthreads();
     if (threadIdx.x == 0) {
         double mean = 0.0;
-        for (int b = 0; b < n; ++b) mean += pw[b];
+        for (int i = 0; i < n; ++i) mean += pw[i];
         mean /= n;
-        for (int b = 0; b < n; ++b)
-            w[b] = balance && mean > 0.0 ? (float)(mean / (pw[b] + floor_frac * mean)) : 1.0f;
+        for (int i = 0; i < n; ++i)
+            w[i] = balance && mean > 0.0 ? (float)(mean / (pw[i] + floor_frac * mean)) : 1.0f;
     }
 }
 
@@ -604,6 +621,7 @@ int32_t dg_net_create(const dg_net_info *info, dg_net **out) {
     }
     if (!cu(cudaMalloc(&net->wpart, maxrow * net->nsm * 4), "cudaMalloc")) return bail(DG_ERR_CUDA);
     if (!cu(cudaMalloc(&net->loss_part, 4096 * sizeof(double)), "cudaMalloc")) return bail(DG_ERR_CUDA);
+    if (!cu(cudaMalloc(&net->pow_part, 64 * kPowBlocks * sizeof(double)), "cudaMalloc")) return bail(DG_ERR_CUDA);
     if (!cu(cudaMalloc(&net->status, sizeof(unsigned)), "cudaMalloc") ||
         !cu(cudaMemset(net->status, 0, sizeof(unsigned)), "memset"))
         return bail(DG_ERR_CUDA);
@@ -641,6 +659,7 @@ int32_t dg_net_destroy(dg_net *net) {
     }
     cudaFree(net->wpart);
     cudaFree(net->loss_part);
+    cudaFree(net->pow_part);
     cudaFree(net->status);
     if (net->stream) cudaStreamDestroy(net->stream);
     delete net;
@@ -769,7 +788,8 @@ int32_t dg_net_forward_backward_flux(dg_net *net, const void *feat, const float 
     if (int r = forward(net, feat, n, x, y, z, ws.out, true, net->stream)) return r;
     const float scale = (float)(2.0 / ((double)ntgt * 5));
     const int lblocks = (int)std::min<long long>(4096, (ntgt + 255) / 256);
-    sample_weight_kernel<<<1, 256, 0, net->stream>>>(target, n, s, balance, 0.01f, ws.wsample);
+    sample_power_kernel<<<dim3(kPowBlocks, n), 256, 0, net->stream>>>(target, s, net->pow_part);
+    sample_weight_kernel<<<1, 64, 0, net->stream>>>(net->pow_part, n, s, balance, 0.01f, ws.wsample);
     flux_residual_kernel<<<lblocks, 256, 0, net->stream>>>(ws.out, target, n, s, scale, ws.wsample, ws.gbuf,
                                                            net->loss_part);
     flux_grad_kernel<<<1024, 256, 0, net->stream>>>(ws.gbuf, n, s, ws.dz[3]);
