@@ -159,6 +159,12 @@ class Corrector:
 # ---------------------------------------------------------------------------
 # Initial states of the training and evaluation workloads
 # ---------------------------------------------------------------------------
+def _setup_device():
+    """The GPU builds the large initial states (same values as the NumPy path)."""
+    import torch
+    return "cuda" if torch.cuda.is_available() else None
+
+
 def initial_state(kind: str, n: int, seed: int, **kw):
     """'kh': KH layer with shear / ratio (kw, else drawn from seed: shear in
     [0.2, 0.8], density ratio in [1, 4]); 'fourier': 8 random modes."""
@@ -166,10 +172,10 @@ def initial_state(kind: str, n: int, seed: int, **kw):
         rng = np.random.default_rng(seed)
         shear = kw.get("shear", rng.uniform(0.2, 0.8))
         ratio = kw.get("ratio", rng.uniform(1.0, 4.0))
-        prim, _, _ = setups.kelvin_helmholtz(n, seed=seed, shear=shear, ratio=ratio)
+        prim, _, _ = setups.kelvin_helmholtz(n, seed=seed, shear=shear, ratio=ratio, device=_setup_device())
         return prim, {"kind": "kh", "seed": seed, "shear": float(shear), "ratio": float(ratio)}
     if kind == "fourier":
-        prim, _, _ = setups.fourier_modes(n, seed)
+        prim, _, _ = setups.fourier_modes(n, seed, device=_setup_device())
         return prim, {"kind": "fourier", "seed": seed}
     raise ValueError(kind)
 

@@ -47,12 +47,59 @@ def centres(n_int: int, ds: float, lo: float = 0.0) -> np.ndarray:
     return lo + (np.arange(n_int + 4, dtype=np.float64) - 2 + 0.5) * ds
 
 
+def _splitmix64_t(x):
+    """splitmix64 on int64 torch tensors holding uint64 bit patterns
+    (multiplication wraps modulo 2^64 as on uint64; right shifts made
+    logical by masking)."""
+    import torch
+
+    def srl(v, k):
+        return (v >> k) & ((1 << (64 - k)) - 1)
+
+    def c(u):  # uint64 constant as the int64 with the same bits
+        return torch.tensor(u - (1 << 64) if u >= 1 << 63 else u, dtype=torch.int64, device=x.device)
+
+    x = x + c(0x9E3779B97F4A7C15)
+    x = (x ^ srl(x, 30)) * c(0xBF58476D1CE4E5B9)
+    x = (x ^ srl(x, 27)) * c(0x94D049BB133111EB)
+    return x ^ srl(x, 31)
+
+
+def _counter_uniform_t(seed: int, index, comp: int):
+    """counter_uniform on an int64 torch index tensor, bit for bit."""
+    import torch
+    s = seed & _MASK64
+    k0 = (s * 0x9E3779B97F4A7C15) & _MASK64
+    k0 = torch.tensor(k0 - (1 << 64) if k0 >= 1 << 63 else k0, dtype=torch.int64, device=index.device)
+    r = _splitmix64_t(k0 + index * 3 + comp)
+    return ((r >> 11) & ((1 << 53) - 1)).to(torch.float64) * (1.0 / 9007199254740992.0)
+
+
+def _kh_noise_device(vels, seed, noise, shape, n, ny, nz, device):
+    """The noise of kelvin_helmholtz added on a torch device (same bits as
+    the NumPy path: integer hashing, then one multiply and adds per value)."""
+    import torch
+    dev = torch.device(device)
+    ii = (torch.arange(shape[0], device=dev) - 2).remainder(n).view(-1, 1, 1)
+    jj = (torch.arange(shape[1], device=dev) - 2).remainder(ny).view(1, -1, 1)
+    kk = (torch.arange(shape[2], device=dev) - 2).remainder(nz).view(1, 1, -1)
+    idx = ((ii * ny + jj) * nz + kk).to(torch.int64)
+    out = []
+    for comp, v in enumerate(vels):
+        t = torch.from_numpy(v).to(dev)
+        t += noise * (2.0 * _counter_uniform_t(seed, idx, comp) - 1.0)
+        out.append(t.cpu().numpy())
+    return out
+
+
 def kelvin_helmholtz(n: int = 64, seed: int = 1, noise: float = 1e-3, ny: int | None = None,
-                     nz: int | None = None, shear: float = 0.5, ratio: float = 2.0, p0: float = 2.5):
+                     nz: int | None = None, shear: float = 0.5, ratio: float = 2.0, p0: float = 2.5,
+                     device: str | None = None):
     """KH layer: rho=ratio, vx=+shear for |y-0.5|<0.25, else rho=1,
     vx=-shear; p=p0; vy=0.01 sin(4 pi x)(exp(-(y-0.25)^2/0.005)+exp(-(y-0.75)^2/0.005));
     vz=0; plus uniform noise in [-noise, noise] on vx, vy, vz.  The defaults
     (shear 0.5, ratio 2, p 2.5) are the 64^3 periodic parity workload.
+    `device` (a torch device) computes the noise there, with the same bits.
     Returns (prims, ds, bcs)."""
     ny = ny or n
     nz = nz or n
@@ -67,7 +114,9 @@ def kelvin_helmholtz(n: int = 64, seed: int = 1, noise: float = 1e-3, ny: int | 
                                                           + np.exp(-(y - 0.75) ** 2 / 0.005)), shape).copy()
     vz = np.zeros(shape)
     p = np.full(shape, float(p0))
-    if noise:
+    if noise and device is not None:
+        vx, vy, vz = _kh_noise_device((vx, vy, vz), seed, noise, shape, n, ny, nz, device)
+    elif noise:
         # noise indexed by interior cell (i, j, k) -> (i*ny + j)*nz + k
         ii = np.arange(shape[0])[:, None, None] - 2
         jj = np.arange(shape[1])[None, :, None] - 2
@@ -79,15 +128,19 @@ def kelvin_helmholtz(n: int = 64, seed: int = 1, noise: float = 1e-3, ny: int | 
     return [rho, vx, vy, vz, p], ds, (PERIODIC,) * 6
 
 
-def fourier_modes(n: int, seed: int, modes: int = 8, amp: float = 0.1, kmax: int = 4):
+def fourier_modes(n: int, seed: int, modes: int = 8, amp: float = 0.1, kmax: int = 4, device: str | None = None):
     """Smooth periodic state on the unit cube: rho = 1, p = 1, v = 0 plus
     `modes` random Fourier modes sin(2 pi k.x + phase), integer wave vectors
     k in [-kmax, kmax]^3 (not 0), each with its own amplitude in
-    [-amp, amp] on rho, p, vx, vy and vz.  Returns (prims, ds, bcs)."""
+    [-amp, amp] on rho, p, vx, vy and vz.  `device` (a torch device) runs the
+    3-D products and sums there (values within one FP64 unit in the last
+    place of the NumPy path's).  Returns (prims, ds, bcs)."""
     rng = np.random.default_rng(seed)
     ds = 1.0 / n
     c = centres(n, ds)
     shape = (n + 4,) * 3
+    if device is not None:
+        return _fourier_device(rng, c, shape, modes, amp, kmax, device), ds, (PERIODIC,) * 6
     prim = [np.ones(shape), np.zeros(shape), np.zeros(shape), np.zeros(shape), np.ones(shape)]
     for _ in range(modes):
         k = np.zeros(3, dtype=np.int64)
@@ -104,6 +157,36 @@ def fourier_modes(n: int, seed: int, modes: int = 8, amp: float = 0.1, kmax: int
         for f, j in zip(order, range(5)):
             prim[f] += a[j] * s
     return prim, ds, (PERIODIC,) * 6
+
+
+def _fourier_device(rng, c, shape, modes, amp, kmax, device):
+    """fourier_modes' fields on a torch device: the 1-D and 2-D factors in
+    NumPy as there, the 3-D imaginary part as Re(exy) Im(ez) + Im(exy) Re(ez)
+    and the sums on the device."""
+    import torch
+    dev = torch.device(device)
+    prim = [torch.ones(shape, dtype=torch.float64, device=dev), torch.zeros(shape, dtype=torch.float64, device=dev),
+            torch.zeros(shape, dtype=torch.float64, device=dev), torch.zeros(shape, dtype=torch.float64, device=dev),
+            torch.ones(shape, dtype=torch.float64, device=dev)]
+    for _ in range(modes):
+        k = np.zeros(3, dtype=np.int64)
+        while not k.any():
+            k = rng.integers(-kmax, kmax + 1, 3)
+        phase = rng.uniform(0.0, 2.0 * np.pi)
+        a = rng.uniform(-amp, amp, 5)
+        ex = np.exp(1j * (2 * np.pi * k[0] * c + phase))[:, None]
+        ey = np.exp(1j * 2 * np.pi * k[1] * c)[None, :]
+        ez = np.exp(1j * 2 * np.pi * k[2] * c)
+        exy = ex * ey
+        xr = torch.from_numpy(np.ascontiguousarray(exy.real)).to(dev)[:, :, None]
+        xi = torch.from_numpy(np.ascontiguousarray(exy.imag)).to(dev)[:, :, None]
+        zr = torch.from_numpy(np.ascontiguousarray(ez.real)).to(dev)[None, None, :]
+        zi = torch.from_numpy(np.ascontiguousarray(ez.imag)).to(dev)[None, None, :]
+        sn = xr * zi + xi * zr
+        order = (0, 4, 1, 2, 3)
+        for f, j in zip(order, range(5)):
+            prim[f] += float(a[j]) * sn
+    return [t.cpu().numpy() for t in prim]
 
 
 def sod(n: int = 64, ny: int | None = None, nz: int | None = None):

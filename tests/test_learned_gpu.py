@@ -208,3 +208,13 @@ def test_step_falls_back_when_the_totals_move():
     st = cor.stats()
     assert st["fallback_steps"] == 1 and st["steps"] == 1
     cor.close()
+
+
+def test_initial_states_on_the_gpu_match_numpy():
+    from deepgreen import setups
+    a, _, _ = setups.kelvin_helmholtz(20, seed=3, shear=0.6, ratio=1.5)
+    b, _, _ = setups.kelvin_helmholtz(20, seed=3, shear=0.6, ratio=1.5, device="cuda")
+    assert all(np.array_equal(x, y) for x, y in zip(a, b))
+    a, _, _ = setups.fourier_modes(20, 4)
+    b, _, _ = setups.fourier_modes(20, 4, device="cuda")
+    assert all(np.allclose(x, y, rtol=0, atol=4 * np.finfo(np.float64).eps) for x, y in zip(a, b))

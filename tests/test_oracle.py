@@ -120,3 +120,17 @@ def test_nan_gives_cfl_fallback_dt():
     o = pyoracle.Oracle(shape, 0.1, (P,) * 6, gamma=1.4, cfl=0.4)
     o.set_primitives(prim)
     assert o.step(1)[0] == pytest.approx(0.4)
+
+
+def test_setups_device_path_matches_numpy():
+    """The torch path of the KH generator (used on the GPU for the learned
+    workload's large states) gives the NumPy path's bits; Fourier modes
+    agree to an FP64 unit in the last place."""
+    pytest.importorskip("torch")
+    for n in (12, 21):
+        a, _, _ = setups.kelvin_helmholtz(n, seed=7, shear=0.4, ratio=3.0)
+        b, _, _ = setups.kelvin_helmholtz(n, seed=7, shear=0.4, ratio=3.0, device="cpu")
+        assert all(np.array_equal(x, y) for x, y in zip(a, b))
+        a, _, _ = setups.fourier_modes(n, 5)
+        b, _, _ = setups.fourier_modes(n, 5, device="cpu")
+        assert all(np.allclose(x, y, rtol=0, atol=4 * np.finfo(np.float64).eps) for x, y in zip(a, b))
