@@ -100,6 +100,49 @@ int copy_in(dg_ctx *c, void *dst, const void *const src[5], cudaMemcpyKind kind)
     return DG_OK;
 }
 
+// Host transfers move each field as one contiguous copy (the copy engines'
+// fast case; row-by-row copies of the pitched layout from host memory run
+// at about half the rate) through a dense device copy of the fields; the
+// re-pitch between the dense and the pitched layout is a device-to-device
+// copy.
+size_t dense_field_bytes(const dg_ctx *c) { return (size_t)c->nx * c->ny * c->nz * c->elem; }
+
+int upload_dense(dg_ctx *c, void *dense, const void *const src[5]) {
+    const size_t fb = dense_field_bytes(c);
+    for (int f = 0; f < 5; ++f) {
+        if (!src[f]) return fail(c, DG_ERR_INVALID, "null field pointer");
+        DG_CUDA(c, cudaMemcpyAsync(static_cast<char *>(dense) + f * fb, src[f], fb, cudaMemcpyHostToDevice,
+                                   c->stream));
+    }
+    return DG_OK;
+}
+
+int download_dense(dg_ctx *c, void *const dst[5], const void *dense) {
+    const size_t fb = dense_field_bytes(c);
+    for (int f = 0; f < 5; ++f) {
+        if (!dst[f]) return fail(c, DG_ERR_INVALID, "null field pointer");
+        DG_CUDA(c, cudaMemcpyAsync(dst[f], static_cast<const char *>(dense) + f * fb, fb, cudaMemcpyDeviceToHost,
+                                   c->stream));
+    }
+    return DG_OK;
+}
+
+// dense <-> pitched, on the device
+int repitch(dg_ctx *c, void *dst, const void *src, bool to_pitched) {
+    const size_t row = (size_t)c->nz * c->elem, fb = dense_field_bytes(c);
+    const size_t pitched = (size_t)c->pitch * c->elem;
+    for (int f = 0; f < 5; ++f) {
+        const size_t po = (size_t)f * c->fstride * c->elem;
+        if (to_pitched)
+            DG_CUDA(c, cudaMemcpy2DAsync(static_cast<char *>(dst) + po, pitched, static_cast<const char *>(src) + f * fb,
+                                         row, row, (size_t)c->nx * c->ny, cudaMemcpyDeviceToDevice, c->stream));
+        else
+            DG_CUDA(c, cudaMemcpy2DAsync(static_cast<char *>(dst) + f * fb, row, static_cast<const char *>(src) + po,
+                                         pitched, row, (size_t)c->nx * c->ny, cudaMemcpyDeviceToDevice, c->stream));
+    }
+    return DG_OK;
+}
+
 int copy_out(dg_ctx *c, void *const dst[5], const void *src, cudaMemcpyKind kind) {
     const size_t row = (size_t)c->nz * c->elem;
     for (int f = 0; f < 5; ++f) {
@@ -278,7 +321,9 @@ int32_t dg_set_conserved(dg_ctx *c, const void *const cons[5]) {
     int r;
     if ((r = use_device(c)) != DG_OK) return r;
     if ((r = reset_ctl(c)) != DG_OK) return r;
-    if ((r = copy_in(c, c->buf[c->cur], cons, cudaMemcpyHostToDevice)) != DG_OK) return r;
+    // the other state buffer holds the dense upload
+    if ((r = upload_dense(c, c->buf[1 - c->cur], cons)) != DG_OK) return r;
+    if ((r = repitch(c, c->buf[c->cur], c->buf[1 - c->cur], true)) != DG_OK) return r;
     if ((r = finish_state(c)) != DG_OK) return r;
     return check_flags(c);
 }
@@ -298,17 +343,18 @@ int32_t dg_set_primitives(dg_ctx *c, const void *const prim[5]) {
     int r;
     if ((r = use_device(c)) != DG_OK) return r;
     if ((r = reset_ctl(c)) != DG_OK) return r;
-    // stage the primitives in the other state buffer, convert into the current one
+    // stage the primitives densely in the other state buffer, convert into the current one
     void *stage = c->buf[1 - c->cur];
-    if ((r = copy_in(c, stage, prim, cudaMemcpyHostToDevice)) != DG_OK) return r;
+    if ((r = upload_dense(c, stage, prim)) != DG_OK) return r;
+    const long long dfs = (long long)c->nx * c->ny * c->nz;
     cudaError_t e;
     if (c->elem == 8) {
         auto a = grid_args<double>(c, stage, c->buf[c->cur]);
-        e = launch_prim_to_cons<double>(a, static_cast<const double *>(stage), c->fstride, c->pitch,
+        e = launch_prim_to_cons<double>(a, static_cast<const double *>(stage), dfs, c->nz,
                                         static_cast<double *>(c->buf[c->cur]), c->stream);
     } else {
         auto a = grid_args<float>(c, stage, c->buf[c->cur]);
-        e = launch_prim_to_cons<float>(a, static_cast<const float *>(stage), c->fstride, c->pitch,
+        e = launch_prim_to_cons<float>(a, static_cast<const float *>(stage), dfs, c->nz,
                                        static_cast<float *>(c->buf[c->cur]), c->stream);
     }
     if (e != cudaSuccess) return cuda_fail(c, e, "prim_to_cons");
@@ -386,7 +432,9 @@ int32_t dg_get_conserved(dg_ctx *c, void *const cons[5]) {
     if (!c->has_state) return fail(c, DG_ERR_NO_STATE, "no state set");
     int r;
     if ((r = use_device(c)) != DG_OK) return r;
-    if ((r = copy_out(c, cons, c->buf[c->cur], cudaMemcpyDeviceToHost)) != DG_OK) return r;
+    if (!c->prim_scratch) DG_CUDA(c, cudaMalloc(&c->prim_scratch, c->state_bytes));
+    if ((r = repitch(c, c->prim_scratch, c->buf[c->cur], false)) != DG_OK) return r;
+    if ((r = download_dense(c, cons, c->prim_scratch)) != DG_OK) return r;
     DG_CUDA(c, cudaStreamSynchronize(c->stream));
     return DG_OK;
 }
@@ -405,24 +453,25 @@ int32_t dg_get_primitives(dg_ctx *c, void *const prim[5]) {
     int r;
     if ((r = use_device(c)) != DG_OK) return r;
     if (!c->prim_scratch) DG_CUDA(c, cudaMalloc(&c->prim_scratch, c->state_bytes));
-    // the state at the start of the last step is the other buffer
+    // the state at the start of the last step is the other buffer; the
+    // primitives are written densely for contiguous host copies
     const void *src = c->steps > 0 ? c->buf[1 - c->cur] : c->buf[c->cur];
+    const long long dfs = (long long)c->nx * c->ny * c->nz;
     cudaError_t e;
     if (c->elem == 8) {
         auto a = grid_args<double>(c, src, nullptr);
         e = launch_cons_to_prim_policy<double, true>(a, static_cast<const double *>(src),
-                                                     static_cast<double *>(c->prim_scratch), c->fstride, c->pitch,
-                                                     c->stream);
+                                                     static_cast<double *>(c->prim_scratch), dfs, c->nz, c->stream);
     } else {
         auto a = grid_args<float>(c, src, nullptr);
         auto *dstp = static_cast<float *>(c->prim_scratch);
-        e = c->exact ? launch_cons_to_prim_policy<float, true>(a, static_cast<const float *>(src), dstp, c->fstride,
-                                                               c->pitch, c->stream)
-                     : launch_cons_to_prim_policy<float, false>(a, static_cast<const float *>(src), dstp, c->fstride,
-                                                                c->pitch, c->stream);
+        e = c->exact ? launch_cons_to_prim_policy<float, true>(a, static_cast<const float *>(src), dstp, dfs, c->nz,
+                                                               c->stream)
+                     : launch_cons_to_prim_policy<float, false>(a, static_cast<const float *>(src), dstp, dfs, c->nz,
+                                                                c->stream);
     }
     if (e != cudaSuccess) return cuda_fail(c, e, "cons_to_prim");
-    if ((r = copy_out(c, prim, c->prim_scratch, cudaMemcpyDeviceToHost)) != DG_OK) return r;
+    if ((r = download_dense(c, prim, c->prim_scratch)) != DG_OK) return r;
     DG_CUDA(c, cudaStreamSynchronize(c->stream));
     return DG_OK;
 }
