@@ -46,7 +46,10 @@
 // all output positions v.  D[M=128, N=COUT] per (dy, dz) pair, 9 TMEM
 // accumulators; the M rows are (dx in 0..3, ci) -- dx = 3 is a block of
 // ones, which turns its rows into the bias gradient sum_v dZ[v][co].  Both
-// operands are MN-major: K is the position along z, 16 bytes apart.
+// operands are MN-major: K is the position along z, 16 bytes apart.  A block
+// walks a column of output rows along y (one tile = one row segment of kM
+// positions): the input rows y, y+1, y+2 that tile y reads sit in a ring of
+// 4 rows per (dx, channel group), so each tile brings one new input row.
 //
 // Every wait is bounded (~2 s); a timeout sets a status bit and the block
 // drains its copies and MMAs and frees its TMEM before returning.
@@ -94,7 +97,8 @@ struct ConvArgs {
 struct WgradArgs {
     int nb, xo, yo, zo;             // extents of the output-gradient region
     int nseg;                       // z segments of kM positions per row
-    int ntiles;                     // nb * xo * yo * nseg
+    int ych, nyc;                   // rows per work unit, units per column: ceil(yo / ych)
+    int nunits;                     // work units (n, x, z segment, y chunk): nb * xo * nseg * nyc
     float *part;                    // per block: [COUT][CIN][27] weight partials then [COUT] bias partials
     unsigned *status;
 };
@@ -451,9 +455,11 @@ __global__ void __launch_bounds__(kFwdThreads, 1)
 
 template <int CIN, int COUT>
 struct WgradSmem {
-    static constexpr int XSTAGE = 16 * kBox;                 // 16 row groups (dx, cg) of [dy][kWz][8]
+    static constexpr int ROWB = kWz * 16;                    // one input row of one group: [kWz][8 ch]
+    static constexpr int GROUP = 4 * ROWB;                   // a ring of 4 rows per group (the SBO of A)
+    static constexpr int XRING = 16 * GROUP;                 // 16 groups (dx, cg); dx = 3 holds ones
     static constexpr int GSTAGE = (COUT / 8) * kM * 16;      // output gradient [co/8][kM][8]
-    static constexpr int BYTES = kStages * (XSTAGE + GSTAGE) + 128 + 128;
+    static constexpr int BYTES = XRING + kStages * GSTAGE + 128 + 128;
 };
 
 template <int CIN, int COUT>
@@ -466,24 +472,23 @@ __global__ void __launch_bounds__(kConvThreads, 1)
     constexpr uint32_t NACC = 9 * COUT;
     constexpr uint32_t TCOLS = NACC <= 256 ? 256 : 512;
     constexpr uint32_t IDESC = tc::idesc_bf16(kM, COUT, 1, 1);
-    constexpr uint32_t TX = 3 * CG * kBox + GG * kM * 16;    // bytes landing per tile
+    constexpr uint32_t ROWTX = 3 * CG * L::ROWB;             // one new input row of every data group
+    constexpr uint32_t GTX = GG * kM * 16;                   // one tile's output-gradient segment
 
     extern __shared__ unsigned char smem_raw[];
     unsigned char *smem = align128(smem_raw);
-    unsigned char *xs = smem;                                  // kStages x XSTAGE
-    unsigned char *gs = smem + kStages * L::XSTAGE;            // kStages x GSTAGE
+    unsigned char *xr = smem;                                  // input-row rings [16 groups][4 rows]
+    unsigned char *gs = smem + L::XRING;                       // kStages x GSTAGE
     uint64_t *bars = reinterpret_cast<uint64_t *>(gs + kStages * L::GSTAGE);
     uint64_t *full = bars, *empty = bars + 2, *done = bars + 4;
     uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 6);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // rows dx = 3 of both stages hold ones (bias gradient)
+    // the dx = 3 groups hold ones in every ring row (bias gradient)
     {
         const uint4 ones = make_uint4(0x3F803F80u, 0x3F803F80u, 0x3F803F80u, 0x3F803F80u);
-        for (int s = 0; s < kStages; ++s) {
-            uint4 *p = reinterpret_cast<uint4 *>(xs + s * L::XSTAGE + 3 * CG * kBox);
-            for (int i = threadIdx.x; i < CG * kBox / 16; i += blockDim.x) p[i] = ones;
-        }
+        uint4 *p = reinterpret_cast<uint4 *>(xr + 3 * CG * L::GROUP);
+        for (int i = threadIdx.x; i < CG * L::GROUP / 16; i += blockDim.x) p[i] = ones;
         fence_proxy_async();
     }
     if (threadIdx.x == 0) {
@@ -500,33 +505,45 @@ __global__ void __launch_bounds__(kConvThreads, 1)
     tc::fence_after();
     const uint32_t tbase = *tslot;
     bool ok = true;
-    const int mytiles = blockIdx.x < a.ntiles ? (a.ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
 
     if (warp == 0) {
         if (lane == 0) {
-            int it = 0;
-            for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, ++it) {
-                const int s = it & 1, u = it >> 1;
-                if (u > 0 && !mbar_wait(empty + s, (u - 1) & 1, kWaitBudget)) {
-                    ok = false;
-                    break;
-                }
-                int r = tile;
+            int it = 0;                                          // tiles of this block so far
+            for (int unit = blockIdx.x; ok && unit < a.nunits; unit += gridDim.x) {
+                int r = unit;
+                const int yc = r % a.nyc; r /= a.nyc;
                 const int seg = r % a.nseg; r /= a.nseg;
-                const int y = r % a.yo; r /= a.yo;
                 const int x = r % a.xo, b = r / a.xo;
+                const int y0 = yc * a.ych, ylen = min(a.ych, a.yo - y0);
                 const int z0 = seg * kM;
-                mbar_expect_tx(full + s, TX);
-                unsigned char *xd = xs + s * L::XSTAGE;
-                // maps: (C, z, y, x + n * extent_x), boxes of 8 channels; the
-                // x + dx planes stay inside this batch entry
-                for (int dx = 0; dx < 3; ++dx)
-                    for (int cg = 0; cg < CG; ++cg)
-                        tma_load_4d(xd + (dx * CG + cg) * kBox, &x_map, cg * 8, z0, y, b * (a.xo + 2) + x + dx,
+                for (int j = 0; j < ylen; ++j, ++it) {
+                    const int s = it & 1, u = it >> 1;
+                    // tile it-2 done: its gradient stage and the ring row that
+                    // this tile's new row replaces are free
+                    if (u > 0 && !mbar_wait(empty + s, (u - 1) & 1, kWaitBudget)) {
+                        ok = false;
+                        break;
+                    }
+                    // a new column loads rows y0, y0+1 too, over the rows
+                    // that tile it-1 still reads
+                    if (j == 0 && it > 0 && !mbar_wait(empty + ((it - 1) & 1), ((it - 1) >> 1) & 1, kWaitBudget)) {
+                        ok = false;
+                        break;
+                    }
+                    const int first = j == 0 ? 0 : 2;            // new rows: j+first .. j+2
+                    mbar_expect_tx(full + s, (3 - first) * ROWTX + GTX);
+                    for (int dr = first; dr < 3; ++dr) {
+                        const int slot = (it + dr) & 3;
+                        for (int dx = 0; dx < 3; ++dx)
+                            for (int cg = 0; cg < CG; ++cg)
+                                tma_load_4d(xr + (dx * CG + cg) * L::GROUP + slot * L::ROWB, &x_map, cg * 8, z0,
+                                            y0 + j + dr, b * (a.xo + 2) + x + dx, full + s);
+                    }
+                    unsigned char *gd = gs + s * L::GSTAGE;
+                    for (int g = 0; g < GG; ++g)
+                        tma_load_4d(gd + g * kM * 16, &g_map, g * 8, z0 + 2, y0 + j + 2, b * (a.xo + 4) + x + 2,
                                     full + s);
-                unsigned char *gd = gs + s * L::GSTAGE;
-                for (int g = 0; g < GG; ++g)
-                    tma_load_4d(gd + g * kM * 16, &g_map, g * 8, z0 + 2, y + 2, b * (a.xo + 4) + x + 2, full + s);
+                }
             }
             for (int j = it - 2 < 0 ? 0 : it - 2; j < it; ++j) ok &= mbar_wait(full + (j & 1), (j >> 1) & 1, kWaitBudget);
         }
@@ -534,33 +551,40 @@ __global__ void __launch_bounds__(kConvThreads, 1)
         // the whole warp runs the issue loop; the elected lane issues each
         // tile's MMAs and its commit (see elect_one)
         int it = 0;
-        for (int tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, ++it) {
-            const int s = it & 1, u = it >> 1;
-            if (!warp_wait(full + s, u & 1)) {
-                ok = false;
-                break;
-            }
-            tc::fence_after();
-            const int seg = tile % a.nseg;
+        for (int unit = blockIdx.x; ok && unit < a.nunits; unit += gridDim.x) {
+            int r = unit;
+            const int yc = r % a.nyc; r /= a.nyc;
+            const int seg = r % a.nseg;
+            const int ylen = min(a.ych, a.yo - yc * a.ych);
             const int len = min(kM, a.zo - seg * kM);
             const int nk = (len + 15) >> 4;
-            const uint32_t xa = smem_u32(xs + s * L::XSTAGE);
-            const uint32_t ga = smem_u32(gs + s * L::GSTAGE);
-            if (tc::elect_one()) {
-#pragma unroll 1
-                for (int ks = 0; ks < nk; ++ks) {
-                    const uint64_t bd = tc::sdesc(ga + (uint32_t)(ks * 256), 128, kM * 16);
-                    const uint32_t acc = (it | ks) != 0;
-#pragma unroll
-                    for (int j = 0; j < 9; ++j) {
-                        const int dy = j / 3, dz = j % 3;
-                        const uint32_t aa = xa + (uint32_t)((dy * kWz + dz + 16 * ks) * 16);
-                        tc::mma_bf16(tbase + (uint32_t)(j * COUT), tc::sdesc(aa, 128, kBox), bd, IDESC, acc);
-                    }
+            for (int j = 0; j < ylen; ++j, ++it) {
+                const int s = it & 1, u = it >> 1;
+                if (!warp_wait(full + s, u & 1)) {
+                    ok = false;
+                    break;
                 }
-                tc::commit(empty + s);
+                tc::fence_after();
+                const uint32_t xa = smem_u32(xr);
+                const uint32_t ga = smem_u32(gs + s * L::GSTAGE);
+                if (tc::elect_one()) {
+#pragma unroll 1
+                    for (int ks = 0; ks < nk; ++ks) {
+                        const uint64_t bd = tc::sdesc(ga + (uint32_t)(ks * 256), 128, kM * 16);
+                        const uint32_t acc = (it | ks) != 0;
+#pragma unroll
+                        for (int t9 = 0; t9 < 9; ++t9) {
+                            const int dy = t9 / 3, dz = t9 % 3;
+                            const uint32_t aa =
+                                xa + (uint32_t)(((it + dy) & 3) * L::ROWB) + (uint32_t)((dz + 16 * ks) * 16);
+                            tc::mma_bf16(tbase + (uint32_t)(t9 * COUT), tc::sdesc(aa, 128, L::GROUP), bd, IDESC,
+                                         acc);
+                        }
+                    }
+                    tc::commit(empty + s);
+                }
+                __syncwarp();
             }
-            __syncwarp();
         }
         if (tc::elect_one()) tc::commit(done);
         __syncwarp();
@@ -569,7 +593,7 @@ __global__ void __launch_bounds__(kConvThreads, 1)
         const int m = 32 * q + lane;            // TMEM lane = row of D
         const int jgrp = m >> 3, ci_lo = m & 7;
         const int dx = jgrp / CG, cg = jgrp % CG;
-        const bool have = mytiles > 0;
+        const bool have = blockIdx.x < a.nunits;
         if (have && !warp_wait(done, 0)) ok = false;
         tc::fence_after();
         float *wpart = a.part + (size_t)blockIdx.x * (COUT * CIN * 27 + COUT);

@@ -406,15 +406,21 @@ cudaError_t launch_wgrad(dg_net *net, const void *x_in, const void *g_pad, int n
     });
     if (attr_err != cudaSuccess) return attr_err;
     CUtensorMap mx, mg;
-    if (!map_wgrad(&mx, x_in, CIN, nb, xo + 2, yo + 2, zo + 2, kWz, 3)) return cudaErrorInvalidValue;
+    if (!map_wgrad(&mx, x_in, CIN, nb, xo + 2, yo + 2, zo + 2, kWz, 1)) return cudaErrorInvalidValue;
     if (!map_wgrad(&mg, g_pad, COUT, nb, xo + 4, yo + 4, zo + 4, kM, 1)) return cudaErrorInvalidValue;
     WgradArgs a;
     a.nb = nb; a.xo = xo; a.yo = yo; a.zo = zo;
     a.nseg = (zo + kM - 1) / kM;
-    a.ntiles = nb * xo * yo * a.nseg;
+    // columns along y split into chunks so that every block gets ~6 units
+    const long long cols = (long long)nb * xo * a.nseg;
+    const long long want = 6LL * net->nsm;
+    int nyc = (int)std::min<long long>(yo, std::max<long long>(1, (want + cols - 1) / cols));
+    a.ych = (yo + nyc - 1) / nyc;
+    a.nyc = (yo + a.ych - 1) / a.ych;
+    a.nunits = (int)(cols * a.nyc);
     a.part = net->wpart;
     a.status = net->status;
-    const int grid = std::max(1, std::min(a.ntiles, net->nsm));
+    const int grid = std::max(1, std::min(a.nunits, net->nsm));
     kern<<<grid, kConvThreads, L::BYTES, net->stream>>>(mx, mg, a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
