@@ -182,7 +182,7 @@ __global__ void loss_kernel(const float *__restrict__ out, const float *__restri
         float g[kIO];
 #pragma unroll
         for (int c = 0; c < kIO; ++c) {
-            const float d = c < nout ? out[v * kIO + c] - tgt[v * kIO + c] : 0.0f;
+            const float d = c < nout ? out[v * kIO + c] - tgt[(size_t)v * kIO + c] : 0.0f;
             acc += (double)d * d;
             g[c] = scale * d;
         }
@@ -255,16 +255,18 @@ __global__ void sample_weight_kernel(const double *__restrict__ part, int n, int
     }
 }
 
+// I: the index type, 32-bit whenever the batch's cells fit (divisions by
+// the crop extent are then 32-bit).
+template <class I>
 __global__ void flux_residual_kernel(const float *__restrict__ out, const float *__restrict__ tgt, int n, int s,
                                      float scale, const float *__restrict__ wsample, float *__restrict__ gbuf,
                                      double *part) {
     __shared__ double red[32];
-    const long long total = (long long)n * s * s * s;
+    const I total = (I)n * s * s * s;
     const int o = s + 1;
     double acc = 0.0;
-    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < total;
-         v += (long long)gridDim.x * blockDim.x) {
-        long long r = v;
+    for (I v = blockIdx.x * (I)blockDim.x + threadIdx.x; v < total; v += (I)gridDim.x * blockDim.x) {
+        I r = v;
         const int iz = r % s; r /= s;
         const int iy = r % s; r /= s;
         const int ix = r % s;
@@ -276,10 +278,10 @@ __global__ void flux_residual_kernel(const float *__restrict__ out, const float 
             float du = 0.0f;
 #pragma unroll
             for (int d = 0; d < 3; ++d) du += out[c0 + 5 * d + c] - out[lo[d] + 5 * d + c];
-            const float res = du - tgt[v * kIO + c];
+            const float res = du - tgt[(size_t)v * kIO + c];
             const float wb = wsample[b];
             acc += (double)wb * res * res;
-            gbuf[v * 5 + c] = scale * wb * res;
+            gbuf[(size_t)v * 5 + c] = scale * wb * res;
         }
     }
 #pragma unroll
@@ -296,12 +298,12 @@ __global__ void flux_residual_kernel(const float *__restrict__ out, const float 
 // Flux-form loss, pass 2: dL/dF_{d,c}(q) = g_c(q-1) - g_c(q-1+e_d) (terms whose
 // target cell lies outside the target are absent), as BF16 into the interior
 // of the output-gradient buffer padded by 2; channel 15 is zero.
+template <class I>
 __global__ void flux_grad_kernel(const float *__restrict__ gbuf, int n, int s, __nv_bfloat16 *__restrict__ dz) {
     const int o = s + 1;
-    const long long total = (long long)n * o * o * o;
-    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < total;
-         v += (long long)gridDim.x * blockDim.x) {
-        long long r = v;
+    const I total = (I)n * o * o * o;
+    for (I v = blockIdx.x * (I)blockDim.x + threadIdx.x; v < total; v += (I)gridDim.x * blockDim.x) {
+        I r = v;
         const int qz = r % o; r /= o;
         const int qy = r % o; r /= o;
         const int qx = r % o;
@@ -796,9 +798,15 @@ int32_t dg_net_forward_backward_flux(dg_net *net, const void *feat, const float 
     const int lblocks = (int)std::min<long long>(4096, (ntgt + 255) / 256);
     sample_power_kernel<<<dim3(kPowBlocks, n), 256, 0, net->stream>>>(target, s, net->pow_part);
     sample_weight_kernel<<<1, 64, 0, net->stream>>>(net->pow_part, n, s, balance, 0.01f, ws.wsample);
-    flux_residual_kernel<<<lblocks, 256, 0, net->stream>>>(ws.out, target, n, s, scale, ws.wsample, ws.gbuf,
-                                                           net->loss_part);
-    flux_grad_kernel<<<1024, 256, 0, net->stream>>>(ws.gbuf, n, s, ws.dz[3]);
+    if ((long long)n * (s + 1) * (s + 1) * (s + 1) < (1LL << 32)) {
+        flux_residual_kernel<unsigned><<<lblocks, 256, 0, net->stream>>>(ws.out, target, n, s, scale, ws.wsample,
+                                                                        ws.gbuf, net->loss_part);
+        flux_grad_kernel<unsigned><<<1024, 256, 0, net->stream>>>(ws.gbuf, n, s, ws.dz[3]);
+    } else {
+        flux_residual_kernel<unsigned long long><<<lblocks, 256, 0, net->stream>>>(ws.out, target, n, s, scale,
+                                                                                  ws.wsample, ws.gbuf, net->loss_part);
+        flux_grad_kernel<unsigned long long><<<1024, 256, 0, net->stream>>>(ws.gbuf, n, s, ws.dz[3]);
+    }
     NET_CUDA(net, cudaGetLastError());
     if (int r = backward(net, feat, n, x, y, z)) return r;
     if (int r = check_status(net)) return r;
