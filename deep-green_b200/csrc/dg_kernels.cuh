@@ -81,15 +81,16 @@ inline int step_grid_blocks(int nx, int ny, int nz, int kind, int chunk) {
     return tiles_z * tiles_y * chunks;
 }
 // Default x-planes per block: enough blocks for ~14 waves of resident CTAs
-// (2 per SM on 148 SMs; measured best on 512^3: 64 planes per block), at
-// least 32 planes per block (each block re-stages 4 planes at its ends).
+// (2 per SM on 148 SMs), at least 20 planes per block (each block re-stages
+// 4 planes at its ends).  Measured: flat within 1 % from 43 to 74 planes on
+// 512^3; best at 22 planes on 256^3 (5 % faster than 32).
 inline int choose_chunk(int nx, int ny, int nz, int kind) {
     const int ty = step_tile_rows(kind);
     const long long tiles = (long long)((ny - 4 + ty - 1) / ty) * ((nz - 4 + kTZ - 1) / kTZ);
     const int nxi = nx - 4;
     const long long target = 148LL * 2 * 14;
     long long chunks = (target + tiles - 1) / tiles;
-    const long long maxc = nxi / 32 > 0 ? nxi / 32 : 1;
+    const long long maxc = nxi / 20 > 0 ? nxi / 20 : 1;
     if (chunks > maxc) chunks = maxc;
     if (chunks < 1) chunks = 1;
     return (int)((nxi + chunks - 1) / chunks);
