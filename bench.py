@@ -94,6 +94,20 @@ def dist_setup():
     return world, rank, local
 
 
+def job_rate(ms_local, cells_per_rank, steps, world, device=None):
+    """Whole-job rate of `world` independent replicas: all ranks' cell
+    updates over the slowest rank's device time (all_reduce MAX, the same
+    collective on every rank).  Returns (GCUPS, max ms)."""
+    ms = float(ms_local)
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([ms], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return world * cells_per_rank * steps / (ms * 1e-3) / 1e9, ms
+
+
 def workload_name(case, n):
     return f"{case}3d_{n}^3_fp32_minmod_cfl{CFL}"
 
@@ -309,14 +323,9 @@ def run_ours(args, world, rank, local):
     ms = start.elapsed_time(end)
     dts = ctx.get_dts(args.steps)
     status = ctx.status()
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
     cells = n ** 3
+    value, ms = job_rate(ms, cells, args.steps, world, device=dev)
     ms_step = ms / args.steps
-    value = world * cells * args.steps / (ms * 1e-3) / 1e9
 
     # end to end through the C ABI from pinned host buffers
     e2e = None
@@ -341,14 +350,9 @@ def run_ours(args, world, rank, local):
         e1.record(stream)
         e1.synchronize()
         barrier()
-        e2e_ms = e0.elapsed_time(e1)
-        if world > 1:
-            import torch.distributed as dist
-            t = torch.tensor([e2e_ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_ms = float(t.item())
+        e2e_value, e2e_ms = job_rate(e0.elapsed_time(e1), cells, args.steps, world, device=dev)
         state_bytes = 5 * (n + 4) ** 3 * 4
-        e2e = {"value": world * cells * args.steps / (e2e_ms * 1e-3) / 1e9, "unit": UNIT,
+        e2e = {"value": e2e_value, "unit": UNIT,
                "h2d_bytes_per_step": state_bytes / args.steps,
                "d2h_bytes_per_step": state_bytes / args.steps + 8,
                "ms_total": e2e_ms, "path": "dg_set_conserved + K x dg_compute_step(1) + dg_get_conserved"}
@@ -409,11 +413,7 @@ def run_batch(args, world, rank, local):
         end.record(stream)
         end.synchronize()
     ms = start.elapsed_time(end)
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    value, ms = job_rate(ms, cells, args.steps, world, device=dev)
     if rank != 0:
         return
     peak, peak_kind = peaks()
@@ -421,7 +421,7 @@ def run_batch(args, world, rank, local):
     achieved = BYTES_PER_CELL["f32"] * cells / (ms_step * 1e-3) / 1e9
     r, c, items = bt.tiling()
     line = {
-        "metric": METRIC, "value": world * cells * args.steps / (ms * 1e-3) / 1e9, "unit": UNIT, "n_gpus": world,
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "batch64_riemann_fp32_minmod_cfl0.4", "grids": len(shapes), "cells": cells,
