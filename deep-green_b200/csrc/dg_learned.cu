@@ -338,7 +338,7 @@ __device__ __forceinline__ float round_dithered(double x, double h) {
     return (float)(x + h * (double)ulp);
 }
 
-constexpr int kApplyVals = 16;  // per-block partials of the apply pass (+ the wave-speed maximum)
+constexpr int kApplyVals = 11;  // per-block partials of the apply pass (+ the wave-speed maximum)
 
 // Ghosted coordinate of the periodic image of interior coordinate c
 // (0..n-1), or -1: cells 0, 1 reappear as ghosts n+2, n+3 and cells n-2,
@@ -396,7 +396,7 @@ __global__ void __launch_bounds__(kLearnThreads) apply_kernel(View u1, float *__
 #pragma unroll
     for (int c = 0; c < 5; ++c) mean[c] = ctl->mean[c];
     const unsigned long long step = ctl->steps;
-    // acc: 0-4 sum of u - old, 5-9 sum |old|, 10 positivity violations, 11-15 sum old
+    // acc: 0-4 sum of u - old, 5-9 sum |old|, 10 positivity violations
     double acc[kApplyVals];
 #pragma unroll
     for (int k = 0; k < kApplyVals; ++k) acc[k] = 0.0;
@@ -428,7 +428,6 @@ __global__ void __launch_bounds__(kLearnThreads) apply_kernel(View u1, float *__
                 cu[c] = u[c][j];
                 acc[c] += (double)u[c][j] - o;
                 acc[5 + c] += fabs(o);
-                acc[11 + c] += o;
             }
             acc[10] += (keep[j] || positive(cu, g.k.gm1, g.k.inv_vol)) ? 0.0 : 1.0;
             Phys<float, false>::prim(cu, w, g.k);
