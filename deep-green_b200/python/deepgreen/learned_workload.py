@@ -79,7 +79,7 @@ def evaluate_case(net, norm, kind, seed, n_coarse, fine_steps, log=print, **kw):
     warm.synchronize()
     cw.close()
     warm.close()
-    # plain fine solve: the judge (reads dt every step, as the reference loop)
+    # plain fine solve: the reference solution (reads dt every step, as the reference loop)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     t_end = 0.0
