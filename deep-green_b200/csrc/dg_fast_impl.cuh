@@ -748,7 +748,10 @@ __global__ void __launch_bounds__(32 * W, 2) batch_step_kernel(const GridArgs<fl
         for (int i = tid; i < kWords; i += 32 * W)
             reinterpret_cast<int *>(&s_args)[i] = reinterpret_cast<const int *>(&args[bi.g])[i];
         __syncthreads();
-        const bool ok = Kernel<W, R>::run_tile(s_args, &maps[bi.g], bi.tz, bi.ty, bi.cx, chunk, bi.local, s_args.nparts,
+        // a register copy: the tile code reads the arguments all through the
+        // march, and shared-memory loads of them cost ~10 % of the step
+        const GridArgs<float> ga = s_args;
+        const bool ok = Kernel<W, R>::run_tile(ga, &maps[bi.g], bi.tz, bi.ty, bi.cx, chunk, bi.local, ga.nparts,
                                                smem_raw);
         __syncthreads();
         if (!ok) return;
