@@ -180,7 +180,10 @@ template <int W, int R> struct Smem {
     int is_last;
 };
 
-template <int W, int R> struct Kernel {
+// SKIP_PAD: leave the states of cells past the first ghost layer (the
+// padding of ragged tiles, common in batches of small grids) uncomputed; the
+// single-grid kernel keeps the smaller code.
+template <int W, int R, bool SKIP_PAD = false> struct Kernel {
     using Sm = Smem<W, R>;
     static constexpr int TY = Sm::TY, NT = Sm::NT, NOWN = Sm::NOWN;
 
@@ -312,11 +315,20 @@ template <int W, int R> struct Kernel {
             }
             predict(c, sx, sy, sz, hd, k, xt);
         } else {
+            // cells past the first ghost layer (the padding of a ragged tile)
+            // feed no face of an interior cell: their states may be left zero
+            const bool needA = !SKIP_PAD || (gyA <= a.ny - 2 && gzA <= a.nz - 2);
+            const bool needB = !SKIP_PAD || (gyB <= a.ny - 2 && gzB <= a.nz - 2);
 #pragma unroll
             for (int r = 0; r < 2; ++r) {
                 float t[5], gx[5], gy[5], gz[5];
-                cell_scalar(s, a, k, hd, sm, s0, sp, r ? ryB : ryA, r ? rzB : rzA, r ? gyB : gyA, r ? gzB : gzA, t, gx,
-                            gy, gz);
+                if (r ? needB : needA) {
+                    cell_scalar(s, a, k, hd, sm, s0, sp, r ? ryB : ryA, r ? rzB : rzA, r ? gyB : gyA, r ? gzB : gzA, t,
+                                gx, gy, gz);
+                } else {
+#pragma unroll
+                    for (int f = 0; f < 5; ++f) t[f] = gx[f] = gy[f] = gz[f] = 0.0f;
+                }
 #pragma unroll
                 for (int f = 0; f < 5; ++f) {
                     setc(xt[f], r, t[f]);
@@ -751,7 +763,7 @@ __global__ void __launch_bounds__(32 * W, 2) batch_step_kernel(const GridArgs<fl
         // a register copy: the tile code reads the arguments all through the
         // march, and shared-memory loads of them cost ~10 % of the step
         const GridArgs<float> ga = s_args;
-        const bool ok = Kernel<W, R>::run_tile(ga, &maps[bi.g], bi.tz, bi.ty, bi.cx, chunk, bi.local, ga.nparts,
+        const bool ok = Kernel<W, R, true>::run_tile(ga, &maps[bi.g], bi.tz, bi.ty, bi.cx, chunk, bi.local, ga.nparts,
                                                smem_raw);
         __syncthreads();
         if (!ok) return;
