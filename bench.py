@@ -33,6 +33,9 @@ measured BF16 peak beside it.  Takes about two minutes.
 convolutions, random weights) on an (n+8)^3 input, as the corrector runs it
 on an n^3 grid; TFLOP/s against the measured BF16 peak.
 
+--case corrector: one corrected coarse step (plain step, network, checked
+correction) on an n^3 periodic KH state with random network weights.
+
 --case snapshot: the state output of the reference's time loop
 (save_to_disk, io.rs:5-196) for the 512^3 state: capture time on the step
 stream, device->host copy rate, the step time while a copy is in flight,
@@ -74,7 +77,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=512, help="interior cells per axis")
-    ap.add_argument("--case", default="sod", choices=["sod", "vortex", "batch64", "learned", "netfwd", "snapshot"])
+    ap.add_argument("--case", default="sod", choices=["sod", "vortex", "batch64", "learned", "netfwd", "snapshot", "corrector"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -603,6 +606,51 @@ def run_snapshot(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def run_corrector(args, world, rank, local):
+    """One corrected coarse step (plain step + the correction network + the
+    checked correction) on an n^3 periodic KH state, random network weights:
+    the per-step cost of the learned workload's coarse solve."""
+    import torch
+    from deepgreen import learned
+    from deepgreen.net import Net
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n = args.n
+    prim, _ = learned.initial_state("kh", n, 5, shear=0.5, ratio=2.0)
+    g = learned.grid(n, device=local)
+    g.set_primitives(prim)
+    del prim
+    net = Net(learned.INPUTS, learned.OUTPUTS, seed=0, out_scale=0.01)
+    norm = learned.Norm.identity()
+    for c in range(5):
+        norm.out_std[c] = 1e-4
+    for c in range(14, 16):
+        norm.in_inv_std[c] = 0.0
+    cor = learned.Corrector(g, net, norm)
+    cor.step(args.warmup)
+    g.synchronize()
+    stream = torch.cuda.ExternalStream(g.stream(), device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        cor.step(args.steps)
+        e1.record(stream)
+        e1.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    st = cor.stats()
+    cor.close()
+    line = {
+        "metric": "corrected coarse step time", "value": ms, "unit": "ms", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "none", "vs_baseline": None,
+        "dtype": "bf16 network, f32 state", "data": "synthetic",
+        "config": {"workload": f"corrected_step_kh_{n}^3", "network": "14-32-32-32-15, 3x3x3, random weights"},
+        "fallback_steps": st["fallback_steps"], "clocks": clk.summary(), "gpu_launches": 9 * args.steps,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup()
@@ -617,6 +665,8 @@ def main():
             run_netfwd(args, world, rank, local)
         elif args.case == "snapshot":
             run_snapshot(args, world, rank, local)
+        elif args.case == "corrector":
+            run_corrector(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:
