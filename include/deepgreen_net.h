@@ -150,7 +150,8 @@ typedef struct dg_learned_stats {
     uint64_t violations;      /* cells that lost positivity after the mean removal (each rejects its step) */
 } dg_learned_stats;
 
-/* A corrector couples a coarse FP32 context (cubic, periodic) and a network
+/* A corrector couples a coarse FP32 context (cubic, periodic, n a multiple of
+ * 4 and at most 1024 cells per axis) and a network
  * (14 inputs, 15 flux outputs).  Each step: one plain step; the network's
  * correction, zero in cells where rho or p of the corrected state would not
  * be positive, minus its mean over the other cells; the whole step falls back
