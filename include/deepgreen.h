@@ -142,8 +142,8 @@ int32_t dg_get_dts(dg_ctx *ctx, int32_t nsteps, double *dts);
 int32_t dg_synchronize(dg_ctx *ctx);
 /* The cudaStream_t the context launches on, as void*. */
 int32_t dg_get_stream(dg_ctx *ctx, void **stream);
-/* Number of kernel launches one step makes (1) and the grid of the step
- * kernel (blocks, threads per block, x-planes per block). */
+/* The grid of the step kernel (blocks, threads per block, x-planes per
+ * block); one step is one launch of it.  Any pointer may be NULL. */
 int32_t dg_step_launch_shape(dg_ctx *ctx, int32_t *blocks, int32_t *threads, int32_t *chunk);
 /* Override the x-planes per block of the step kernel (0 = automatic). */
 int32_t dg_set_chunk(dg_ctx *ctx, int32_t chunk);
