@@ -139,7 +139,7 @@ int rebuild(dg_batch *b) {
         long long cells = 0;
         for (auto &s : b->g) cells += (long long)(s.nx - 4) * (s.ny - 4) * (s.nz - 4);
         // ~14 waves of 2 CTAs per SM worth of items, at least 16 planes
-        const long long items_target = 148LL * 2 * 14;
+        const long long items_target = 2LL * kSms * 14;
         const long long tile_cells = (long long)ty * kTZ;
         long long c = cells / std::max<long long>(1, items_target * tile_cells);
         chunk = (int)std::max<long long>(16, c);
@@ -219,15 +219,13 @@ template <int W> cudaError_t prepare_kernel() {
 // one step of every grid (no synchronisation)
 int launch_one(dg_batch *b, int parity) {
     B_CUDA(b, cudaMemsetAsync(b->d_queue, 0, sizeof(unsigned), b->stream));
-    const int ctas = std::min(b->nitems, 148 * 2);
     if (b->tile_rows == 16) {
-        fastk::batch_step_kernel<8, kRing><<<ctas, dim3(32, 8), smem_bytes<8>(), b->stream>>>(
+        fastk::batch_step_kernel<8, kRing><<<std::min(b->nitems, kSms * 2), dim3(32, 8), smem_bytes<8>(), b->stream>>>(
             b->d_args[parity], b->d_maps[parity], b->d_items, b->nitems, b->d_queue, b->chunk_used);
     } else {
-        fastk::batch_step_kernel<4, kRing><<<std::min(b->nitems, 148 * 4), dim3(32, 4), smem_bytes<4>(), b->stream>>>(
+        fastk::batch_step_kernel<4, kRing><<<std::min(b->nitems, kSms * 4), dim3(32, 4), smem_bytes<4>(), b->stream>>>(
             b->d_args[parity], b->d_maps[parity], b->d_items, b->nitems, b->d_queue, b->chunk_used);
     }
-    (void)ctas;
     B_CUDA(b, cudaGetLastError());
     return DG_OK;
 }

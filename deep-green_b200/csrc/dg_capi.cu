@@ -21,8 +21,8 @@ using namespace dg;
 
 namespace {
 
-std::string g_create_err = "no error";
-std::mutex g_err_mu;
+// message of the calling thread's last failure outside a context
+thread_local std::string g_create_err = "no error";
 
 PFN_cuTensorMapEncodeTiled_v12000 get_encode_fn() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -220,20 +220,14 @@ namespace {
 __global__ void set_next_dt_kernel(DevCtl *ctl, double dt) { ctl->dt[ctl->step & 1] = dt; }
 }  // namespace
 
-void dg::set_global_error(const std::string &msg) {
-    std::lock_guard<std::mutex> g(g_err_mu);
-    g_create_err = msg;
-}
+void dg::set_global_error(const std::string &msg) { g_create_err = msg; }
 
 extern "C" {
 
 int32_t dg_abi_version(void) { return DG_ABI_VERSION; }
 
 int32_t dg_create(const dg_sim_info *info, dg_ctx **out) {
-    auto set_err = [](const std::string &m) {
-        std::lock_guard<std::mutex> g(g_err_mu);
-        g_create_err = m;
-    };
+    auto set_err = [](const std::string &m) { g_create_err = m; };
     if (!out) return DG_ERR_INVALID;
     *out = nullptr;
     if (!info) { set_err("null info"); return DG_ERR_INVALID; }
@@ -530,11 +524,7 @@ int32_t dg_status(dg_ctx *c, uint32_t *flags) {
 }
 
 const char *dg_last_error(const dg_ctx *c) {
-    if (!c) {
-        std::lock_guard<std::mutex> g(g_err_mu);
-        return g_create_err.c_str();
-    }
-    return c->err.c_str();
+    return c ? c->err.c_str() : g_create_err.c_str();
 }
 
 }  // extern "C"

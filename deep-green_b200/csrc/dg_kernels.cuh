@@ -56,7 +56,9 @@ template <class T> struct GridArgs {
     Partial *part;
 };
 
-constexpr int kReduceBlocks = 148 * 8;   // grid of the state-reduction kernel
+// SMs of a B200 (2 dies x 74); grid sizes below are multiples of it
+constexpr int kSms = 148;
+constexpr int kReduceBlocks = kSms * 8;   // grid of the state-reduction kernel
 
 // The three step kernels: reference rounding in double and in float
 // (dg_step_impl.cuh) and the fast float kernel (dg_fast_impl.cuh).
@@ -81,14 +83,14 @@ inline int step_grid_blocks(int nx, int ny, int nz, int kind, int chunk) {
     return tiles_z * tiles_y * chunks;
 }
 // Default x-planes per block: enough blocks for ~14 waves of resident CTAs
-// (2 per SM on 148 SMs), at least 20 planes per block (each block re-stages
+// (2 per SM), at least 20 planes per block (each block re-stages
 // 4 planes at its ends).  Measured: flat within 1 % from 43 to 74 planes on
 // 512^3; best at 22 planes on 256^3 (5 % faster than 32).
 inline int choose_chunk(int nx, int ny, int nz, int kind) {
     const int ty = step_tile_rows(kind);
     const long long tiles = (long long)((ny - 4 + ty - 1) / ty) * ((nz - 4 + kTZ - 1) / kTZ);
     const int nxi = nx - 4;
-    const long long target = 148LL * 2 * 14;
+    const long long target = 2LL * kSms * 14;
     long long chunks = (target + tiles - 1) / tiles;
     const long long maxc = nxi / 20 > 0 ? nxi / 20 : 1;
     if (chunks > maxc) chunks = maxc;

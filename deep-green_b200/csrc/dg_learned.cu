@@ -19,7 +19,7 @@ using namespace dg;
 
 namespace {
 
-constexpr int kLearnBlocks = 148 * 4;
+constexpr int kLearnBlocks = kSms * 4;
 constexpr int kLearnThreads = 256;
 
 // A conserved FP32 state: 5 fields of ghosted rows, interior cube of n.
@@ -523,7 +523,7 @@ NormDev to_dev(const dg_learned_norm *n) {
     return d;
 }
 
-std::string g_learn_err;
+thread_local std::string g_learn_err;   // the calling thread's last failure
 
 int lfail(int code, const std::string &m) {
     g_learn_err = m;

@@ -12,6 +12,7 @@
 
 #include "../../include/deepgreen_net.h"
 #include "dg_conv.cuh"
+#include "dg_host.h"
 #include "dg_net_impl.h"
 
 using namespace dg;
@@ -60,15 +61,12 @@ struct dg_net {
 
 namespace {
 
-std::mutex g_net_err_mu;
-std::string g_net_err;
+// message of the calling thread's last failure outside a network
+thread_local std::string g_net_err;
 
 int fail(dg_net *n, int code, const std::string &m) {
     if (n) n->err = m;
-    else {
-        std::lock_guard<std::mutex> g(g_net_err_mu);
-        g_net_err = m;
-    }
+    else g_net_err = m;
     return code;
 }
 
@@ -363,11 +361,8 @@ cudaError_t launch_conv(dg_net *net, const void *in, int nb, int xi, int yi, int
                         ConvArgs a, cudaStream_t st) {
     using L = ConvSmem<CIN, COUT>;
     auto kern = conv_fwd_kernel<CIN, COUT, EPI>;
-    static std::once_flag once;
-    static cudaError_t attr_err = cudaSuccess;
-    std::call_once(once, [&] {
-        attr_err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::BYTES);
-    });
+    static std::atomic<unsigned long long> attr_set{0};
+    const cudaError_t attr_err = ensure_dynamic_smem(kern, L::BYTES, attr_set);
     if (attr_err != cudaSuccess) return attr_err;
     CUtensorMap m;
     if (!map_conv_input(&m, in, CIN, nb, xi, yi, zi)) return cudaErrorInvalidValue;
@@ -401,11 +396,8 @@ cudaError_t launch_wgrad(dg_net *net, const void *x_in, const void *g_pad, int n
                          float *gb) {
     using L = WgradSmem<CIN, COUT>;
     auto kern = conv_wgrad_kernel<CIN, COUT>;
-    static std::once_flag once;
-    static cudaError_t attr_err = cudaSuccess;
-    std::call_once(once, [&] {
-        attr_err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::BYTES);
-    });
+    static std::atomic<unsigned long long> attr_set{0};
+    const cudaError_t attr_err = ensure_dynamic_smem(kern, L::BYTES, attr_set);
     if (attr_err != cudaSuccess) return attr_err;
     CUtensorMap mx, mg;
     if (!map_wgrad(&mx, x_in, CIN, nb, xo + 2, yo + 2, zo + 2, kWz, 1)) return cudaErrorInvalidValue;
@@ -878,9 +870,7 @@ int32_t dg_net_synchronize(dg_net *net) {
 void *dg_net_get_stream(dg_net *net) { return net ? net->stream : nullptr; }
 
 const char *dg_net_last_error(const dg_net *net) {
-    if (net) return net->err.c_str();
-    std::lock_guard<std::mutex> g(g_net_err_mu);
-    return g_net_err.c_str();
+    return net ? net->err.c_str() : g_net_err.c_str();
 }
 
 }  // extern "C"

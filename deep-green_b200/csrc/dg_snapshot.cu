@@ -23,7 +23,7 @@ using namespace dg;
 
 namespace {
 
-std::string g_snap_err;
+thread_local std::string g_snap_err;   // the calling thread's last failure
 
 int sfail(int code, const std::string &msg) {
     g_snap_err = msg;

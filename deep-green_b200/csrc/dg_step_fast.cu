@@ -1,6 +1,7 @@
 // dg_step_fast.cu -- FP32 step with the fast arithmetic policy (fused
 // multiply-add contraction allowed).  Kernels: dg_step_impl.cuh.
 #include "dg_fast_impl.cuh"
+#include "dg_host.h"
 #include "dg_step_impl.cuh"
 
 namespace dg {
@@ -10,15 +11,9 @@ cudaError_t launch_fast_step(const GridArgs<float> &a, const CUtensorMap *tmap, 
     using Sm = fastk::Smem<W, R>;
     auto kern = fastk::fast_step_kernel<W, R>;
     const int smem = (int)sizeof(Sm) + 1024;
-    static unsigned long long attr_set = 0;
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    static std::atomic<unsigned long long> attr_set{0};
+    const cudaError_t e = ensure_dynamic_smem(kern, smem, attr_set);
     if (e != cudaSuccess) return e;
-    if (dev >= 64 || !(attr_set & (1ull << dev))) {
-        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return e;
-        if (dev < 64) attr_set |= 1ull << dev;
-    }
     const int blocks = step_grid_blocks(a.nx, a.ny, a.nz, kFastF32, chunk);
     kern<<<blocks, dim3(32, W), smem, st>>>(a, *tmap, chunk);
     return cudaGetLastError();

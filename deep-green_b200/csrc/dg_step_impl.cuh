@@ -38,6 +38,7 @@
 #include <cstdio>
 
 #include "dg_common.cuh"
+#include "dg_host.h"
 
 namespace dg {
 
@@ -626,15 +627,9 @@ static cudaError_t launch_step_t(const GridArgs<T> &a, const CUtensorMap *tmap, 
     using S = StepSmem<T, TY, kRing>;
     auto kern = step_kernel<T, TY, LIM, kRing, EXACT>;
     const int smem = (int)sizeof(S) + 1024;
-    static unsigned long long attr_set = 0;  // per instantiation, one bit per device
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    static std::atomic<unsigned long long> attr_set{0};   // per instantiation
+    const cudaError_t e = ensure_dynamic_smem(kern, smem, attr_set);
     if (e != cudaSuccess) return e;
-    if (dev >= 64 || !(attr_set & (1ull << dev))) {
-        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        if (e != cudaSuccess) return e;
-        if (dev < 64) attr_set |= 1ull << dev;
-    }
     const int blocks = step_grid_blocks(a, chunk);
     kern<<<blocks, dim3(kTZ, TY), smem, st>>>(a, *tmap, chunk);
     return cudaGetLastError();
@@ -656,7 +651,7 @@ template <class T, bool EXACT> cudaError_t launch_reduce_policy(const GridArgs<T
 
 inline int flat_blocks(long long total) {
     long long b = (total + 255) / 256;
-    if (b > 148 * 16) b = 148 * 16;
+    if (b > kSms * 16) b = kSms * 16;
     if (b < 1) b = 1;
     return (int)b;
 }

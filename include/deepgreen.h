@@ -223,7 +223,7 @@ int32_t dg_snapshot_write(dg_snapshot *snap, const char *path);
 int32_t dg_snapshot_write_host(const char *path, int32_t dtype, const int32_t shape[3], int32_t nfields,
                                const char *const names[], const void *const data[], uint64_t steps,
                                const char *attrs);
-/* Message of the last failed snapshot call (shared by all snapshots). */
+/* Message of the calling thread's last failed snapshot call. */
 const char *dg_snapshot_last_error(const dg_snapshot *snap);
 
 /* ---- Batches: many independent grids, one persistent launch per step ----
@@ -259,8 +259,8 @@ const char *dg_batch_last_error(const dg_batch *b);
  * set (dg_set_*). */
 int32_t dg_status(dg_ctx *ctx, uint32_t *flags);
 
-/* Message of the last failed call on ctx (or of the last failed dg_create
- * when ctx is NULL).  Never NULL. */
+/* Message of the last failed call on ctx (or, when ctx is NULL, of the
+ * calling thread's last failed dg_create).  Never NULL. */
 const char *dg_last_error(const dg_ctx *ctx);
 
 #ifdef __cplusplus
