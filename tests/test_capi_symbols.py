@@ -52,3 +52,52 @@ def test_create_rejects_bad_configurations_without_gpu_work():
     info.bcs[0], info.bcs[1] = capi.PERIODIC, capi.OUTFLOW   # unpaired periodic face (grid.rs:55-63)
     assert lib.dg_create(ctypes.byref(info), ctypes.byref(h)) == capi.DG_ERR_INVALID
     assert not h.value
+
+
+def _bad_info(**kw):
+    info = capi.SimInfo()
+    info.nx = info.ny = info.nz = 8
+    info.nghosts = 2
+    info.ds, info.gamma, info.cfl = 0.1, 1.4, 0.4
+    for k, v in kw.items():
+        setattr(info, k, v)
+    return info
+
+
+def test_creation_errors_are_per_thread():
+    """dg_last_error(NULL) reports the calling thread's own failed create:
+    two threads fail differently, and each reads its own message after both
+    have failed."""
+    import ctypes
+    import threading
+    lib = capi.load()
+    barrier = threading.Barrier(2)
+    seen = {}
+
+    def worker(name, info):
+        h = ctypes.c_void_p()
+        rc = lib.dg_create(ctypes.byref(info), ctypes.byref(h))
+        barrier.wait(timeout=30)
+        seen[name] = (rc, lib.dg_last_error(None))
+
+    infos = {"ghosts": _bad_info(nghosts=3), "constants": _bad_info(gamma=0.5)}
+    threads = [threading.Thread(target=worker, args=item) for item in infos.items()]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join(timeout=60)
+    assert seen["ghosts"][0] == capi.DG_ERR_INVALID and b"nghosts" in seen["ghosts"][1]
+    assert seen["constants"][0] == capi.DG_ERR_INVALID and b"gamma" in seen["constants"][1]
+
+
+def test_batch_create_rejects_bad_grids_without_gpu_work():
+    import ctypes
+    lib = capi.load()
+    h = ctypes.c_void_p()
+    infos = (capi.SimInfo * 2)(_bad_info(), _bad_info(precision=capi.F64))
+    assert lib.dg_batch_create(2, infos, ctypes.byref(h)) == capi.DG_ERR_INVALID
+    assert b"FP32" in lib.dg_batch_last_error(None) and not h.value
+    infos = (capi.SimInfo * 2)(_bad_info(), _bad_info(nx=1))
+    assert lib.dg_batch_create(2, infos, ctypes.byref(h)) == capi.DG_ERR_INVALID
+    assert b"grid 1" in lib.dg_batch_last_error(None)
+    assert lib.dg_batch_create(0, infos, ctypes.byref(h)) == capi.DG_ERR_INVALID
