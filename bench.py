@@ -281,7 +281,8 @@ def run_reference(args, world, rank):
         "impl": "reference", "metric": METRIC, "value": gcups, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": workload_name(args.case, n), "sample": f"{n}x{n}x{nz_sample} slab of the grid"},
+        "config": {"workload": workload_name(args.case, n), "grid": [n, n, n], "ghosts": 2,
+                   "parallelism": f"host CPU, {cores} threads", "sample": f"{n}x{n}x{nz_sample} slab of the grid"},
         "cpu_baseline": {"value": gcups, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": f"{args.steps} steps of a {n}x{n}x{nz_sample} slab, same physics, FP32, "
                                    f"C restatement of the Rust step, OpenMP over {cores} threads"},

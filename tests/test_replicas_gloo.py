@@ -58,3 +58,25 @@ def test_single_rank_rate_needs_no_process_group():
     import bench
     value, ms = bench.job_rate(2.0, 500, 10, 1)
     assert ms == 2.0 and value == pytest.approx(500 * 10 / 2e-3 / 1e9)
+
+
+def test_reference_arm_line_keeps_the_contract(capsys):
+    """The reference arm (the CPU restatement on the host cores) prints one
+    JSON line with our arm's metric, unit and workload, a cpu_baseline block
+    and an e2e block without host transfers."""
+    import json
+    sys.path.insert(0, str(ROOT))
+    import bench
+
+    class Args:
+        n, steps, warmup, case, gpus = 16, 2, 1, "sod", 1
+    bench.run_reference(Args, 1, 0)
+    lines = [ln for ln in capsys.readouterr().out.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["metric"] == bench.METRIC and d["unit"] == bench.UNIT
+    assert d["higher_is_better"] is True and d["steps"] == 2 and d["warmup"] == 1 and d["n_gpus"] == 1
+    assert d["config"]["workload"] == bench.workload_name("sod", 16) and d["config"]["grid"] == [16, 16, 16]
+    assert d["value"] > 0 and d["cpu_baseline"]["value"] == d["value"]
+    assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
+    assert d["e2e"] == {"value": d["value"], "unit": bench.UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
