@@ -180,12 +180,21 @@ template <int W, int R> struct Smem {
     int is_last;
 };
 
+// LIM: the slope limiter as a compile-time constant, or -1 to read it from
+// the grid's arguments.
 // SKIP_PAD: leave the states of cells past the first ghost layer (the
 // padding of ragged tiles, common in batches of small grids) uncomputed; the
 // single-grid kernel keeps the smaller code.
-template <int W, int R, bool SKIP_PAD = false> struct Kernel {
+template <int W, int R, bool SKIP_PAD = false, int LIM = -1> struct Kernel {
     using Sm = Smem<W, R>;
     static constexpr int TY = Sm::TY, NT = Sm::NT, NOWN = Sm::NOWN;
+
+    // slope with the limiter fixed at compile time (LIM >= 0) or read at
+    // run time (LIM < 0: grids of a batch may differ)
+    template <class V> static __device__ __forceinline__ V slp(V qm, V q0, V qp, int lim) {
+        if constexpr (LIM >= 0) return slope(qm, q0, qp, LIM);
+        else return slope(qm, q0, qp, lim);
+    }
 
     static __device__ __forceinline__ float &P(Sm &s, int slot, int f, int ry, int rz) {
         return s.ring[slot * Sm::kSlotElems + f * Sm::kFieldElems + ry * kRZ + rz];
@@ -207,9 +216,9 @@ template <int W, int R, bool SKIP_PAD = false> struct Kernel {
             for (int f = 0; f < 5; ++f) {
                 const float c = P(s, s0, f, y, z);
                 w[f] = c;
-                gx[f] = slope(P(s, sm, f, y, z), c, P(s, sp, f, y, z), k.lim);
-                gy[f] = slope(P(s, s0, f, y - 1, z), c, P(s, s0, f, y + 1, z), k.lim);
-                gz[f] = slope(P(s, s0, f, y, z - 1), c, P(s, s0, f, y, z + 1), k.lim);
+                gx[f] = slp(P(s, sm, f, y, z), c, P(s, sp, f, y, z), k.lim);
+                gy[f] = slp(P(s, s0, f, y - 1, z), c, P(s, s0, f, y + 1, z), k.lim);
+                gz[f] = slp(P(s, s0, f, y, z - 1), c, P(s, s0, f, y, z + 1), k.lim);
             }
         };
         float w[5];
@@ -309,9 +318,9 @@ template <int W, int R, bool SKIP_PAD = false> struct Kernel {
                 const f2 yp = make_float2(P(s, s0, f, ryA + 1, rzA), P(s, s0, f, ryB + 1, rzB));
                 const f2 zm = make_float2(P(s, s0, f, ryA, rzA - 1), P(s, s0, f, ryB, rzB - 1));
                 const f2 zp = make_float2(P(s, s0, f, ryA, rzA + 1), P(s, s0, f, ryB, rzB + 1));
-                sx[f] = slope(xm, c[f], xp, k.lim);
-                sy[f] = slope(ym, c[f], yp, k.lim);
-                sz[f] = slope(zm, c[f], zp, k.lim);
+                sx[f] = slp(xm, c[f], xp, k.lim);
+                sy[f] = slp(ym, c[f], yp, k.lim);
+                sz[f] = slp(zm, c[f], zp, k.lim);
             }
             predict(c, sx, sy, sz, hd, k, xt);
         } else {
@@ -521,9 +530,9 @@ template <int W, int R, bool SKIP_PAD = false> struct Kernel {
                         const f2 yp = make_float2(c[f].y, P(s, s0, f, ry1 + 1, rzo));
                         const f2 zm = make_float2(P(s, s0, f, ry0, rzo - 1), P(s, s0, f, ry1, rzo - 1));
                         const f2 zp = make_float2(P(s, s0, f, ry0, rzo + 1), P(s, s0, f, ry1, rzo + 1));
-                        sx[f] = slope(xm, c[f], xp, lim);
-                        sy[f] = slope(ym, c[f], yp, lim);
-                        sz[f] = slope(zm, c[f], zp, lim);
+                        sx[f] = slp(xm, c[f], xp, lim);
+                        sy[f] = slp(ym, c[f], yp, lim);
+                        sz[f] = slp(zm, c[f], zp, lim);
                     }
                     predict(c, sx, sy, sz, hd, k, xt);
                 } else {
@@ -717,7 +726,7 @@ template <int W, int R, bool SKIP_PAD = false> struct Kernel {
     }
 };
 
-template <int W, int R>
+template <int W, int R, int LIM>
 __global__ void __launch_bounds__(32 * W, 2) fast_step_kernel(const GridArgs<float> a,
                                                                    const __grid_constant__ CUtensorMap tmap,
                                                                    int chunk) {
@@ -729,7 +738,7 @@ __global__ void __launch_bounds__(32 * W, 2) fast_step_kernel(const GridArgs<flo
     const int tz = b % tiles_z;
     b /= tiles_z;
     const int ty = b % tiles_y;
-    Kernel<W, R>::run_tile(a, &tmap, tz, ty, b / tiles_y, chunk, blockIdx.x, gridDim.x, smem_raw);
+    Kernel<W, R, false, LIM>::run_tile(a, &tmap, tz, ty, b / tiles_y, chunk, blockIdx.x, gridDim.x, smem_raw);
 }
 
 // Batched step: one persistent launch advances many independent grids by

@@ -6,10 +6,12 @@
 
 namespace dg {
 
-cudaError_t launch_fast_step(const GridArgs<float> &a, const CUtensorMap *tmap, int chunk, cudaStream_t st) {
+namespace {
+template <int LIM>
+cudaError_t launch_fast_step_t(const GridArgs<float> &a, const CUtensorMap *tmap, int chunk, cudaStream_t st) {
     constexpr int W = kFastOwnWarps, R = 4;
     using Sm = fastk::Smem<W, R>;
-    auto kern = fastk::fast_step_kernel<W, R>;
+    auto kern = fastk::fast_step_kernel<W, R, LIM>;
     const int smem = (int)sizeof(Sm) + 1024;
     static std::atomic<unsigned long long> attr_set{0};
     const cudaError_t e = ensure_dynamic_smem(kern, smem, attr_set);
@@ -17,6 +19,13 @@ cudaError_t launch_fast_step(const GridArgs<float> &a, const CUtensorMap *tmap, 
     const int blocks = step_grid_blocks(a.nx, a.ny, a.nz, kFastF32, chunk);
     kern<<<blocks, dim3(32, W), smem, st>>>(a, *tmap, chunk);
     return cudaGetLastError();
+}
+}  // namespace
+
+// One kernel per limiter: the slope code of the hot loop is fixed at compile
+// time.
+cudaError_t launch_fast_step(const GridArgs<float> &a, const CUtensorMap *tmap, int chunk, cudaStream_t st) {
+    return a.limiter == 0 ? launch_fast_step_t<0>(a, tmap, chunk, st) : launch_fast_step_t<1>(a, tmap, chunk, st);
 }
 template cudaError_t launch_reduce_policy<float, false>(const GridArgs<float> &, int, cudaStream_t);
 template cudaError_t launch_cons_to_prim_policy<float, false>(const GridArgs<float> &, const float *, float *,
