@@ -30,8 +30,14 @@ def read_header(path: os.PathLike) -> dict:
     with open(path, "rb") as f:
         if f.read(8) != MAGIC:
             raise ValueError(f"{path}: not a deep-green snapshot")
-        (hl,) = struct.unpack("<Q", f.read(8))
-        return json.loads(f.read(hl).decode())
+        raw = f.read(8)
+        if len(raw) != 8:
+            raise ValueError(f"{path}: truncated header")
+        (hl,) = struct.unpack("<Q", raw)
+        text = f.read(hl)
+        if len(text) != hl:
+            raise ValueError(f"{path}: truncated header")
+        return json.loads(text.decode())
 
 
 def read(path: os.PathLike, mmap: bool = True) -> dict:
@@ -40,8 +46,12 @@ def read(path: os.PathLike, mmap: bool = True) -> dict:
     h = read_header(path)
     dt = np.dtype(h["dtype"]).newbyteorder("<")
     shape = tuple(h["shape"])
+    size = os.path.getsize(path)
+    want = int(np.prod(shape)) * dt.itemsize
     out = {"meta": h}
     for d in h["datasets"]:
+        if d["nbytes"] != want or d["offset"] + want > size:
+            raise ValueError(f"{path}: dataset {d['name']} is truncated or does not match the header's shape")
         group, name = d["name"].split("/", 1)
         if mmap:
             a = np.memmap(path, dtype=dt, mode="r", offset=d["offset"], shape=shape)

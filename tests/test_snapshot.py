@@ -55,3 +55,17 @@ def test_host_writer_rejects_bad_input(tmp_path):
     bad.write_bytes(b"NOTASNAP" + bytes(8))
     with pytest.raises(ValueError):
         snapshot.read(bad)
+
+
+def test_reader_rejects_truncated_files(tmp_path):
+    a = {"conserved/mass": np.ones((4, 4, 4), np.float32), "conserved/energy": np.ones((4, 4, 4), np.float32)}
+    path = tmp_path / "s.dgsnap"
+    snapshot.write_host(path, a)
+    raw = path.read_bytes()
+    cut = tmp_path / "cut.dgsnap"
+    cut.write_bytes(raw[:-10])           # last dataset short
+    with pytest.raises(ValueError, match="truncated"):
+        snapshot.read(cut)
+    cut.write_bytes(raw[:20])            # header short
+    with pytest.raises(ValueError, match="truncated"):
+        snapshot.read_header(cut)
