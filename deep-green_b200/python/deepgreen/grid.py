@@ -12,7 +12,7 @@ the host arrays are synchronised on demand (reading ``grid.conserved`` or
 """
 from __future__ import annotations
 
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 from enum import IntEnum
 
 import numpy as np

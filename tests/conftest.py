@@ -3,7 +3,6 @@ import sys
 from pathlib import Path
 
 import numpy as np
-import pytest
 
 ROOT = Path(__file__).resolve().parents[1]
 for p in (ROOT / "deep-green_b200" / "python", ROOT / "oracle", ROOT / "tests"):

@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 from conftest import random_primitives
-from deepgreen import capi, learned
+from deepgreen import learned
 from deepgreen import net as dnet
 
 pytestmark = pytest.mark.gpu
