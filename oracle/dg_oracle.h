@@ -22,16 +22,19 @@
  * fills ghosts with whole-slice copies exactly as the reference does.
  *
  * Parameters that the reference hard-codes as statics (globals.rs:3-8:
- * GAMMA, CFL, G) are runtime fields here.  Two additions that the reference
- * does not have are switchable and off by default: a minmod slope limiter
- * (limiter = 1) and nothing else; gravity follows physics.rs:366-372.
+ * GAMMA, CFL, G) are runtime fields here.  One addition that the reference
+ * does not have is switchable and off by default: a minmod slope limiter
+ * (limiter = 1).  Gravity follows physics.rs:366-372.
  *
  * PARITY UNPINNED: the reference ships no tests, golden vectors or stored
  * outputs, and none of its implementations can be built or run in this
  * environment (no Rust toolchain or crates, no gfortran, no warp, and the
  * CUDA path needs HighFive/HDF5).  This oracle is cross-checked against an
- * independent NumPy restatement (oracle/numpy_twin.py) and against physics
- * invariants, not against reference outputs.
+ * independent NumPy restatement (oracle/numpy_twin.py), against physics
+ * invariants (uniform states, conservation, axis symmetry) and against the
+ * mathematics (the Sod tube converges to the exact Riemann solution, the
+ * periodic isentropic vortex returns after one period), not against
+ * reference outputs.
  *
  * Build: make -C oracle   (gcc, -O2 -fopenmp -ffp-contract=off)
  */
