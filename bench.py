@@ -13,7 +13,8 @@ Keys beside the contract's ones:
                 achieved = 40 B per cell update (read + write 5 FP32 fields)
                 x cells / mean kernel time (CUDA events on the library's
                 stream); traffic = ncu DRAM bytes per launch from the
-                committed profile summary when present.
+                committed profile of the same kernel instantiation
+                (profiles/step_traffic.json), else null.
   e2e           the same metric through the C ABI from pinned HOST buffers:
                 upload of the state, K steps reading dt back after each one
                 (as the reference's time loop does), download of the state.
@@ -22,6 +23,12 @@ Keys beside the contract's ones:
                 OpenMP over every loop, and under "rust_like" threaded only
                 where the Rust step is (its serial loops stay serial).
   clocks        nvidia-smi samples during the timed region.
+  vortex        the workload's second case, the 512^3 isentropic vortex
+                (periodic), timed the same way (GCUPS, ms per step).
+  parity        per-field relative L1 of the FP32 step against the FP64
+                oracle after 20 steps of Sod and of the vortex at 128^3, and
+                the relative difference of the last dt (computed with the
+                CPU baseline, outside every timed region).
 
 --case learned: the learned coarse-grid correction end to end -- training
 pairs made by the solver (256^3 fine / 128^3 coarse), 2000 Adam steps of the
@@ -254,15 +261,19 @@ def cpu_oracle_gcups(case, n, nz_sample, steps, warmup=1, rust_like=False):
     return cells / statistics.mean(times) / 1e9, times
 
 
-def ncu_traffic_per_launch():
-    """DRAM bytes per launch of the step kernel from the committed ncu
-    summary (profiles/step_kernel_sod512.json), or None."""
-    p = ROOT / "profiles" / "step_kernel_sod512.json"
+def ncu_traffic_per_launch(kernel, n):
+    """DRAM bytes per launch of the benchmarked step kernel, from the
+    committed ncu summary (profiles/step_traffic.json): only when that
+    capture is of the same kernel instantiation, and scaled to n^3 cells from
+    the captured grid in proportion to the cells.  None otherwise."""
+    p = ROOT / "profiles" / "step_traffic.json"
     if not p.exists():
         return None
     try:
         d = json.loads(p.read_text())
-        return float(d["dram_bytes_per_launch"])
+        if d["kernel"] != kernel:
+            return None
+        return float(d["dram_bytes_per_cell"]) * n ** 3
     except Exception:
         return None
 
@@ -297,40 +308,97 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+STEP_KERNEL = "dg::sweep::sweep_step_kernel<float, 12, 5, 1, false>"
+
+
+def timed_steps(ctx, steps, warmup, local, world, barrier):
+    """K steps of the context's kernel timed with CUDA events on its stream
+    (max over ranks), with the clock samples of the timed region."""
+    import torch
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    ctx.enqueue_steps(warmup)
+    ctx.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        start.record(stream)
+        ctx.enqueue_steps(steps)
+        end.record(stream)
+        end.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    return start.elapsed_time(end), clk.summary()
+
+
+def parity_block(n=128, steps=20):
+    """Per-field relative L1 (sum|a-b| / sum|b| over the interior) of the FP32
+    production kernel against the FP64 oracle after `steps` steps of the Sod
+    and vortex workloads at n^3 (a size the oracle runs in about a second),
+    and the relative difference of the last dt.  Part of the CPU-baseline leg:
+    the oracle is the checker here, nothing of it is timed or shipped."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle
+    from deepgreen import capi, setups
+    out = {"grid": [n, n, n], "steps": steps, "against": "FP64 oracle (C restatement of the Rust step)",
+           "tolerance": 1e-5}
+    for case in ("sod", "vortex"):
+        if case == "sod":
+            prim, ds, bcs = setups.sod(n)
+        else:
+            prim, ds, bcs = setups.isentropic_vortex(n, gamma=GAMMA)
+        o = pyoracle.Oracle((n, n, n), ds, bcs, gamma=GAMMA, cfl=CFL, limiter=1, dtype=np.float64,
+                            threads=pyoracle.ALL_PARALLEL)
+        o.set_primitives([np.asarray(a, np.float64) for a in prim])
+        odts = o.step(steps)
+        ref = o.conserved()
+        o.close()
+        ctx = capi.Context((n, n, n), ds, bcs, gamma=GAMMA, cfl=CFL, limiter=capi.LIMITER_MINMOD,
+                           precision=capi.F32)
+        ctx.set_primitives([np.asarray(a, np.float32) for a in prim])
+        gdts = ctx.compute_step(steps)
+        got = ctx.get_conserved()
+        ctx.close()
+        inner = (slice(2, -2),) * 3
+        errs = {}
+        for f, name in enumerate(("mass", "mom_x", "mom_y", "mom_z", "energy")):
+            b = np.asarray(ref[f], np.float64)[inner]
+            a = np.asarray(got[f], np.float64)[inner]
+            den = np.abs(b).sum()
+            # a field that is zero in the reference (the Sod tube's transverse
+            # momenta) is reported as the absolute L1 over the mass's scale
+            errs[name] = float(np.abs(a - b).sum() / den) if den > 0 else \
+                float(np.abs(a - b).sum() / np.abs(np.asarray(ref[0], np.float64)[inner]).sum())
+        out[case] = {"rel_l1": errs, "max": max(errs.values()),
+                     "dt_rel": float(abs(gdts[-1] - odts[-1]) / odts[-1])}
+    return out
+
+
 def run_ours(args, world, rank, local):
     import torch
     from deepgreen import capi
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     n = args.n
-    cons, ds, bcs = device_initial_state(args.case, n, dev)
-    ctx = capi.Context((n, n, n), ds, bcs, gamma=GAMMA, cfl=CFL, limiter=capi.LIMITER_MINMOD,
-                       precision=capi.F32, device=local)
-    ctx.set_conserved_device([c.data_ptr() for c in cons])
-    torch.cuda.synchronize()
-    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
-    blocks, threads, chunk = ctx.launch_shape()
-
-    # warm-up
-    ctx.enqueue_steps(args.warmup)
-    ctx.synchronize()
 
     def barrier():
         if world > 1:
             import torch.distributed as dist
             dist.barrier()
 
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        start.record(stream)
-        ctx.enqueue_steps(args.steps)
-        end.record(stream)
-        end.synchronize()
-    torch.cuda.synchronize()
-    barrier()
-    ms = start.elapsed_time(end)
+    def make(case):
+        cons, ds, bcs = device_initial_state(case, n, dev)
+        c = capi.Context((n, n, n), ds, bcs, gamma=GAMMA, cfl=CFL, limiter=capi.LIMITER_MINMOD,
+                         precision=capi.F32, device=local)
+        c.set_conserved_device([x.data_ptr() for x in cons])
+        torch.cuda.synchronize()
+        return c, cons
+
+    ctx, cons = make(args.case)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    blocks, threads, chunk = ctx.launch_shape()
+    ms, clocks = timed_steps(ctx, args.steps, args.warmup, local, world, barrier)
     dts = ctx.get_dts(args.steps)
     status = ctx.status()
     cells = n ** 3
@@ -366,13 +434,28 @@ def run_ours(args, world, rank, local):
                "h2d_bytes_per_step": state_bytes / args.steps,
                "d2h_bytes_per_step": state_bytes / args.steps + 8,
                "ms_total": e2e_ms, "path": "dg_set_conserved + K x dg_compute_step(1) + dg_get_conserved"}
+        del host_in, host_out
+    del cons
+    ctx.close()
+
+    # the workload's second case: the 512^3 isentropic vortex (periodic)
+    other = None
+    if args.case == "sod":
+        vctx, vcons = make("vortex")
+        del vcons
+        vms, vclk = timed_steps(vctx, args.steps, args.warmup, local, world, barrier)
+        vvalue, vms = job_rate(vms, cells, args.steps, world, device=dev)
+        vctx.close()
+        other = {"workload": workload_name("vortex", n), "value": vvalue, "unit": UNIT,
+                 "ms_per_step": vms / args.steps, "clocks": vclk}
 
     if rank != 0:
         return
     peak, peak_kind = peaks()
     achieved = BYTES_PER_CELL["f32"] * cells / (ms_step * 1e-3) / 1e9
-    traffic = ncu_traffic_per_launch()
+    traffic = ncu_traffic_per_launch(STEP_KERNEL, n)
     cpu = None
+    parity = None
     if not args.no_cpu and world == 1:
         nz_sample = 64
         g, times = cpu_oracle_gcups(args.case, n, nz_sample, 5, warmup=1)
@@ -385,6 +468,7 @@ def run_ours(args, world, rank, local):
         cpu["rust_like"] = {"value": g_rust, "unit": UNIT,
                             "sample": f"2 steps of a {n}x{n}x16 slab; threads only where the Rust step "
                                       f"uses par_for_each (calc_primitives, calc_timestep, calc_gradients)"}
+        parity = parity_block()
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
@@ -392,17 +476,22 @@ def run_ours(args, world, rank, local):
         "config": {"workload": workload_name(args.case, n), "grid": [n, n, n], "ghosts": 2,
                    "parallelism": f"replicas x{world}" if world > 1 else "single grid",
                    "l2": "state (2.9 GB read + 2.9 GB written per step) is larger than L2",
+                   "kernel": STEP_KERNEL,
                    "launch": {"blocks": blocks, "threads": threads, "x_planes_per_block": chunk}},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": BYTES_PER_CELL["f32"] * cells},
         "cpu_baseline": cpu,
         "e2e": e2e,
-        "clocks": clk.summary(),
+        "clocks": clocks,
         "gpu_launches": args.steps,
         "dt_first_last": [float(dts[0]), float(dts[-1])],
         "status_flags": status,
     }
+    if other:
+        line["vortex"] = other
+    if parity:
+        line["parity"] = parity
     print(json.dumps(line), flush=True)
 
 

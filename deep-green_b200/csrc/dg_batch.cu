@@ -17,15 +17,21 @@
 #include <vector>
 
 #include "../../include/deepgreen.h"
-#include "dg_fast_impl.cuh"
+#include "dg_host.h"
 #include "dg_kernels.cuh"
+#include "dg_sweep_impl.cuh"
 
 using namespace dg;
-using fastk::BatchItem;
+using sweep::BatchItem;
 
 namespace {
 
-constexpr int kRing = 4;
+constexpr int kTY = kSweepRowsF32;   // tile rows of the batched sweep
+constexpr int kRing = 5;
+constexpr int kTZs = sweep::kTileZ;  // tile columns
+constexpr int kCombos = 4;           // (limiter, gravity) pairs; one launch each
+
+int combo_of(const dg_sim_info &f) { return (f.limiter ? 1 : 0) + (f.gravity ? 2 : 0); }
 
 struct GridSlot {
     dg_sim_info info;
@@ -51,8 +57,9 @@ struct dg_batch {
     BatchItem *d_items = nullptr;
     size_t items_cap = 0;
     int nitems = 0;
-    unsigned *d_queue = nullptr;
-    int tile_rows = 16;              // 16 (8 warps) or 8 (4 warps)
+    int combo_off[kCombos + 1] = {0, 0, 0, 0, 0};   // items of each (limiter, gravity) pair
+    unsigned *d_queue = nullptr;     // one counter per pair
+    int tile_rows = kTY;
     int chunk = 0;                   // x-planes per work item (0 = automatic)
     int chunk_used = 0;
     unsigned long long steps = 0;    // steps since the states were set
@@ -131,32 +138,36 @@ int rebuild(dg_batch *b) {
     long long tiles_total = 0;
     int min_nx = 1 << 30;
     for (auto &s : b->g) {
-        tiles_total += (long long)((s.ny - 4 + ty - 1) / ty) * ((s.nz - 4 + kTZ - 1) / kTZ);
+        tiles_total += (long long)((s.ny - 4 + ty - 1) / ty) * ((s.nz - 4 + kTZs - 1) / kTZs);
         min_nx = std::min(min_nx, s.nx - 4);
     }
     int chunk = b->chunk;
     if (chunk <= 0) {
         long long cells = 0;
         for (auto &s : b->g) cells += (long long)(s.nx - 4) * (s.ny - 4) * (s.nz - 4);
-        // ~14 waves of 2 CTAs per SM worth of items, at least 16 planes
-        const long long items_target = 2LL * kSms * 14;
-        const long long tile_cells = (long long)ty * kTZ;
+        // ~8 waves of one block per SM worth of items, at least 16 planes
+        const long long items_target = (long long)kSms * 8;
+        const long long tile_cells = (long long)ty * kTZs;
         long long c = cells / std::max<long long>(1, items_target * tile_cells);
         chunk = (int)std::max<long long>(16, c);
     }
     b->chunk_used = chunk;
-    // items: largest grids first, each grid's items contiguous
+    // items: grouped by (limiter, gravity), largest grids first, each grid's
+    // items contiguous
     std::vector<int> order(b->n);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        const int cx = combo_of(b->g[x].info), cy = combo_of(b->g[y].info);
+        if (cx != cy) return cx < cy;
         auto sz = [&](int i) { return (long long)b->g[i].nx * b->g[i].ny * b->g[i].nz; };
         return sz(x) > sz(y);
     });
     std::vector<BatchItem> items;
     int off = 0;
+    for (int c = 0; c <= kCombos; ++c) b->combo_off[c] = 0;
     for (int i : order) {
         GridSlot &s = b->g[i];
-        const int tz_n = (s.nz - 4 + kTZ - 1) / kTZ, ty_n = (s.ny - 4 + ty - 1) / ty;
+        const int tz_n = (s.nz - 4 + kTZs - 1) / kTZs, ty_n = (s.ny - 4 + ty - 1) / ty;
         const int cx_n = (s.nx - 4 + chunk - 1) / chunk;
         s.item_off = off;
         s.nitems = tz_n * ty_n * cx_n;
@@ -165,7 +176,9 @@ int rebuild(dg_batch *b) {
             for (int yy = 0; yy < ty_n; ++yy)
                 for (int zz = 0; zz < tz_n; ++zz) items.push_back(BatchItem{i, local++, zz, yy, cx});
         off += s.nitems;
+        b->combo_off[combo_of(s.info) + 1] = off;
     }
+    for (int c = 1; c <= kCombos; ++c) b->combo_off[c] = std::max(b->combo_off[c], b->combo_off[c - 1]);
     b->nitems = (int)items.size();
     if ((size_t)b->nitems > b->items_cap) {
         if (b->d_items) cudaFree(b->d_items);
@@ -188,7 +201,7 @@ int rebuild(dg_batch *b) {
             cuuint64_t dims[4] = {(cuuint64_t)s.nz, (cuuint64_t)s.ny, (cuuint64_t)s.nx, 5};
             cuuint64_t strides[3] = {(cuuint64_t)s.pitch * 4, (cuuint64_t)s.pitch * s.ny * 4,
                                      (cuuint64_t)s.fstride * 4};
-            cuuint32_t box[4] = {(cuuint32_t)kRZ, (cuuint32_t)(ty + 4), 1, 5};
+            cuuint32_t box[4] = {(cuuint32_t)(kTZs + 4), (cuuint32_t)(ty + 4), 1, 5};
             cuuint32_t estr[4] = {1, 1, 1, 1};
             if (fn(&maps[i], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, s.buf[p], dims, strides, box, estr,
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -209,24 +222,33 @@ int rebuild(dg_batch *b) {
     return DG_OK;
 }
 
-template <int W> size_t smem_bytes() { return sizeof(fastk::Smem<W, kRing>) + 1024; }
+constexpr int kSmem = sweep::smem_bytes<float, kTY, kRing>();
 
-template <int W> cudaError_t prepare_kernel() {
-    return cudaFuncSetAttribute(fastk::batch_step_kernel<W, kRing>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem_bytes<W>());
+template <int LIM, bool GRAV> cudaError_t prepare_kernel() {
+    static std::atomic<unsigned long long> done{0};
+    return ensure_dynamic_smem(sweep::sweep_batch_kernel<kTY, kRing, LIM, GRAV>, kSmem, done);
 }
 
-// one step of every grid (no synchronisation)
+template <int LIM, bool GRAV> void launch_combo(dg_batch *b, int parity, int c) {
+    const int n = b->combo_off[c + 1] - b->combo_off[c];
+    sweep::sweep_batch_kernel<kTY, kRing, LIM, GRAV><<<std::min(n, kSms), 32 * (kTY + 2), kSmem, b->stream>>>(
+        b->d_args[parity], b->d_maps[parity], b->d_items + b->combo_off[c], n, b->d_queue + c, b->chunk_used);
+}
+
+// one step of every grid (no synchronisation): one persistent launch per
+// (limiter, gravity) pair present in the batch
 int launch_one(dg_batch *b, int parity) {
-    B_CUDA(b, cudaMemsetAsync(b->d_queue, 0, sizeof(unsigned), b->stream));
-    if (b->tile_rows == 16) {
-        fastk::batch_step_kernel<8, kRing><<<std::min(b->nitems, kSms * 2), dim3(32, 8), smem_bytes<8>(), b->stream>>>(
-            b->d_args[parity], b->d_maps[parity], b->d_items, b->nitems, b->d_queue, b->chunk_used);
-    } else {
-        fastk::batch_step_kernel<4, kRing><<<std::min(b->nitems, kSms * 4), dim3(32, 4), smem_bytes<4>(), b->stream>>>(
-            b->d_args[parity], b->d_maps[parity], b->d_items, b->nitems, b->d_queue, b->chunk_used);
+    B_CUDA(b, cudaMemsetAsync(b->d_queue, 0, kCombos * sizeof(unsigned), b->stream));
+    for (int c = 0; c < kCombos; ++c) {
+        if (b->combo_off[c + 1] == b->combo_off[c]) continue;
+        switch (c) {
+            case 0: launch_combo<0, false>(b, parity, c); break;
+            case 1: launch_combo<1, false>(b, parity, c); break;
+            case 2: launch_combo<0, true>(b, parity, c); break;
+            default: launch_combo<1, true>(b, parity, c); break;
+        }
+        B_CUDA(b, cudaGetLastError());
     }
-    B_CUDA(b, cudaGetLastError());
     return DG_OK;
 }
 
@@ -328,11 +350,13 @@ int32_t dg_batch_create(int32_t n, const dg_sim_info *infos, dg_batch **out) {
         e = cudaMalloc(&b->d_args[p], n * sizeof(GridArgs<float>));
         if (e == cudaSuccess) e = cudaMalloc(&b->d_maps[p], n * sizeof(CUtensorMap));
     }
-    if (e == cudaSuccess) e = cudaMalloc(&b->d_queue, sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_queue, kCombos * sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMemsetAsync(b->arena, 0, total, b->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(b->ctl, 0, n * sizeof(DevCtl), b->stream);
-    if (e == cudaSuccess) e = prepare_kernel<8>();
-    if (e == cudaSuccess) e = prepare_kernel<4>();
+    if (e == cudaSuccess) e = prepare_kernel<0, false>();
+    if (e == cudaSuccess) e = prepare_kernel<1, false>();
+    if (e == cudaSuccess) e = prepare_kernel<0, true>();
+    if (e == cudaSuccess) e = prepare_kernel<1, true>();
     if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
     if (e != cudaSuccess) { b->err = std::string("batch set-up: ") + cudaGetErrorString(e); return bail(DG_ERR_CUDA); }
     char *p = static_cast<char *>(b->arena);
@@ -437,9 +461,10 @@ int32_t dg_batch_get_conserved(dg_batch *b, int32_t i, void *const cons[5]) {
     return DG_OK;
 }
 
-// Tile rows (16 or 8) and x-planes per work item (0 = automatic).
+// Tile rows (12: the sweep kernel's tile) and x-planes per work item
+// (0 = automatic).
 int32_t dg_batch_set_tiling(dg_batch *b, int32_t tile_rows, int32_t chunk) {
-    if (!b || (tile_rows != 16 && tile_rows != 8) || chunk < 0) return bfail(b, DG_ERR_INVALID, "bad tiling");
+    if (!b || tile_rows != kTY || chunk < 0) return bfail(b, DG_ERR_INVALID, "bad tiling (tile rows must be 12)");
     b->tile_rows = tile_rows;
     b->chunk = chunk;
     b->dirty = true;
@@ -477,8 +502,8 @@ int32_t dg_batch_autotune(dg_batch *b, int32_t steps, int32_t *tile_rows, int32_
     B_CUDA(b, cudaMemcpyAsync(save, b->arena, total, cudaMemcpyDeviceToDevice, b->stream));
     B_CUDA(b, cudaMemcpyAsync(save_ctl, b->ctl, b->n * sizeof(DevCtl), cudaMemcpyDeviceToDevice, b->stream));
     const unsigned long long steps0 = b->steps;
-    const int rows_cand[2] = {16, 8};
-    const int chunk_cand[4] = {16, 32, 64, 128};
+    const int rows_cand[1] = {kTY};
+    const int chunk_cand[5] = {16, 24, 32, 64, 128};
     double best = 1e30;
     int best_rows = b->tile_rows, best_chunk = b->chunk;
     cudaEvent_t e0, e1;

@@ -48,7 +48,7 @@ int encode_map(dg_ctx *c, int i) {
     cuuint64_t dims[4] = {(cuuint64_t)c->nz, (cuuint64_t)c->ny, (cuuint64_t)c->nx, 5};
     cuuint64_t strides[3] = {(cuuint64_t)c->pitch * c->elem, (cuuint64_t)c->pitch * c->ny * c->elem,
                              (cuuint64_t)c->fstride * c->elem};
-    cuuint32_t box[4] = {(cuuint32_t)kRZ, (cuuint32_t)(ty + 4), 1, 5};
+    cuuint32_t box[4] = {(cuuint32_t)step_box_cols(c->kind), (cuuint32_t)(ty + 4), 1, 5};
     cuuint32_t estr[4] = {1, 1, 1, 1};
     CUresult r = fn(&c->tmap[i], c->elem == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
                     4, c->buf[i], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -172,11 +172,13 @@ int enqueue(dg_ctx *c, int nsteps) {
         cudaError_t e;
         if (c->elem == 8) {
             auto a = grid_args<double>(c, c->buf[src], c->buf[dst]);
-            e = launch_step_policy<double, true>(a, &c->tmap[src], c->info.limiter, chunk, c->stream);
+            e = c->kind == kFastF64 ? launch_sweep(a, &c->tmap[src], chunk, c->stream)
+                                    : launch_step_policy<double, true>(a, &c->tmap[src], c->info.limiter, chunk,
+                                                                       c->stream);
         } else {
             auto a = grid_args<float>(c, c->buf[src], c->buf[dst]);
             e = c->exact ? launch_step_policy<float, true>(a, &c->tmap[src], c->info.limiter, chunk, c->stream)
-                         : launch_fast_step(a, &c->tmap[src], chunk, c->stream);
+                         : launch_sweep(a, &c->tmap[src], chunk, c->stream);
         }
         if (e != cudaSuccess) return cuda_fail(c, e, "step kernel launch");
         c->cur = dst;
@@ -236,7 +238,8 @@ int32_t dg_create(const dg_sim_info *info, dg_ctx **out) {
     if (!(info->ds > 0) || !(info->gamma > 1) || !(info->cfl > 0)) { set_err("ds > 0, gamma > 1, cfl > 0 required"); return DG_ERR_INVALID; }
     if (info->precision != DG_F32 && info->precision != DG_F64) { set_err("precision must be DG_F32 or DG_F64"); return DG_ERR_INVALID; }
     if (info->limiter != DG_LIMITER_NONE && info->limiter != DG_LIMITER_MINMOD) { set_err("unknown limiter"); return DG_ERR_INVALID; }
-    if (info->rounding != DG_ROUNDING_DEFAULT && info->rounding != DG_ROUNDING_REFERENCE) { set_err("unknown rounding policy"); return DG_ERR_INVALID; }
+    if (info->rounding != DG_ROUNDING_DEFAULT && info->rounding != DG_ROUNDING_REFERENCE &&
+        info->rounding != DG_ROUNDING_FAST) { set_err("unknown rounding policy"); return DG_ERR_INVALID; }
     for (int a = 0; a < 3; ++a) {
         const int lo = info->bcs[2 * a], hi = info->bcs[2 * a + 1];
         if (lo < 0 || lo > 2 || hi < 0 || hi > 2) { set_err("unknown boundary type"); return DG_ERR_INVALID; }
@@ -257,12 +260,21 @@ int32_t dg_create(const dg_sim_info *info, dg_ctx **out) {
     if (!c) { set_err("out of host memory"); return DG_ERR_INVALID; }
     c->info = *info;
     c->elem = info->precision == DG_F64 ? 8 : 4;
-    c->exact = c->elem == 8 || info->rounding == DG_ROUNDING_REFERENCE;
-    c->kind = c->elem == 8 ? kRefF64 : (c->exact ? kRefF32 : kFastF32);
+    c->exact = info->rounding == DG_ROUNDING_REFERENCE || (c->elem == 8 && info->rounding == DG_ROUNDING_DEFAULT);
+    c->kind = c->elem == 8 ? (c->exact ? kRefF64 : kFastF64) : (c->exact ? kRefF32 : kFastF32);
     c->nx = info->nx + 4;
     c->ny = info->ny + 4;
     c->nz = info->nz + 4;
     c->pitch = (c->nz + 31) / 32 * 32;
+    // Test hook: a context created while DG_DEBUG_WAIT_BUDGET is set gives
+    // its step kernels' waits for staged planes that many SM clocks (0 or
+    // less: give up at the first unfinished wait) instead of ~2 s, so that a
+    // test can make a wait run out and check that the step reports
+    // DG_ERR_TIMEOUT and the device stays usable.
+    if (const char *wb = std::getenv("DG_DEBUG_WAIT_BUDGET")) {
+        const long long v = std::atoll(wb);
+        c->wait_budget = v > 0 ? v : -1;
+    }
     c->fstride = (long long)c->nx * c->ny * c->pitch;
     c->state_bytes = (size_t)5 * c->fstride * c->elem;
     auto bail = [&](int code) {
@@ -275,8 +287,8 @@ int32_t dg_create(const dg_sim_info *info, dg_ctx **out) {
     for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaMalloc(&c->buf[i], c->state_bytes);
     if (e == cudaSuccess) e = cudaMalloc(&c->ctl, sizeof(DevCtl));
     if (e == cudaSuccess) {
-        const int ty = step_tile_rows(c->kind);
-        long long tiles = (long long)((c->ny - 4 + ty - 1) / ty) * ((c->nz - 4 + kTZ - 1) / kTZ);
+        const int ty = step_tile_rows(c->kind), tzc = step_tile_cols(c->kind);
+        long long tiles = (long long)((c->ny - 4 + ty - 1) / ty) * ((c->nz - 4 + tzc - 1) / tzc);
         long long cap = tiles * (c->nx - 4);   // chunk >= 1
         if (cap < kReduceBlocks) cap = kReduceBlocks;
         c->part_cap = (int)cap;

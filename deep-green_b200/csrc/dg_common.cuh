@@ -66,6 +66,13 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, i
 
 constexpr long long kWaitBudget = 4000000000LL;  // ~2 s of SM clock
 
+// The budget a step kernel gives its waits for staged planes: the grid's own
+// (a context created with DG_DEBUG_WAIT_BUDGET set) or the default.  Waits
+// that let copies in flight land before a block exits keep kWaitBudget.
+template <class A> __device__ __forceinline__ long long wait_budget_of(const A &a) {
+    return a.wait_budget > 0 ? a.wait_budget : (a.wait_budget < 0 ? 0 : kWaitBudget);
+}
+
 // ---------------------------------------------------------------------------
 // Ghost images: the set of cells (interior cell itself plus ghosts) that
 // hold a copy of interior coordinate c along one axis of extent n

@@ -26,6 +26,7 @@ struct dg_ctx {
     int chunk;                 // 0 = automatic
     bool exact;                // reference-rounding policy
     int kind;                  // KernelKind of the step kernel
+    long long wait_budget;     // 0: default; from DG_DEBUG_WAIT_BUDGET (tests of the timeout path)
     std::string err;
 };
 
@@ -58,6 +59,8 @@ template <class T> inline GridArgs<T> grid_args(const dg_ctx *c, const void *src
     for (int i = 0; i < 6; ++i) a.bc[i] = c->info.bcs[i];
     a.gravity = c->info.gravity;
     a.limiter = c->info.limiter;
+    a.nparts = 0;
+    a.wait_budget = c->wait_budget;
     const T ds = (T)c->info.ds;
     a.k.ds = ds;
     a.k.vol = ds * ds * ds;

@@ -51,6 +51,7 @@ template <class T> struct GridArgs {
     int gravity;
     int limiter;               // 0 central slopes, 1 minmod
     int nparts;                // work items of this grid in a batched launch
+    long long wait_budget;     // SM clocks a wait for a staged plane may take (kWaitBudget)
     Consts<T> k;
     DevCtl *ctl;
     Partial *part;
@@ -60,36 +61,62 @@ template <class T> struct GridArgs {
 constexpr int kSms = 148;
 constexpr int kReduceBlocks = kSms * 8;   // grid of the state-reduction kernel
 
-// The three step kernels: reference rounding in double and in float
-// (dg_step_impl.cuh) and the fast float kernel (dg_fast_impl.cuh).
-enum KernelKind : int { kRefF64 = 0, kRefF32 = 1, kFastF32 = 2 };
+// The step kernels: reference rounding in double and in float
+// (dg_step_impl.cuh) and the fused-arithmetic sweep in float and in double
+// (dg_sweep_impl.cuh).
+enum KernelKind : int { kRefF64 = 0, kRefF32 = 1, kFastF32 = 2, kFastF64 = 3 };
 
-// Warps of the fast kernel; each owns 2 rows of the tile.
-constexpr int kFastOwnWarps = 8;
+inline bool is_sweep(int kind) { return kind == kFastF32 || kind == kFastF64; }
 
-// Tile rows (y) of each kernel; every tile is 32 cells wide in z.
+// Owned tile rows (y) of each kernel.  A sweep block also runs two halo warps.
+constexpr int kSweepRowsF32 = 12;
+constexpr int kSweepRowsF64 = 4;
 inline int step_tile_rows(int kind) {
-    return kind == kRefF64 ? 4 : (kind == kRefF32 ? 8 : 2 * kFastOwnWarps);
+    switch (kind) {
+        case kRefF64: return 4;
+        case kRefF32: return 8;
+        case kFastF32: return kSweepRowsF32;
+        default: return kSweepRowsF64;
+    }
 }
-inline int step_threads(int kind) { return kind == kFastF32 ? 32 * kFastOwnWarps : 32 * step_tile_rows(kind); }
+// Tile columns (z) and the staged box width (2-cell halo each side).
+inline int step_tile_cols(int kind) { return is_sweep(kind) ? 64 : kTZ; }
+inline int step_box_cols(int kind) { return step_tile_cols(kind) + 4; }
+inline int step_threads(int kind) {
+    return is_sweep(kind) ? 32 * (step_tile_rows(kind) + 2) : 32 * step_tile_rows(kind);
+}
 
 // Blocks of one step launch: (y tiles) x (z tiles) x (x chunks of `chunk`
 // planes).
 inline int step_grid_blocks(int nx, int ny, int nz, int kind, int chunk) {
-    const int ty = step_tile_rows(kind);
-    const int tiles_z = (nz - 4 + kTZ - 1) / kTZ;
+    const int ty = step_tile_rows(kind), tzc = step_tile_cols(kind);
+    const int tiles_z = (nz - 4 + tzc - 1) / tzc;
     const int tiles_y = (ny - 4 + ty - 1) / ty;
     const int chunks = (nx - 4 + chunk - 1) / chunk;
     return tiles_z * tiles_y * chunks;
 }
-// Default x-planes per block: enough blocks for ~14 waves of resident CTAs
-// (2 per SM), at least 20 planes per block (each block re-stages
-// 4 planes at its ends).  Measured: flat within 1 % from 43 to 74 planes on
-// 512^3; best at 22 planes on 256^3 (5 % faster than 32).
+// Default x-planes per block.  Reference-rounding kernels: enough blocks for
+// ~14 waves of resident CTAs (2 per SM), at least 20 planes per block (each
+// block re-stages 4 planes at its ends); measured flat within 1 % from 43
+// to 74 planes on 512^3.  Sweep kernels (one block per SM): the split of x
+// into chunks that minimises waves x (planes per block + 3 re-staged),
+// with at least 24 planes per block.
 inline int choose_chunk(int nx, int ny, int nz, int kind) {
-    const int ty = step_tile_rows(kind);
-    const long long tiles = (long long)((ny - 4 + ty - 1) / ty) * ((nz - 4 + kTZ - 1) / kTZ);
+    const int ty = step_tile_rows(kind), tzc = step_tile_cols(kind);
+    const long long tiles = (long long)((ny - 4 + ty - 1) / ty) * ((nz - 4 + tzc - 1) / tzc);
     const int nxi = nx - 4;
+    if (is_sweep(kind)) {
+        const int maxc = nxi / 24 > 0 ? nxi / 24 : 1;
+        long long best = -1;
+        int bestc = 1;
+        for (int c = 1; c <= maxc && c <= 64; ++c) {
+            const long long per = (nxi + c - 1) / c;
+            const long long waves = (tiles * c + kSms - 1) / kSms;
+            const long long cost = waves * (per + 3);
+            if (best < 0 || cost < best) { best = cost; bestc = c; }
+        }
+        return (nxi + bestc - 1) / bestc;
+    }
     const long long target = 2LL * kSms * 14;
     long long chunks = (target + tiles - 1) / tiles;
     const long long maxc = nxi / 20 > 0 ? nxi / 20 : 1;
@@ -115,7 +142,10 @@ cudaError_t launch_cons_to_prim_policy(const GridArgs<T> &a, const T *cons, T *p
 // Message returned by dg_last_error(NULL) (errors not tied to a context).
 void set_global_error(const std::string &msg);
 
-cudaError_t launch_fast_step(const GridArgs<float> &a, const CUtensorMap *tmap_src, int chunk, cudaStream_t st);
+// The sweep kernel (kFastF32 / kFastF64 contexts); the tensor map's box is
+// step_box_cols x (step_tile_rows + 4) x 1 x 5.
+cudaError_t launch_sweep(const GridArgs<float> &a, const CUtensorMap *tmap_src, int chunk, cudaStream_t st);
+cudaError_t launch_sweep(const GridArgs<double> &a, const CUtensorMap *tmap_src, int chunk, cudaStream_t st);
 template <class T> cudaError_t launch_fill_ghosts(const GridArgs<T> &a, T *buf, cudaStream_t st);
 template <class T>
 cudaError_t launch_prim_to_cons(const GridArgs<T> &a, const T *prim, long long prim_fstride, int prim_pitch, T *cons,

@@ -93,6 +93,8 @@ GridArgs<T> args_for(const dg_sim_info *info, const void *src, void *dst, void *
     for (int i = 0; i < 6; ++i) a.bc[i] = info->bcs[i];
     a.gravity = info->gravity;
     a.limiter = info->limiter;
+    a.nparts = 0;
+    a.wait_budget = 0;
     const T ds = (T)info->ds;
     a.k.ds = ds;
     a.k.vol = ds * ds * ds;
@@ -128,7 +130,7 @@ int run(const dg_sim_info *info, int kind, void *cons_in, void *cons_out, double
     cuuint64_t dims[4] = {(cuuint64_t)a.nz, (cuuint64_t)a.ny, (cuuint64_t)a.nx, 5};
     cuuint64_t strides[3] = {(cuuint64_t)a.pitch * elem, (cuuint64_t)a.pitch * a.ny * elem,
                              (cuuint64_t)a.fstride * elem};
-    cuuint32_t box[4] = {(cuuint32_t)kRZ, (cuuint32_t)(ty + 4), 1, 5};
+    cuuint32_t box[4] = {(cuuint32_t)step_box_cols(kind), (cuuint32_t)(ty + 4), 1, 5};
     cuuint32_t estr[4] = {1, 1, 1, 1};
     if (fn(&map, elem == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, cons_in, dims,
            strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -141,14 +143,16 @@ int run(const dg_sim_info *info, int kind, void *cons_in, void *cons_out, double
     if constexpr (sizeof(T) == 4) {
         if (kind == kFastF32) {
             if (e == cudaSuccess) e = launch_reduce_policy<float, false>(a, 1, st);
-            if (e == cudaSuccess) e = launch_fast_step(a, &map, chunk, st);
+            if (e == cudaSuccess) e = launch_sweep(a, &map, chunk, st);
         } else {
             if (e == cudaSuccess) e = launch_reduce_policy<float, true>(a, 1, st);
             if (e == cudaSuccess) e = launch_step_policy<float, true>(a, &map, info->limiter, chunk, st);
         }
     } else {
         if (e == cudaSuccess) e = launch_reduce_policy<double, true>(a, 1, st);
-        if (e == cudaSuccess) e = launch_step_policy<double, true>(a, &map, info->limiter, chunk, st);
+        if (e == cudaSuccess)
+            e = kind == kFastF64 ? launch_sweep(a, &map, chunk, st)
+                                 : launch_step_policy<double, true>(a, &map, info->limiter, chunk, st);
     }
     if (e != cudaSuccess) return fail(DG_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
     if (dt_used) {
@@ -169,6 +173,15 @@ int run(const dg_sim_info *info, int kind, void *cons_in, void *cons_out, double
 }  // namespace
 }  // namespace dg
 
+// Restores the calling thread's current device on every return path: the
+// callers of this entry point manage their own devices.
+struct DeviceGuard {
+    int prev = -1;
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
 extern "C" int32_t dg_compute_step_noalloc(const dg_sim_info *info, void *cons_in, void *cons_out,
                                            double *dt_used, void *stream) {
     using namespace dg;
@@ -179,7 +192,8 @@ extern "C" int32_t dg_compute_step_noalloc(const dg_sim_info *info, void *cons_i
         return fail(DG_ERR_INVALID, "ds > 0, gamma > 1, cfl > 0 required");
     if (info->precision != DG_F32 && info->precision != DG_F64) return fail(DG_ERR_INVALID, "bad precision");
     if (info->limiter != DG_LIMITER_NONE && info->limiter != DG_LIMITER_MINMOD) return fail(DG_ERR_INVALID, "bad limiter");
-    if (info->rounding != DG_ROUNDING_DEFAULT && info->rounding != DG_ROUNDING_REFERENCE)
+    if (info->rounding != DG_ROUNDING_DEFAULT && info->rounding != DG_ROUNDING_REFERENCE &&
+        info->rounding != DG_ROUNDING_FAST)
         return fail(DG_ERR_INVALID, "bad rounding policy");
     for (int ax = 0; ax < 3; ++ax) {
         const int lo = info->bcs[2 * ax], hi = info->bcs[2 * ax + 1];
@@ -194,14 +208,43 @@ extern "C" int32_t dg_compute_step_noalloc(const dg_sim_info *info, void *cons_i
     if (cons_in == cons_out) return fail(DG_ERR_INVALID, "input and output states must differ");
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return fail(DG_ERR_NO_DEVICE, "no current CUDA device");
-    if (dev != info->device && cudaSetDevice(info->device) != cudaSuccess)
-        return fail(DG_ERR_NO_DEVICE, "cannot select the requested device");
+    DeviceGuard guard;
+    if (dev != info->device) {
+        if (cudaSetDevice(info->device) != cudaSuccess) return fail(DG_ERR_NO_DEVICE, "cannot select the requested device");
+        guard.prev = dev;
+    }
     void *scratch = nullptr;
     int r = scratch_address(info->device, &scratch);
     if (r != DG_OK) return r;
-    const int kind = elem == 8 ? kRefF64 : (info->rounding == DG_ROUNDING_REFERENCE ? kRefF32 : kFastF32);
+    const bool exact = info->rounding == DG_ROUNDING_REFERENCE || (elem == 8 && info->rounding == DG_ROUNDING_DEFAULT);
+    const int kind = elem == 8 ? (exact ? kRefF64 : kFastF64) : (exact ? kRefF32 : kFastF32);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     return elem == 8 ? run<double>(info, kind, cons_in, cons_out, dt_used, st, scratch)
                      : run<float>(info, kind, cons_in, cons_out, dt_used, st, scratch);
 }
 
+// Status flags left in the shared scratch by the last no-allocation step on
+// `device` (the flags word of its control block; the next call clears it).
+extern "C" int32_t dg_noalloc_status(int32_t device, uint32_t *flags) {
+    using namespace dg;
+    if (!flags) return fail(DG_ERR_INVALID, "null argument");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+        return fail(DG_ERR_NO_DEVICE, "no CUDA device with that ordinal");
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return fail(DG_ERR_NO_DEVICE, "no current CUDA device");
+    DeviceGuard guard;
+    if (dev != device) {
+        if (cudaSetDevice(device) != cudaSuccess) return fail(DG_ERR_NO_DEVICE, "cannot select the requested device");
+        guard.prev = dev;
+    }
+    void *scratch = nullptr;
+    int r = scratch_address(device, &scratch);
+    if (r != DG_OK) return r;
+    unsigned f = 0;
+    const cudaError_t e = cudaMemcpy(&f, static_cast<unsigned char *>(scratch) + offsetof(DevCtl, flags), sizeof(f),
+                                     cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return fail(DG_ERR_CUDA, std::string("read-back: ") + cudaGetErrorString(e));
+    *flags = f;
+    return DG_OK;
+}

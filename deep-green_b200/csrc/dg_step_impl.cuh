@@ -181,17 +181,20 @@ struct StepKernel {
         const int gyo = y0 + ly, gzo = z0 + lz;            // own cell (ghosted coordinates)
         const bool own_valid = gyo <= a.ny - 3 && gzo <= a.nz - 3;
 
-        // a previous launch timed out: the state is invalid, do nothing
-        if (*(volatile unsigned *)&a.ctl->flags & kStatusTimeout) return;
         const unsigned step = (unsigned)a.ctl->step;
         const T dt = (T)a.ctl->dt[step & 1];
 
+        // a previous launch timed out: the state is invalid, do nothing (the
+        // flag is read once, so that every thread takes the same branch)
         if (tid == 0) {
-            s.abort_flag = 0;
-            for (int i = 0; i < R; ++i) mbar_init(&s.bar[i], 1);
-            fence_mbar_init();
+            s.abort_flag = (*(volatile unsigned *)&a.ctl->flags & kStatusTimeout) ? 2 : 0;
+            if (!s.abort_flag) {
+                for (int i = 0; i < R; ++i) mbar_init(&s.bar[i], 1);
+                fence_mbar_init();
+            }
         }
         __syncthreads();
+        if (s.abort_flag) return;
         if (tid == 0) {
             for (int l = 0; l < R && l < np; ++l) {
                 mbar_expect_tx(&s.bar[l], S::kBoxBytes);
@@ -219,7 +222,7 @@ struct StepKernel {
         // the own cell's conserved values go to `keep`.
         auto convert = [&](int l, T keep[5]) -> bool {
             const int slot = l % R;
-            if (!mbar_wait(&s.bar[slot], (l / R) & 1, kWaitBudget)) return false;
+            if (!mbar_wait(&s.bar[slot], (l / R) & 1, wait_budget_of(a))) return false;
             {
                 const int ry = ly + 2, rz = lz + 2;
                 T u[5], w[5];

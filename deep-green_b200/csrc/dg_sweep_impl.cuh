@@ -1,0 +1,928 @@
+// dg_sweep_impl.cuh -- the production step kernel: one launch per
+// compute_step (deep-green src/rs/src/physics.rs:595-681) with fused
+// arithmetic (the "fast" policy), in FP32 on packed pairs or in FP64.
+//
+// Decomposition.  A block owns a tile of TY rows (y) x 64 columns (z) of
+// cells and marches along x through a chunk of planes.  Each plane arrives by
+// one 4-D TMA copy (68 columns x (TY + 4) rows x 5 fields: the tile and its
+// 2-cell halo, no multicast) in a ring of R slots, and stays there as
+// conserved totals until its cells are updated.
+//   * Owned warps (TY): warp r owns row y0 + r; lane l owns the two adjacent
+//     cells (z, z + 1), z = z0 + 2l, as one pair.  Every per-cell formula is
+//     written on pairs, and in FP32 a pair is one packed register, so the
+//     arithmetic runs on Blackwell's packed instructions (add/sub/mul/fma
+//     .f32x2: two cells per instruction).  The x-neighbours of a cell are
+//     carried in registers along the march; the y-neighbours come from the
+//     other warps' rows through shared memory; the z-neighbours from shared
+//     memory (primitives) and warp shuffles (face states, fluxes).
+//   * Halo warp A: the row below the tile and the halo columns left/right of
+//     it; halo warp B: the row above the tile, the face between it and the
+//     tile's top row, and the faces on the tile's right edge.  They produce
+//     the predicted face states (or, on a domain face, what the reference's
+//     ghost-layer rules leave there) and the fluxes no owned lane computes,
+//     so the owned warps run no halo code: their only boundary handling is
+//     per-plane / per-row / per-lane switches.
+// One block barrier per plane.  Before it: convert plane m + 1 to
+// primitives, slopes and predicted state of plane m, the x-face flux between
+// planes m - 1 and m, publish face states.  After it: the y- and z-face
+// fluxes of plane m and the update of plane m - 1.
+//
+// Ghost-layer rules of the reference's derived arrays (gradients, predicted
+// states, fluxes; boundaries.rs:5-195 and handle_walls :197-407 applied to
+// them in compute_step, physics.rs:595-681), as composed rules:
+//   periodic: ghosts are computed like interior cells from the ghost
+//             primitives (the ghost layers hold the wrapped copies);
+//   outflow:  a ghost takes the adjacent interior cell's slopes and
+//             prediction, and the lower face repeats the next face's flux,
+//             so the first interior cell sees no divergence along that axis;
+//   wall:     a ghost's slopes come from its own (mirrored) primitives and
+//             its prediction is the mirrored prediction of the interior cell.
+//
+// Flux convention: face() returns 2F for mass and momenta and 4F for energy
+// (F the reference's flux without its final *ds); the update scales undo it.
+#pragma once
+#include "dg_common.cuh"
+
+namespace dg {
+namespace sweep {
+
+constexpr int kTileZ = 64;            // tile columns: 32 lanes x 2 cells
+constexpr int kBoxZ = kTileZ + 4;     // staged columns: 2-cell halo each side
+
+// ---------------------------------------------------------------------------
+// Pair arithmetic.  float2: packed FP32 instructions; double2: two scalar
+// operations.  Scalars of the pair's element type have the same interface.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 vadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 vmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 vfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 vsub(float2 a, float2 b) {
+    float2 r;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\t"
+        "mov.b64 rb, {%4, %5};\n\t"
+        "sub.rn.f32x2 rd, ra, rb;\n\t"
+        "mov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+__device__ __forceinline__ double2 vadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 vsub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 vmul(double2 a, double2 b) { return make_double2(a.x * b.x, a.y * b.y); }
+__device__ __forceinline__ double2 vfma(double2 a, double2 b, double2 c) {
+    return make_double2(fma(a.x, b.x, c.x), fma(a.y, b.y, c.y));
+}
+
+template <class T> struct PairT;
+template <> struct PairT<float> { using type = float2; };
+template <> struct PairT<double> { using type = double2; };
+
+template <class V> __device__ __forceinline__ V spl(double s);
+template <> __device__ __forceinline__ float2 spl<float2>(double s) { return make_float2((float)s, (float)s); }
+template <> __device__ __forceinline__ double2 spl<double2>(double s) { return make_double2(s, s); }
+__device__ __forceinline__ float2 mk(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ double2 mk(double a, double b) { return make_double2(a, b); }
+
+// 1/x of both cells: the fast policy's reciprocal (Phys<T, false>::prim).
+__device__ __forceinline__ float2 vrcp(float2 a) { return make_float2(__fdividef(1.0f, a.x), __fdividef(1.0f, a.y)); }
+__device__ __forceinline__ double2 vrcp(double2 a) { return make_double2(1.0 / a.x, 1.0 / a.y); }
+__device__ __forceinline__ float2 vrsq(float2 a) { return make_float2(rsqrtf(a.x), rsqrtf(a.y)); }
+__device__ __forceinline__ double2 vrsq(double2 a) { return make_double2(rsqrt(a.x), rsqrt(a.y)); }
+__device__ __forceinline__ float2 vmax(float2 a, float2 b) { return make_float2(fmaxf(a.x, b.x), fmaxf(a.y, b.y)); }
+__device__ __forceinline__ double2 vmax(double2 a, double2 b) { return make_double2(fmax(a.x, b.x), fmax(a.y, b.y)); }
+__device__ __forceinline__ float2 vabs(float2 a) { return make_float2(fabsf(a.x), fabsf(a.y)); }
+__device__ __forceinline__ double2 vabs(double2 a) { return make_double2(fabs(a.x), fabs(a.y)); }
+
+// minmod(a, b): 0 when the signs differ or either is zero, else the one of
+// smaller magnitude.  FP32: min(|a|, |b|) carrying the product of the signs
+// (min.xorsign.abs), clamped at zero, given a's sign; equal to the clamp
+// form min(max(b, min(a, 0)), max(a, 0)) except for the sign of a zero.
+__device__ __forceinline__ float mm(float a, float b) {
+    float r;
+    asm("min.xorsign.abs.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+    r = fmaxf(r, 0.0f);
+    return __int_as_float(__float_as_int(r) | (__float_as_int(a) & (int)0x80000000));
+}
+__device__ __forceinline__ double mm(double a, double b) { return fmin(fmax(b, fmin(a, 0.0)), fmax(a, 0.0)); }
+__device__ __forceinline__ float2 mm(float2 a, float2 b) { return make_float2(mm(a.x, b.x), mm(a.y, b.y)); }
+__device__ __forceinline__ double2 mm(double2 a, double2 b) { return make_double2(mm(a.x, b.x), mm(a.y, b.y)); }
+
+// Slope in cell units (slope * ds) from the backward and forward
+// differences: minmod (LIM 1) or the reference's central difference
+// (LIM 0, physics.rs:206-208, times ds).
+template <int LIM, class V> __device__ __forceinline__ V slope(V dm, V dp) {
+    if constexpr (LIM == 0) return vmul(vadd(dm, dp), spl<V>(0.5));
+    else return mm(dm, dp);
+}
+template <int LIM, class S> __device__ __forceinline__ S slope1(S dm, S dp) {
+    if constexpr (LIM == 0) return (dm + dp) * S(0.5);
+    else return mm(dm, dp);
+}
+
+// Per-grid constants of the kernel in the pair type.
+template <class T> struct K {
+    T inv_vol, gamma, gm1, kp, c1, sg, hd;
+    T sc[5];   // update scale per field: -dt ds^2 / 2 (mass, momenta), / 4 (energy)
+};
+
+// Conserved totals -> primitives (calc_primitives, physics.rs:112-140), the
+// fast policy's operation sequence (the same as Phys<T, false>::prim, so the
+// dt of the updated state agrees bit for bit with the state reduction).
+template <class V, class T> __device__ __forceinline__ void prim(const V u[5], V w[5], const K<T> &k) {
+    const V ir = vrcp(u[0]);
+    const V rho = vmul(u[0], spl<V>(k.inv_vol));
+    const V vx = vmul(u[1], ir), vy = vmul(u[2], ir), vz = vmul(u[3], ir);
+    const V v2 = vfma(vz, vz, vfma(vy, vy, vmul(vx, vx)));
+    w[0] = rho;
+    w[1] = vx;
+    w[2] = vy;
+    w[3] = vz;
+    w[4] = vmul(vfma(vmul(spl<V>(-0.5), rho), v2, vmul(u[4], spl<V>(k.inv_vol))), spl<V>(k.gm1));
+}
+
+// Half-step predictor (extrapolate_primitives_t, physics.rs:251-278) with
+// cell-unit slopes; hd = dt / (2 ds).
+template <class V, class T>
+__device__ __forceinline__ void predict(const V w[5], const V sx[5], const V sy[5], const V sz[5], const K<T> &k,
+                                        V out[5]) {
+    const V rho = w[0], vx = w[1], vy = w[2], vz = w[3], p = w[4];
+    const V nh = spl<V>(-(double)k.hd);
+    const V ir = vrcp(rho);
+    const V div = vadd(vadd(sx[1], sy[2]), sz[3]);
+    out[0] = vfma(nh, vfma(rho, div, vfma(vz, sz[0], vfma(vy, sy[0], vmul(vx, sx[0])))), rho);
+    out[1] = vfma(nh, vfma(ir, sx[4], vfma(vz, sz[1], vfma(vy, sy[1], vmul(vx, sx[1])))), vx);
+    out[2] = vfma(nh, vfma(ir, sy[4], vfma(vz, sz[2], vfma(vy, sy[2], vmul(vx, sx[2])))), vy);
+    out[3] = vfma(nh, vfma(ir, sz[4], vfma(vz, sz[3], vfma(vy, sy[3], vmul(vx, sx[3])))), vz);
+    const V gp = vmul(spl<V>(k.gamma), p);
+    out[4] = vfma(nh, vfma(vz, sz[4], vfma(vy, sy[4], vfma(vx, sx[4], vmul(gp, div)))), p);
+}
+
+// Rusanov face flux (calc_flux_reconstruction, physics.rs:338-400): a is the
+// state on the lower side of the face, b on the upper side, both (rho, vx,
+// vy, vz, p); N is the index of the normal velocity.  Star state = mean of
+// the two conserved states; flux = physical flux of the star state minus
+// c/2 (U_b - U_a), c the larger of the two sides' c_s + |v_n|.  Returns
+// 2F (mass, momenta) and 4F (energy), F without its *ds; with GRAV the
+// gravity source term of the z faces (physics.rs:366-372), gh = G h.
+template <int N, bool GRAV, class V, class T>
+__device__ __forceinline__ void face(const V a[5], const V b[5], V gh, const K<T> &k, V F[5]) {
+    constexpr int T1 = N == 1 ? 2 : 1, T2 = N == 3 ? 2 : 3;
+    const V ra = a[0], ua = a[N], va = a[T1], wa = a[T2], pa = a[4];
+    const V rb = b[0], ub = b[N], vb = b[T1], wb = b[T2], pb = b[4];
+    const V mua = vmul(ra, ua), mva = vmul(ra, va), mwa = vmul(ra, wa);
+    const V mub = vmul(rb, ub), mvb = vmul(rb, vb), mwb = vmul(rb, wb);
+    // twice the total energy of each side: rho |v|^2 + 2 p / (gamma - 1)
+    const V ea = vfma(mwa, wa, vfma(mva, va, vfma(mua, ua, vmul(spl<V>(k.kp), pa))));
+    const V eb = vfma(mwb, wb, vfma(mvb, vb, vfma(mub, ub, vmul(spl<V>(k.kp), pb))));
+    const V sr = vadd(ra, rb), smu = vadd(mua, mub), smv = vadd(mva, mvb), smw = vadd(mwa, mwb);
+    const V se = vadd(ea, eb);
+    const V irs = vrcp(sr);
+    const V us = vmul(smu, irs);                                                 // star normal velocity
+    const V kk = vfma(smu, us, vmul(vfma(smw, smw, vmul(smv, smv)), irs));       // |S_m|^2 / S_rho
+    const V p2 = vfma(kk, spl<V>(-(double)k.c1), vmul(se, spl<V>(k.c1)));        // 2 p*
+    const V ca = vfma(vmul(pa, vrsq(vmul(pa, ra))), spl<V>(k.sg), vabs(ua));   // c_s + |v_n|, side a
+    const V cb = vfma(vmul(pb, vrsq(vmul(pb, rb))), spl<V>(k.sg), vabs(ub));
+    const V nc = vmul(vmax(ca, cb), spl<V>(-1.0));
+    V fu = vfma(smu, us, p2);
+    V fe = vmul(vfma(p2, spl<V>(2.0), se), us);
+    if constexpr (GRAV) {
+        fu = vfma(sr, gh, fu);
+        fe = vfma(vmul(sr, vadd(ua, ub)), gh, fe);
+    }
+    F[0] = vfma(nc, vsub(rb, ra), smu);
+    F[N] = vfma(nc, vsub(mub, mua), fu);
+    F[T1] = vfma(nc, vsub(mvb, mva), vmul(smv, us));
+    F[T2] = vfma(nc, vsub(mwb, mwa), vmul(smw, us));
+    F[4] = vfma(nc, vsub(eb, ea), fe);
+}
+
+// xt +- s/2
+template <class V> __device__ __forceinline__ void half_step(const V xt[5], const V s[5], double sign, V out[5]) {
+#pragma unroll
+    for (int f = 0; f < 5; ++f) out[f] = vfma(s[f], spl<V>(0.5 * sign), xt[f]);
+}
+
+// Boundary modes of a tile side.
+enum Mode : int { kNormal = 0, kOut = 1, kWallM = 2 };
+
+__device__ __forceinline__ int side_mode(bool on_face, int bc) {
+    if (!on_face || bc == kPeriodic) return kNormal;
+    return bc == kOutflow ? kOut : kWallM;
+}
+
+template <class T, int TY, int R> struct Smem {
+    static constexpr int kRows = TY + 4;                  // staged rows y0-2 .. y0+TY+1
+    static constexpr int kFieldElems = kRows * kBoxZ;
+    static constexpr int kBoxBytes = 5 * kFieldElems * (int)sizeof(T);
+    static constexpr int kSlotElems = ((kBoxBytes + 127) / 128) * 128 / (int)sizeof(T);
+    static constexpr int kPbRows = TY + 2;                // primitive rows y0-1 .. y0+TY
+    T ring[R * kSlotElems];                               // conserved totals as staged
+    T pb[2][5][kPbRows][kBoxZ];                           // primitives, by plane parity
+    T ypl[2][TY + 1][5][kTileZ];                          // upper y state, rows y0-1 .. y0+TY-1
+    T fy[2][TY + 1][5][kTileZ];                           // flux of the lower y face, rows y0 .. y0+TY
+    T ytop[2][5][kTileZ];                                 // top row's xt (wall) or lower state (outflow)
+    T zl[2][TY][5];                                       // left halo column: upper z state (wall: +sz/2)
+    T zr[2][TY][5];                                       // right halo column: lower z state (wall: -sz/2)
+    T zeu[2][TY][5];                                      // last column's upper z state (even width)
+    T zex[2][TY][5];                                      // last column's xt (wall) or lower state (outflow)
+    T fz[2][TY][5];                                       // flux of the right edge face (even width)
+    uint64_t bar[R];
+    double red[(TY + 2) * 7];
+    // set when a wait gave up, read after the next barrier; two slots by
+    // plane parity, so a warp already working on plane m + 1 cannot flag a
+    // warp that is still between the barriers of plane m
+    int abort_flag[2];
+    int skip;
+    int is_last;
+};
+
+template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
+    using V = typename PairT<T>::type;
+    using Sm = Smem<T, TY, R>;
+    static constexpr int W = TY + 2;      // warps: TY owned rows, A, B
+    static constexpr int NT = 32 * W;
+    static constexpr int WA = TY, WB = TY + 1;
+
+    static __device__ __forceinline__ T *slot(Sm &s, int l) { return s.ring + (l % R) * Sm::kSlotElems; }
+    // staged conserved value: field f, staged row ry (0 = y0-2), column cz (0 = z0-2)
+    static __device__ __forceinline__ T &C(T *sl, int f, int ry, int cz) {
+        return sl[(f * Sm::kRows + ry) * kBoxZ + cz];
+    }
+    static __device__ __forceinline__ V ldv(const T *p) { return *reinterpret_cast<const V *>(p); }
+    static __device__ __forceinline__ void stv(T *p, V v) { *reinterpret_cast<V *>(p) = v; }
+
+    static __device__ __forceinline__ V mirror(V v, bool on) { return on ? vmul(v, spl<V>(-1.0)) : v; }
+
+    // Gravity height term of a z face whose lower cell has ghosted index klow.
+    static __device__ __forceinline__ T grav_h(const GridArgs<T> &a, int klow) {
+        return a.k.g * (T(a.nz - 4) * a.k.ds - T(klow - 2) * a.k.ds);
+    }
+
+    // NaN-propagating maximum of wave speeds.
+    static __device__ __forceinline__ float smax_of(float m, float v) { return max_nan(m, v); }
+    static __device__ __forceinline__ double smax_of(double m, double v) {
+        return (m != m || v != v) ? (m + v) : fmax(m, v);
+    }
+
+    // Wave speed c_s + |v| of one cell of the updated state (the quantity
+    // whose maximum sets the next dt, physics.rs:186-190).
+    static __device__ __forceinline__ T speed(T r, T vx, T vy, T vz, T p, const K<T> &k) {
+        if constexpr (sizeof(T) == 4) return fast_speed(r, vx, vy, vz, p, k.gamma);
+        else return sqrt(k.gamma * p / r) + sqrt(vx * vx + vy * vy + vz * vz);
+    }
+
+    // New state of a pair: wave speed (next dt) and the store, with the
+    // ghost-cell images of cells next to a domain face.
+    static __device__ __forceinline__ void epilogue(const GridArgs<T> &a, const K<T> &k, int xu, int y, int z,
+                                                    const V u[5], bool val0, bool val1, T &smax) {
+        V q[5];
+        prim(u, q, k);
+        if (val0) smax = smax_of(smax, speed(q[0].x, q[1].x, q[2].x, q[3].x, q[4].x, k));
+        if (val1) smax = smax_of(smax, speed(q[0].y, q[1].y, q[2].y, q[3].y, q[4].y, k));
+        const bool xi = xu <= 3 || xu >= a.nx - 4;
+        const bool yi = y <= 3 || y >= a.ny - 4;
+        const bool zi = z <= 3 || z + 1 >= a.nz - 4;
+        if (!xi && !yi && !zi && val1) {
+            const long long o = ((long long)xu * a.ny + y) * a.pitch + z;
+#pragma unroll
+            for (int f = 0; f < 5; ++f) stv(a.dst + f * a.fstride + o, u[f]);
+            return;
+        }
+        int ximg[4], xflp[4], yimg[4], yflp[4];
+        const int nxi = axis_images(xu, a.nx, a.bc[0], a.bc[1], ximg, xflp);
+        const int nyi = axis_images(y, a.ny, a.bc[2], a.bc[3], yimg, yflp);
+        for (int c = 0; c < 2; ++c) {
+            if (!(c ? val1 : val0)) continue;
+            int zimg[4], zflp[4];
+            const int nzi = axis_images(z + c, a.nz, a.bc[4], a.bc[5], zimg, zflp);
+            const T u0 = c ? u[0].y : u[0].x, u1 = c ? u[1].y : u[1].x, u2 = c ? u[2].y : u[2].x;
+            const T u3 = c ? u[3].y : u[3].x, u4 = c ? u[4].y : u[4].x;
+            for (int ix = 0; ix < nxi; ++ix)
+                for (int iy = 0; iy < nyi; ++iy)
+                    for (int iz = 0; iz < nzi; ++iz) {
+                        const long long o = ((long long)ximg[ix] * a.ny + yimg[iy]) * a.pitch + zimg[iz];
+                        a.dst[o] = u0;
+                        a.dst[a.fstride + o] = xflp[ix] ? -u1 : u1;
+                        a.dst[2 * a.fstride + o] = yflp[iy] ? -u2 : u2;
+                        a.dst[3 * a.fstride + o] = zflp[iz] ? -u3 : u3;
+                        a.dst[4 * a.fstride + o] = u4;
+                    }
+        }
+    }
+
+    // Load a pair of staged conserved values and convert it.
+    static __device__ __forceinline__ void load_prim_pair(T *sl, int ry, int cz, const K<T> &k, V q[5]) {
+        V u[5];
+#pragma unroll
+        for (int f = 0; f < 5; ++f) u[f] = ldv(&C(sl, f, ry, cz));
+        prim(u, q, k);
+    }
+    // Two staged cells that are not adjacent (columns c0, c1 of row ry).
+    static __device__ __forceinline__ void load_prim_split(T *sl, int ry, int c0, int c1, const K<T> &k, V q[5]) {
+        V u[5];
+#pragma unroll
+        for (int f = 0; f < 5; ++f) u[f] = mk(C(sl, f, ry, c0), C(sl, f, ry, c1));
+        prim(u, q, k);
+    }
+    static __device__ __forceinline__ void store_pb(Sm &s, int par, int row, int col, const V q[5]) {
+#pragma unroll
+        for (int f = 0; f < 5; ++f) stv(&s.pb[par][f][row][col], q[f]);
+    }
+
+    // Slopes and prediction of the pair of adjacent cells at primitive-buffer
+    // row `row`, columns (col, col + 1): x from the carried difference dq and
+    // the new one dn, y from rows row -+ 1 (or the values ym / yp when given),
+    // z from columns col - 1 and col + 2.
+    static __device__ __forceinline__ void slopes_adj(Sm &s, int par, int row, int col, const V q[5], const V dq[5],
+                                                      const V dn[5], const V *ym, const V *yp, V sx[5], V sy[5],
+                                                      V sz[5]) {
+#pragma unroll
+        for (int f = 0; f < 5; ++f) {
+            sx[f] = slope<LIM>(dq[f], dn[f]);
+            const V m = ym ? ym[f] : ldv(&s.pb[par][f][row - 1][col]);
+            const V p = yp ? yp[f] : ldv(&s.pb[par][f][row + 1][col]);
+            sy[f] = slope<LIM>(vsub(q[f], m), vsub(p, q[f]));
+            const T zl = s.pb[par][f][row][col - 1], zr = s.pb[par][f][row][col + 2];
+            const T dmid = q[f].y - q[f].x;
+            sz[f] = mk(slope1<LIM>(q[f].x - zl, dmid), slope1<LIM>(dmid, zr - q[f].y));
+        }
+    }
+
+    // Block-wide barrier reached from the three roles' own code (bar.sync
+    // counts arrivals, not call sites; every role takes the same sequence).
+    static __device__ __forceinline__ void barrier() { asm volatile("bar.sync 0;" ::: "memory"); }
+
+    // Geometry and constants of one work item, shared by the three roles.
+    struct Tile {
+        long long budget;   // SM clocks a wait for a staged plane may take
+        int y0, z0, xs, xe, np, vy, vz, e;
+        bool odd;
+        int ylo, yhi, zlo, zhi;
+        K<T> k;
+        V gh, ghe;   // gravity terms: the lane's two lower z faces, the right edge face
+    };
+
+    static __device__ __forceinline__ bool wait_plane(Sm &s, int l, long long budget) {
+        return mbar_wait(&s.bar[l % R], (l / R) & 1, budget);
+    }
+
+    // ---------------------------------------------------------------------
+    // Owned warp: row y0 + r, lane pair at buffer columns (col, col + 1).
+    // ---------------------------------------------------------------------
+    static __device__ void run_owned(Sm &s, const GridArgs<T> &a, const Tile &t, int r, int lane, T &smax) {
+        const unsigned full = 0xffffffffu;
+        const K<T> &k = t.k;
+        const int col = 2 + 2 * lane;
+        const bool active = r < t.vy;
+        const int y = t.y0 + r, z = t.z0 + 2 * lane;
+        const bool val0 = 2 * lane < t.vz, val1 = 2 * lane + 1 < t.vz;
+        const bool edge = lane == t.e;
+        const bool yout = r == 0 && t.ylo == kOut;
+        const bool zout = lane == 0 && t.zlo == kOut;
+        V q[5], dq[5], xtp[5], sxp[5], acc[5];
+#pragma unroll
+        for (int f = 0; f < 5; ++f) q[f] = dq[f] = xtp[f] = sxp[f] = acc[f] = spl<V>(0.0);
+        // prologue: planes xs-2, xs-1
+        bool ok = wait_plane(s, 0, t.budget);
+        if (ok && active) load_prim_pair(slot(s, 0), r + 2, col, k, q);
+        ok = ok && wait_plane(s, 1, t.budget);
+        if (ok && active) {
+            V qn[5];
+            load_prim_pair(slot(s, 1), r + 2, col, k, qn);
+            store_pb(s, (t.xs - 1) & 1, r + 1, col, qn);
+#pragma unroll
+            for (int f = 0; f < 5; ++f) { dq[f] = vsub(qn[f], q[f]); q[f] = qn[f]; }
+        }
+        if (!ok) s.abort_flag[t.xs & 1] = 1;
+        fence_proxy_async();
+        barrier();
+        if (s.abort_flag[t.xs & 1]) return;
+        for (int m = t.xs - 1; m <= t.xe; ++m) {
+            const int l = m - t.xs + 3;
+            const int pm = m & 1;
+            const bool upd = m >= t.xs && m < t.xe;
+            V sy[5], sz[5], tu[5];
+            if (!wait_plane(s, l, t.budget)) s.abort_flag[m & 1] = 1;
+            if (active) {
+                V qn[5], dn[5], sx[5], xt[5];
+                load_prim_pair(slot(s, l), r + 2, col, k, qn);
+                store_pb(s, (m + 1) & 1, r + 1, col, qn);
+#pragma unroll
+                for (int f = 0; f < 5; ++f) dn[f] = vsub(qn[f], q[f]);
+                slopes_adj(s, pm, r + 1, col, q, dq, dn, nullptr, nullptr, sx, sy, sz);
+                predict(q, sx, sy, sz, k, xt);
+                if (m >= t.xs) {
+                    // ghost rules of the x faces: a wall's ghost plane 1 takes the
+                    // mirrored prediction of plane 2; the upper ghost plane takes
+                    // the last plane's state (outflow) or its mirror (wall)
+                    if (m == 2 && a.bc[0] == kWall) {
+#pragma unroll
+                        for (int f = 0; f < 5; ++f) xtp[f] = xt[f];
+                        xtp[1] = mirror(xtp[1], true);
+                    }
+                    if (m == a.nx - 2) {
+                        if (a.bc[1] == kOutflow) {
+#pragma unroll
+                            for (int f = 0; f < 5; ++f) { xt[f] = xtp[f]; sx[f] = sxp[f]; }
+                        } else if (a.bc[1] == kWall) {
+#pragma unroll
+                            for (int f = 0; f < 5; ++f) xt[f] = xtp[f];
+                            xt[1] = mirror(xt[1], true);
+                        }
+                    }
+                    V lo[5], up[5], fx[5];
+                    half_step(xtp, sxp, 1.0, lo);
+                    half_step(xt, sx, -1.0, up);
+                    face<1, false>(lo, up, spl<V>(0.0), k, fx);
+                    // lower outflow x face: plane 2 sees no x divergence
+                    const bool xo_prev = m - 1 == 2 && a.bc[0] == kOutflow;
+                    const bool xo = m == 2 && a.bc[0] == kOutflow;
+#pragma unroll
+                    for (int f = 0; f < 5; ++f) {
+                        tu[f] = xo_prev ? acc[f] : vadd(acc[f], fx[f]);
+                        acc[f] = xo ? spl<V>(0.0) : vmul(fx[f], spl<V>(-1.0));
+                    }
+                }
+#pragma unroll
+                for (int f = 0; f < 5; ++f) { xtp[f] = xt[f]; sxp[f] = sx[f]; }
+                if (upd) {
+                    V st[5];
+                    half_step(xt, sy, 1.0, st);
+#pragma unroll
+                    for (int f = 0; f < 5; ++f) stv(&s.ypl[pm][r + 1][f][2 * lane], st[f]);
+                    if (r == t.vy - 1 && t.yhi != kNormal) {
+                        // for the face above the top row (computed by warp B)
+                        if (t.yhi == kOut) half_step(xt, sy, -1.0, st);
+#pragma unroll
+                        for (int f = 0; f < 5; ++f) stv(&s.ytop[pm][f][2 * lane], t.yhi == kOut ? st[f] : xt[f]);
+                    }
+                    if (edge && !t.odd) {
+                        // the right edge face (warp B) needs the last column's states
+#pragma unroll
+                        for (int f = 0; f < 5; ++f) {
+                            s.zeu[pm][r][f] = xt[f].y + T(0.5) * sz[f].y;
+                            s.zex[pm][r][f] = t.zhi == kOut ? xt[f].y - T(0.5) * sz[f].y : xt[f].y;
+                        }
+                    }
+                }
+#pragma unroll
+                for (int f = 0; f < 5; ++f) { q[f] = qn[f]; dq[f] = dn[f]; }
+            }
+            fence_proxy_async();
+            barrier();
+            if (s.abort_flag[m & 1]) break;
+            if (!active) continue;
+            // ================= after the barrier =================
+            if (upd) {
+                const V *xt = xtp;
+                V dy[5];
+                if (!yout) {
+                    V lo[5], up[5], fyv[5];
+#pragma unroll
+                    for (int f = 0; f < 5; ++f) lo[f] = ldv(&s.ypl[pm][r][f][2 * lane]);
+                    if (r == 0 && t.ylo == kWallM) {
+                        // wall ghost row: mirrored prediction of this row + its own half slope
+#pragma unroll
+                        for (int f = 0; f < 5; ++f) lo[f] = vadd(lo[f], mirror(xt[f], f == 2));
+                    }
+                    half_step(xt, sy, -1.0, up);
+                    face<2, false>(lo, up, spl<V>(0.0), k, fyv);
+#pragma unroll
+                    for (int f = 0; f < 5; ++f) {
+                        stv(&s.fy[pm][r][f][2 * lane], fyv[f]);
+                        dy[f] = vmul(fyv[f], spl<V>(-1.0));
+                    }
+                } else {
+#pragma unroll
+                    for (int f = 0; f < 5; ++f) dy[f] = spl<V>(0.0);
+                }
+                V lo[5], up[5], fzv[5];
+#pragma unroll
+                for (int f = 0; f < 5; ++f) {
+                    const V U = vfma(sz[f], spl<V>(0.5), xt[f]);
+                    const V L = vfma(sz[f], spl<V>(-0.5), xt[f]);
+                    T left = __shfl_up_sync(full, U.y, 1);
+                    if (lane == 0) {
+                        left = s.zl[pm][r][f];
+                        if (t.zlo == kWallM) left += f == 3 ? -xt[f].x : xt[f].x;
+                    }
+                    lo[f] = mk(left, U.x);
+                    up[f] = L;
+                    if (edge && t.odd) {
+                        // the pair's second cell is the right ghost column
+                        T g = s.zr[pm][r][f];
+                        if (t.zhi == kWallM) g += f == 3 ? -xt[f].x : xt[f].x;
+                        if (t.zhi == kOut) g = L.x;
+                        up[f].y = g;
+                    }
+                }
+                face<3, GRAV>(lo, up, t.gh, k, fzv);
+#pragma unroll
+                for (int f = 0; f < 5; ++f) {
+                    T hi = __shfl_down_sync(full, fzv[f].x, 1);
+                    if (edge && !t.odd) hi = T(0);   // right edge face: added at the update
+                    V dz = vsub(mk(fzv[f].y, hi), fzv[f]);
+                    if (zout) dz.x = T(0);
+                    acc[f] = vadd(acc[f], vadd(dy[f], dz));
+                }
+            }
+            if (m - 1 >= t.xs && m - 1 < t.xe) {
+                // update of plane m-1: its upper y flux (row above) and right
+                // edge flux (warp B) arrived with this barrier
+                const int pp = (m - 1) & 1;
+                V u[5];
+                T *sl = slot(s, l - 2);
+#pragma unroll
+                for (int f = 0; f < 5; ++f) {
+                    V tt = tu[f];
+                    if (!yout) tt = vadd(tt, ldv(&s.fy[pp][r + 1][f][2 * lane]));
+                    if (edge && !t.odd) tt.y += s.fz[pp][r][f];
+                    u[f] = vfma(spl<V>(k.sc[f]), tt, ldv(&C(sl, f, r + 2, col)));
+                }
+                epilogue(a, k, m - 1, y, z, u, val0, val1, smax);
+            }
+        }
+    }
+
+    // ---------------------------------------------------------------------
+    // Halo warp A: the row below the tile (y0 - 1, lanes as pairs), the
+    // halo columns z0 - 1 and z0 + vz of rows y0 .. y0 + vy - 1 (lane l: row
+    // y0 + l, the two columns as one pair), the primitives of the staged
+    // columns outside the lanes' pairs, and the TMA copies.  Returns the
+    // number of planes it requested.
+    // ---------------------------------------------------------------------
+    static __device__ int run_a(Sm &s, const GridArgs<T> &a, const CUtensorMap *tmap, const Tile &t, int lane) {
+        const K<T> &k = t.k;
+        const int col = 2 + 2 * lane;
+        const bool tl = lane < t.vy;
+        const bool cl = lane < 2 * (TY + 2);
+        const int crow = lane >> 1, ccol = (lane & 1) ? kTileZ + 2 : 0;
+        const int rc = t.vz + 2;   // buffer column of the right halo column
+        int issued = t.np < R ? t.np : R;
+        V q[5], dq[5], q2[5], qt[5], dqt[5];
+#pragma unroll
+        for (int f = 0; f < 5; ++f) q[f] = dq[f] = q2[f] = qt[f] = dqt[f] = spl<V>(0.0);
+        auto convert = [&](int l, V qn[5], V q2n[5], V qtn[5], bool store) {
+            T *sl = slot(s, l);
+            const int par = (t.xs - 2 + l) & 1;
+            load_prim_pair(sl, 0, col, k, q2n);
+            load_prim_pair(sl, 1, col, k, qn);
+            if (tl) load_prim_split(sl, lane + 2, 1, rc, k, qtn);
+            if (store) {
+                store_pb(s, par, 0, col, qn);
+                if (cl) {
+                    V c[5];
+                    load_prim_pair(sl, crow + 1, ccol, k, c);
+                    store_pb(s, par, crow, ccol, c);
+                }
+            }
+        };
+        bool ok = wait_plane(s, 0, t.budget);
+        if (ok) convert(0, q, q2, qt, false);
+        ok = ok && wait_plane(s, 1, t.budget);
+        if (ok) {
+            V qn[5], q2n[5], qtn[5];
+            convert(1, qn, q2n, qtn, true);
+#pragma unroll
+            for (int f = 0; f < 5; ++f) {
+                dq[f] = vsub(qn[f], q[f]);
+                q[f] = qn[f];
+                q2[f] = q2n[f];
+                dqt[f] = vsub(qtn[f], qt[f]);
+                qt[f] = qtn[f];
+            }
+        }
+        if (!ok) s.abort_flag[t.xs & 1] = 1;
+        fence_proxy_async();
+        barrier();
+        if (s.abort_flag[t.xs & 1]) return issued;
+        for (int m = t.xs - 1; m <= t.xe; ++m) {
+            const int l = m - t.xs + 3;
+            const int pm = m & 1;
+            const bool upd = m >= t.xs && m < t.xe;
+            if (!wait_plane(s, l, t.budget)) s.abort_flag[m & 1] = 1;
+            V qn[5], q2n[5], qtn[5], dn[5], dtn[5];
+#pragma unroll
+            for (int f = 0; f < 5; ++f) qtn[f] = spl<V>(0.0);
+            convert(l, qn, q2n, qtn, true);
+#pragma unroll
+            for (int f = 0; f < 5; ++f) {
+                dn[f] = vsub(qn[f], q[f]);
+                dtn[f] = vsub(qtn[f], qt[f]);
+            }
+            if (upd) {
+                V sx[5], sy[5], sz[5], xt[5], st[5];
+                if (t.ylo != kOut) {
+                    // row y0 - 1: its upper face state (wall ghost: its own half slope)
+                    slopes_adj(s, pm, 0, col, q, dq, dn, q2, nullptr, sx, sy, sz);
+                    if (t.ylo == kNormal) {
+                        predict(q, sx, sy, sz, k, xt);
+                        half_step(xt, sy, 1.0, st);
+                    } else {
+#pragma unroll
+                        for (int f = 0; f < 5; ++f) st[f] = vmul(sy[f], spl<V>(0.5));
+                    }
+#pragma unroll
+                    for (int f = 0; f < 5; ++f) stv(&s.ypl[pm][0][f][2 * lane], st[f]);
+                }
+                if (tl && !(t.zlo == kOut && t.zhi == kOut)) {
+                    // halo columns of row y0 + lane: left (x) and right (y) of the pair
+                    const int row = lane + 1;
+#pragma unroll
+                    for (int f = 0; f < 5; ++f) {
+                        sx[f] = slope<LIM>(dqt[f], dtn[f]);
+                        const V ym = mk(s.pb[pm][f][row - 1][1], s.pb[pm][f][row - 1][rc]);
+                        const V yp = mk(s.pb[pm][f][row + 1][1], s.pb[pm][f][row + 1][rc]);
+                        sy[f] = slope<LIM>(vsub(qt[f], ym), vsub(yp, qt[f]));
+                        const V zm = mk(s.pb[pm][f][row][0], s.pb[pm][f][row][rc - 1]);
+                        const V zp = mk(s.pb[pm][f][row][2], s.pb[pm][f][row][rc + 1]);
+                        sz[f] = slope<LIM>(vsub(qt[f], zm), vsub(zp, qt[f]));
+                    }
+                    predict(qt, sx, sy, sz, k, xt);
+#pragma unroll
+                    for (int f = 0; f < 5; ++f) {
+                        const T hz0 = T(0.5) * sz[f].x, hz1 = T(0.5) * sz[f].y;
+                        s.zl[pm][lane][f] = t.zlo == kWallM ? hz0 : xt[f].x + hz0;
+                        s.zr[pm][lane][f] = t.zhi == kWallM ? -hz1 : xt[f].y - hz1;
+                    }
+                }
+            }
+#pragma unroll
+            for (int f = 0; f < 5; ++f) {
+                q[f] = qn[f];
+                dq[f] = dn[f];
+                q2[f] = q2n[f];
+                qt[f] = qtn[f];
+                dqt[f] = dtn[f];
+            }
+            fence_proxy_async();
+            barrier();
+            if (s.abort_flag[m & 1]) break;
+            // the slot of plane m-2 is free: stage plane m-2+R
+            const int nl = m - t.xs + R;
+            if (lane == 0 && nl < t.np) {
+                mbar_expect_tx(&s.bar[nl % R], Sm::kBoxBytes);
+                tma_load_4d(slot(s, nl), tmap, t.z0 - 2, t.y0 - 2, t.xs - 2 + nl, 0, &s.bar[nl % R]);
+            }
+            if (nl < t.np) issued = nl + 1;
+        }
+        return issued;
+    }
+
+    // ---------------------------------------------------------------------
+    // Halo warp B: the row above the tile (y0 + vy, lanes as pairs), the
+    // face between it and the tile's top row, and (even tile width) the
+    // faces on the tile's right edge, two rows per lane.
+    // ---------------------------------------------------------------------
+    static __device__ void run_b(Sm &s, const GridArgs<T> &a, const Tile &t, int lane) {
+        const K<T> &k = t.k;
+        const int col = 2 + 2 * lane;
+        const int br = t.vy + 1;   // buffer row of y0 + vy
+        V q[5], dq[5], q2[5], lb[5];
+#pragma unroll
+        for (int f = 0; f < 5; ++f) q[f] = dq[f] = q2[f] = lb[f] = spl<V>(0.0);
+        bool ok = wait_plane(s, 0, t.budget);
+        if (ok) {
+            load_prim_pair(slot(s, 0), br + 1, col, k, q);
+            load_prim_pair(slot(s, 0), br + 2, col, k, q2);
+        }
+        ok = ok && wait_plane(s, 1, t.budget);
+        if (ok) {
+            V qn[5];
+            load_prim_pair(slot(s, 1), br + 1, col, k, qn);
+            load_prim_pair(slot(s, 1), br + 2, col, k, q2);
+            store_pb(s, (t.xs - 1) & 1, br, col, qn);
+#pragma unroll
+            for (int f = 0; f < 5; ++f) { dq[f] = vsub(qn[f], q[f]); q[f] = qn[f]; }
+        }
+        if (!ok) s.abort_flag[t.xs & 1] = 1;
+        fence_proxy_async();
+        barrier();
+        if (s.abort_flag[t.xs & 1]) return;
+        for (int m = t.xs - 1; m <= t.xe; ++m) {
+            const int l = m - t.xs + 3;
+            const int pm = m & 1;
+            const bool upd = m >= t.xs && m < t.xe;
+            if (!wait_plane(s, l, t.budget)) s.abort_flag[m & 1] = 1;
+            V qn[5], q2n[5], dn[5];
+            load_prim_pair(slot(s, l), br + 1, col, k, qn);
+            load_prim_pair(slot(s, l), br + 2, col, k, q2n);
+            store_pb(s, (m + 1) & 1, br, col, qn);
+#pragma unroll
+            for (int f = 0; f < 5; ++f) dn[f] = vsub(qn[f], q[f]);
+            if (upd && t.yhi != kOut) {
+                V sx[5], sy[5], sz[5], xt[5];
+                slopes_adj(s, pm, br, col, q, dq, dn, nullptr, q2, sx, sy, sz);
+                if (t.yhi == kNormal) {
+                    predict(q, sx, sy, sz, k, xt);
+                    half_step(xt, sy, -1.0, lb);
+                } else {
+#pragma unroll
+                    for (int f = 0; f < 5; ++f) lb[f] = vmul(sy[f], spl<V>(-0.5));
+                }
+            }
+#pragma unroll
+            for (int f = 0; f < 5; ++f) { q[f] = qn[f]; dq[f] = dn[f]; q2[f] = q2n[f]; }
+            fence_proxy_async();
+            barrier();
+            if (s.abort_flag[m & 1]) break;
+            if (!upd) continue;
+            {   // face (y0+vy-1 | y0+vy)
+                V lo[5], up[5], F[5];
+#pragma unroll
+                for (int f = 0; f < 5; ++f) {
+                    lo[f] = ldv(&s.ypl[pm][t.vy][f][2 * lane]);
+                    if (t.yhi == kNormal) up[f] = lb[f];
+                    else {
+                        const V x = ldv(&s.ytop[pm][f][2 * lane]);
+                        up[f] = t.yhi == kOut ? x : vadd(lb[f], mirror(x, f == 2));
+                    }
+                }
+                face<2, false>(lo, up, spl<V>(0.0), k, F);
+#pragma unroll
+                for (int f = 0; f < 5; ++f) stv(&s.fy[pm][t.vy][f][2 * lane], F[f]);
+            }
+            if (!t.odd && lane < TY / 2) {
+                // right edge faces of rows lane and lane + TY/2
+                const int ra = lane, rb = lane + TY / 2;
+                V lo[5], up[5], F[5];
+#pragma unroll
+                for (int f = 0; f < 5; ++f) {
+                    lo[f] = mk(s.zeu[pm][ra][f], s.zeu[pm][rb][f]);
+                    const V zr = mk(s.zr[pm][ra][f], s.zr[pm][rb][f]);
+                    const V zx = mk(s.zex[pm][ra][f], s.zex[pm][rb][f]);
+                    up[f] = t.zhi == kNormal ? zr : (t.zhi == kOut ? zx : vadd(zr, mirror(zx, f == 3)));
+                }
+                face<3, GRAV>(lo, up, t.ghe, k, F);
+#pragma unroll
+                for (int f = 0; f < 5; ++f) {
+                    s.fz[pm][ra][f] = F[f].x;
+                    s.fz[pm][rb][f] = F[f].y;
+                }
+            }
+        }
+    }
+
+    // One work item: tile (ty, tz) of grid `a`, x-planes of chunk cx.  Its
+    // partial result goes to a.part[part_idx]; the last of the grid's
+    // nparts items reduces them (next dt).  Returns false after a
+    // device-side wait timed out (status flag set).
+    static __device__ bool run_tile(const GridArgs<T> &a, const CUtensorMap *tmap, int tz, int ty, int cx, int chunk,
+                                    int part_idx, int nparts, unsigned char *raw) {
+        Sm &s = *reinterpret_cast<Sm *>(raw);
+        const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+        Tile t;
+        t.budget = wait_budget_of(a);
+        t.y0 = 2 + ty * TY;
+        t.z0 = 2 + tz * kTileZ;
+        t.xs = 2 + cx * chunk;
+        t.xe = min(t.xs + chunk, a.nx - 2);
+        t.np = t.xe - t.xs + 4;
+        t.vy = min(TY, a.ny - 2 - t.y0);
+        t.vz = min(kTileZ, a.nz - 2 - t.z0);
+        t.e = (t.vz - 1) >> 1;
+        t.odd = (t.vz & 1) != 0;
+        t.ylo = side_mode(t.y0 == 2, a.bc[2]);
+        t.yhi = side_mode(t.y0 + t.vy == a.ny - 2, a.bc[3]);
+        t.zlo = side_mode(t.z0 == 2, a.bc[4]);
+        t.zhi = side_mode(t.z0 + t.vz == a.nz - 2, a.bc[5]);
+
+        const unsigned step = (unsigned)a.ctl->step;
+        const T dt = (T)a.ctl->dt[step & 1];
+        t.k.inv_vol = a.k.inv_vol;
+        t.k.gamma = a.k.gamma;
+        t.k.gm1 = a.k.gm1;
+        t.k.kp = T(2) * a.k.inv_gm1;
+        t.k.c1 = T(0.5) * a.k.gm1;
+        t.k.sg = (T)sqrt((double)a.k.gamma);
+        t.k.hd = T(0.5) * dt * a.k.inv_ds;
+        {
+            const T scale = dt * a.k.ds * a.k.ds;
+            t.k.sc[0] = t.k.sc[1] = t.k.sc[2] = t.k.sc[3] = T(-0.5) * scale;
+            t.k.sc[4] = T(-0.25) * scale;
+        }
+        t.gh = t.ghe = spl<V>(0.0);
+        if constexpr (GRAV) {
+            t.gh = mk(grav_h(a, t.z0 + 2 * lane - 1), grav_h(a, t.z0 + 2 * lane));
+            const T g1 = grav_h(a, t.z0 + t.vz - 1);
+            t.ghe = mk(g1, g1);
+        }
+
+        // an earlier step's wait gave up: leave the state alone (read once,
+        // so every thread of the block takes the same branch)
+        if (tid == 0) {
+            s.skip = (*(volatile unsigned *)&a.ctl->flags & kStatusTimeout) != 0;
+            s.abort_flag[0] = s.abort_flag[1] = 0;
+            if (!s.skip) {
+                for (int i = 0; i < R; ++i) mbar_init(&s.bar[i], 1);
+                fence_mbar_init();
+            }
+        }
+        __syncthreads();
+        if (s.skip) return false;
+        if (warp == WA && lane == 0) {
+            for (int l = 0; l < R && l < t.np; ++l) {
+                mbar_expect_tx(&s.bar[l], Sm::kBoxBytes);
+                tma_load_4d(slot(s, l), tmap, t.z0 - 2, t.y0 - 2, t.xs - 2 + l, 0, &s.bar[l]);
+            }
+        }
+        T smax = T(0);
+        int issued = 0;
+        if (warp < TY) run_owned(s, a, t, warp, lane, smax);
+        else if (warp == WA) issued = run_a(s, a, tmap, t, lane);
+        else run_b(s, a, t, lane);
+        __syncthreads();
+        if (s.abort_flag[0] | s.abort_flag[1]) {
+            if (warp == WA && lane == 0) {
+                // let the copies in flight land before the block exits
+                for (int l2 = issued > R ? issued - R : 0; l2 < issued; ++l2)
+                    mbar_wait(&s.bar[l2 % R], (l2 / R) & 1, kWaitBudget);
+                atomicOr(&a.ctl->flags, kStatusTimeout);
+            }
+            return false;
+        }
+        // every staged plane was consumed: the barriers can be re-initialised
+        // by the next work item of a persistent launch
+        if (tid == 0)
+            for (int i = 0; i < R; ++i) mbar_inval(&s.bar[i]);
+        // min over cells of ds/speed = ds / max speed
+        const unsigned nanf = smax != smax;
+        double wmin;
+        if constexpr (sizeof(T) == 4) wmin = nanf ? INFINITY : (double)__fdiv_rn(a.k.ds, smax);
+        else wmin = nanf ? INFINITY : a.k.ds / smax;
+        double sum[5] = {0, 0, 0, 0, 0};
+        if (block_partial(a, sum, wmin, nanf, tid, NT, s.red, &s.is_last, part_idx, nparts)) {
+            __threadfence();
+            final_reduce<T>(a, tid, NT, s.red, kAdvance, nparts);
+        }
+        return true;
+    }
+};
+
+// Shared memory of one block (bytes), with room to align the base to 1 KB.
+template <class T, int TY, int R> constexpr int smem_bytes() {
+    static_assert(sizeof(Smem<T, TY, R>) + 1024 <= 232448, "sweep tile exceeds the 227 KB of shared memory per block");
+    return (int)sizeof(Smem<T, TY, R>) + 1024;
+}
+
+// Registers per thread: the whole register file for one block of 32 (TY+2)
+// threads, in the allocation granule of 8 (FP32: 144 for 448 threads).
+template <int TY> constexpr int sweep_max_regs() {
+    return (65536 / (32 * (TY + 2))) / 8 * 8 > 255 ? 255 : (65536 / (32 * (TY + 2))) / 8 * 8;
+}
+
+template <class T, int TY, int R, int LIM, bool GRAV>
+__global__ void __maxnreg__(sweep_max_regs<TY>()) sweep_step_kernel(const GridArgs<T> a,
+                                                                      const __grid_constant__ CUtensorMap tmap,
+                                                                      int chunk) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    const int tiles_z = (a.nz - 4 + kTileZ - 1) / kTileZ;
+    const int tiles_y = (a.ny - 4 + TY - 1) / TY;
+    int b = blockIdx.x;
+    const int tz = b % tiles_z;
+    b /= tiles_z;
+    const int ty = b % tiles_y;
+    Sweep<T, TY, R, LIM, GRAV>::run_tile(a, &tmap, tz, ty, b / tiles_y, chunk, blockIdx.x, gridDim.x, smem_raw);
+}
+
+// Batched step: one persistent launch advances many independent grids by
+// one step each.  Work items (grid, tile, x-chunk) are taken from an atomic
+// queue; each grid keeps its own control block, so its dt is its own CFL dt.
+// Grid arguments are copied to shared memory per item and then to
+// registers; the grid's TMA descriptor is read from global memory (written
+// by the host before launch).  All grids of one launch share the limiter and
+// the gravity switch (the host launches one kernel per combination).
+struct BatchItem {
+    int g, local, tz, ty, cx;
+};
+
+template <int TY, int R, int LIM, bool GRAV>
+__global__ void __maxnreg__(sweep_max_regs<TY>()) sweep_batch_kernel(const GridArgs<float> *__restrict__ args,
+                                                                     const CUtensorMap *__restrict__ maps,
+                                                                     const BatchItem *__restrict__ items,
+                                                                     int nitems, unsigned *queue, int chunk) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ int s_item;
+    __shared__ __align__(16) GridArgs<float> s_args;
+    const int tid = threadIdx.x;
+    for (;;) {
+        if (tid == 0) s_item = (int)atomicAdd(queue, 1u);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= nitems) return;
+        const BatchItem bi = items[it];
+        constexpr int kWords = (int)(sizeof(GridArgs<float>) / 4);
+        for (int i = tid; i < kWords; i += blockDim.x)
+            reinterpret_cast<int *>(&s_args)[i] = reinterpret_cast<const int *>(&args[bi.g])[i];
+        __syncthreads();
+        const GridArgs<float> ga = s_args;
+        const bool ok = Sweep<float, TY, R, LIM, GRAV>::run_tile(ga, &maps[bi.g], bi.tz, bi.ty, bi.cx, chunk,
+                                                                 bi.local, ga.nparts, smem_raw);
+        __syncthreads();
+        if (!ok) return;
+    }
+}
+
+}  // namespace sweep
+}  // namespace dg

@@ -26,7 +26,7 @@ DG_ERR_NO_DEVICE = -5
 PERIODIC, OUTFLOW, WALL = 0, 1, 2
 LIMITER_NONE, LIMITER_MINMOD = 0, 1
 F32, F64 = 0, 1
-ROUNDING_DEFAULT, ROUNDING_REFERENCE = 0, 1
+ROUNDING_DEFAULT, ROUNDING_REFERENCE, ROUNDING_FAST = 0, 1, 2
 STATUS_NONFINITE = 0x1
 STATUS_TIMEOUT = 0x2
 SNAP_PRIMITIVES, SNAP_CONSERVED = 0x1, 0x2
@@ -80,6 +80,7 @@ SIGNATURES = {
     "dg_compute_step_dt": [_P, ctypes.c_double],
     "dg_next_dt": [_P, ctypes.POINTER(ctypes.c_double)],
     "dg_compute_step_noalloc": [ctypes.POINTER(SimInfo), _P, _P, ctypes.POINTER(ctypes.c_double), _P],
+    "dg_noalloc_status": [_I, ctypes.POINTER(ctypes.c_uint32)],
     "dg_snapshot_create": [_P, ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p)],
     "dg_snapshot_destroy": [_P],
     "dg_snapshot_begin": [_P],

@@ -66,9 +66,13 @@ extern "C" {
 /* arithmetic policy: DEFAULT = fast fused arithmetic for DG_F32 and the
  * reference's rounding for DG_F64; REFERENCE = the reference's operation
  * order without fused multiply-add, IEEE divide/sqrt (bitwise reproducible
- * against a scalar restatement of the Rust code) for either precision */
+ * against a scalar restatement of the Rust code) for either precision;
+ * FAST = the fused-arithmetic production kernel in either precision (in
+ * DG_F64 it is that kernel's double build, within 1e-12 of the reference's
+ * arithmetic rather than bit for bit) */
 #define DG_ROUNDING_DEFAULT 0
 #define DG_ROUNDING_REFERENCE 1
+#define DG_ROUNDING_FAST 2
 
 /* status flags (dg_status) */
 #define DG_STATUS_NONFINITE 0x1u  /* a NaN wave speed was seen; dt fell back to cfl*1.0
@@ -176,17 +180,26 @@ int32_t dg_compute_step_dt(dg_ctx *ctx, double dt);
  *             step, ghosts filled.
  *   dt_used   host pointer or NULL: the dt of the step (from cons_in, as
  *             calc_timestep computes it); when given, the call waits for
- *             the stream.
+ *             the stream and reports a device-side wait that gave up as
+ *             DG_ERR_TIMEOUT.  Without it the call returns at once and
+ *             cannot see the device's status: read it with
+ *             dg_noalloc_status after synchronizing the stream.
  *   stream    cudaStream_t or NULL.
  * The step's scratch (control block and per-block partials) is a 1 MiB
  * array in the library's device image, held by every GPU that loads the
  * library until exit; grids needing more than it holds are rejected with
  * DG_ERR_INVALID.  All calls share that array: calls that overlap on the
  * GPU race.  The first call on a device looks up the array's address with
- * that device current; make it before any stream capture.  Errors:
- * dg_last_error(NULL). */
+ * that device current; make it before any stream capture.  The calling
+ * thread's current device is the same after the call as before it.
+ * Errors: dg_last_error(NULL). */
 int32_t dg_compute_step_noalloc(const dg_sim_info *info, void *cons_in, void *cons_out, double *dt_used,
                                 void *stream);
+/* DG_STATUS_* flags the last dg_compute_step_noalloc call on `device` left
+ * in the shared scratch (DG_STATUS_TIMEOUT: that step's output is invalid).
+ * Call it after the stream of that step has been synchronized; the next
+ * no-allocation step on the device clears them.  Allocates nothing. */
+int32_t dg_noalloc_status(int32_t device, uint32_t *flags);
 
 /* ---- Snapshots (save_to_disk, io.rs:5-196) -------------------------------
  * The groups save_to_disk writes for the state: "primitives" (rho, vx, vy,
@@ -245,7 +258,8 @@ int32_t dg_batch_enqueue(dg_batch *b, int32_t nsteps);
 int32_t dg_batch_get_dts(dg_batch *b, int32_t i, int32_t nsteps, double *dts);
 /* grid i's conserved state, ghosts filled, as dg_get_conserved */
 int32_t dg_batch_get_conserved(dg_batch *b, int32_t i, void *const cons[5]);
-/* tile rows (16 or 8) and x-planes per work item (0 = automatic) */
+/* tile rows (12, the production kernel's tile) and x-planes per work item
+ * (0 = automatic) */
 int32_t dg_batch_set_tiling(dg_batch *b, int32_t tile_rows, int32_t chunk);
 int32_t dg_batch_get_tiling(dg_batch *b, int32_t *tile_rows, int32_t *chunk, int32_t *items);
 /* times `steps` steps of each candidate tiling on the live batch, keeps the

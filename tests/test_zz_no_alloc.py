@@ -6,8 +6,10 @@ start-up.  For them the library offers this entry point: the caller passes
 the input and output states, and the step's scratch lives in a fixed array
 inside the library.  These tests call it through the C ABI on buffers the
 test owns and check it against the context entry point (dg_create +
-dg_compute_step) on the same state, two calls in a row, within the parity
-tolerances used elsewhere (1e-5 relative L1 for FP32, 1e-12 for FP64).
+dg_compute_step) on the same state, two calls in a row.  Both run the same
+kernels on the same values (only the row pitch of the layout can differ),
+so the outputs and dts must agree bit for bit; the parity tolerances used
+elsewhere (1e-5 relative L1 for FP32, 1e-12 for FP64) are far looser.
 
 The file is named to be collected last, so that a failure here does not
 stop the rest of a `pytest -x` run.
@@ -17,7 +19,7 @@ import ctypes
 import numpy as np
 import pytest
 
-from conftest import rel_l1, random_primitives
+from conftest import INTERIOR, rel_l1, random_primitives
 from deepgreen import capi
 
 pytestmark = pytest.mark.gpu
@@ -33,14 +35,27 @@ def _noalloc(lib, info, src_ptr, dst_ptr):
     return dt.value
 
 
-@pytest.mark.parametrize("precision", [capi.F32, capi.F64])
+CASES = [
+    # (precision, rounding, limiter): every kernel the entry point dispatches to
+    (capi.F32, capi.ROUNDING_DEFAULT, capi.LIMITER_MINMOD),
+    (capi.F32, capi.ROUNDING_DEFAULT, capi.LIMITER_NONE),
+    (capi.F32, capi.ROUNDING_REFERENCE, capi.LIMITER_MINMOD),
+    (capi.F64, capi.ROUNDING_DEFAULT, capi.LIMITER_MINMOD),
+    (capi.F64, capi.ROUNDING_FAST, capi.LIMITER_MINMOD),
+]
+# (20, 18, 28): nz + 4 = 32, the same row pitch as a context; (13, 18, 40):
+# ragged tiles along y and z and a row pitch (44) unlike the context's (64)
+SHAPES = [(20, 18, 28), (13, 18, 40)]
+
+
+@pytest.mark.parametrize("precision, rounding, limiter", CASES)
 @pytest.mark.parametrize("bcs", [(0,) * 6, (2, 2, 1, 1, 0, 0)])
-def test_noalloc_matches_context_entry_point_two_calls(precision, bcs):
+@pytest.mark.parametrize("shape", SHAPES)
+def test_noalloc_matches_context_entry_point_two_calls(precision, rounding, limiter, bcs, shape):
     import torch
 
-    shape = (20, 18, 28)            # nz + 4 = 32: rows are 16-byte multiples
     ds = 0.05
-    ctx = capi.Context(shape, ds, bcs, gamma=1.4, cfl=0.4, limiter=capi.LIMITER_MINMOD, precision=precision)
+    ctx = capi.Context(shape, ds, bcs, gamma=1.4, cfl=0.4, limiter=limiter, precision=precision, rounding=rounding)
     ctx.set_primitives(random_primitives(shape, 321))
     start = ctx.get_conserved()
     ref_dts, ref = [], []
@@ -50,6 +65,7 @@ def test_noalloc_matches_context_entry_point_two_calls(precision, bcs):
 
     lib = capi.load()
     dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
     tdtype = torch.float64 if precision == capi.F64 else torch.float32
     a = torch.from_numpy(np.stack(start)).to(device=dev, dtype=tdtype).contiguous()
     b = torch.empty_like(a)
@@ -57,10 +73,45 @@ def test_noalloc_matches_context_entry_point_two_calls(precision, bcs):
     dts = [_noalloc(lib, ctx.info, a.data_ptr(), b.data_ptr()),
            _noalloc(lib, ctx.info, b.data_ptr(), c.data_ptr())]
     outs = [b.cpu().numpy(), c.cpu().numpy()]
+    flags = ctypes.c_uint32(99)
+    assert lib.dg_noalloc_status(0, ctypes.byref(flags)) == capi.DG_OK
+    assert flags.value == 0
     for call in range(2):
-        np.testing.assert_allclose(dts[call], ref_dts[call], rtol=TOL[precision])
+        assert dts[call] == ref_dts[call], (call, dts[call], ref_dts[call])
+        for f in range(5):
+            np.testing.assert_array_equal(outs[call][f][INTERIOR], ref[call][f][INTERIOR],
+                                          err_msg=f"call {call} field {f}")
         errs = [rel_l1(outs[call][f], ref[call][f]) for f in range(5)]
         assert max(errs) <= TOL[precision], (call, errs)
+
+
+def test_noalloc_without_dt_returns_at_once_and_reports_status():
+    """dt_used NULL: no wait inside the call; after the caller synchronizes,
+    dg_noalloc_status reads the step's flags; the current device is kept."""
+    import torch
+
+    shape = (16, 16, 28)
+    ctx = capi.Context(shape, 0.05, (0,) * 6, gamma=1.4, cfl=0.4, limiter=capi.LIMITER_MINMOD, precision=capi.F32)
+    ctx.set_primitives(random_primitives(shape, 9))
+    start = ctx.get_conserved()
+    ctx.compute_step(1)
+    ref = ctx.get_conserved()
+    lib = capi.load()
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    a = torch.from_numpy(np.stack(start)).to(dev).contiguous()
+    b = torch.empty_like(a)
+    rc = lib.dg_compute_step_noalloc(ctypes.byref(ctx.info), ctypes.c_void_p(a.data_ptr()),
+                                     ctypes.c_void_p(b.data_ptr()), None, None)
+    assert rc == capi.DG_OK, lib.dg_last_error(None).decode()
+    torch.cuda.synchronize()
+    flags = ctypes.c_uint32(99)
+    assert lib.dg_noalloc_status(0, ctypes.byref(flags)) == capi.DG_OK
+    assert flags.value == 0
+    assert torch.cuda.current_device() == 0
+    out = b.cpu().numpy()
+    for f in range(5):
+        np.testing.assert_array_equal(out[f][INTERIOR], ref[f][INTERIOR])
 
 
 def test_noalloc_rejects_grids_beyond_its_scratch():
@@ -74,6 +125,13 @@ def test_noalloc_rejects_grids_beyond_its_scratch():
     rc = lib.dg_compute_step_noalloc(ctypes.byref(info), ctypes.c_void_p(256), ctypes.c_void_p(512), None, None)
     assert rc == capi.DG_ERR_INVALID
     assert b"scratch" in lib.dg_last_error(None)
+
+
+def test_noalloc_status_rejects_a_bad_device():
+    lib = capi.load()
+    flags = ctypes.c_uint32(0)
+    assert lib.dg_noalloc_status(-1, ctypes.byref(flags)) == capi.DG_ERR_NO_DEVICE
+    assert lib.dg_noalloc_status(0, None) == capi.DG_ERR_INVALID
 
 
 def test_noalloc_rejects_rows_that_break_tma_alignment():
