@@ -27,7 +27,7 @@ using sweep::BatchItem;
 namespace {
 
 constexpr int kTY = kSweepRowsF32;   // tile rows of the batched sweep
-constexpr int kRing = 5;
+constexpr int kRing = sizeof(sweep::Smem<float, kTY, 5>) + 1024 <= 232448 ? 5 : 4;
 constexpr int kTZs = sweep::kTileZ;  // tile columns
 constexpr int kCombos = 4;           // (limiter, gravity) pairs; one launch each
 
@@ -461,10 +461,11 @@ int32_t dg_batch_get_conserved(dg_batch *b, int32_t i, void *const cons[5]) {
     return DG_OK;
 }
 
-// Tile rows (12: the sweep kernel's tile) and x-planes per work item
-// (0 = automatic).
+// Tile rows (the sweep kernel's tile rows, as dg_batch_get_tiling reports
+// them) and x-planes per work item (0 = automatic).
 int32_t dg_batch_set_tiling(dg_batch *b, int32_t tile_rows, int32_t chunk) {
-    if (!b || tile_rows != kTY || chunk < 0) return bfail(b, DG_ERR_INVALID, "bad tiling (tile rows must be 12)");
+    if (!b || tile_rows != kTY || chunk < 0)
+        return bfail(b, DG_ERR_INVALID, "bad tiling (tile rows must be " + std::to_string(kTY) + ")");
     b->tile_rows = tile_rows;
     b->chunk = chunk;
     b->dirty = true;

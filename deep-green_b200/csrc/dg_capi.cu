@@ -268,9 +268,9 @@ int32_t dg_create(const dg_sim_info *info, dg_ctx **out) {
     c->pitch = (c->nz + 31) / 32 * 32;
     // Test hook: a context created while DG_DEBUG_WAIT_BUDGET is set gives
     // its step kernels' waits for staged planes that many SM clocks (0 or
-    // less: give up at the first unfinished wait) instead of ~2 s, so that a
-    // test can make a wait run out and check that the step reports
-    // DG_ERR_TIMEOUT and the device stays usable.
+    // less: every such wait gives up at once, without waiting) instead of
+    // ~2 s, so that a test can make the waits run out and check that the
+    // step reports DG_ERR_TIMEOUT and the device stays usable.
     if (const char *wb = std::getenv("DG_DEBUG_WAIT_BUDGET")) {
         const long long v = std::atoll(wb);
         c->wait_budget = v > 0 ? v : -1;

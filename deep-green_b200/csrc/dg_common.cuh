@@ -36,8 +36,10 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
                  : "memory");
 }
 
-// Bounded wait on an mbarrier phase: false after ~`budget` SM clocks.
+// Bounded wait on an mbarrier phase: false after ~`budget` SM clocks; a
+// negative budget gives up without waiting (the timeout test hook).
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long budget) {
+    if (budget < 0) return false;
     const uint32_t addr = smem_u32(bar);
     const long long t0 = clock64();
     while (true) {
@@ -67,10 +69,11 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, i
 constexpr long long kWaitBudget = 4000000000LL;  // ~2 s of SM clock
 
 // The budget a step kernel gives its waits for staged planes: the grid's own
-// (a context created with DG_DEBUG_WAIT_BUDGET set) or the default.  Waits
-// that let copies in flight land before a block exits keep kWaitBudget.
+// (a context created with DG_DEBUG_WAIT_BUDGET set; negative: give up at
+// once) or the default (0).  Waits that let copies in flight land before a
+// block exits keep kWaitBudget.
 template <class A> __device__ __forceinline__ long long wait_budget_of(const A &a) {
-    return a.wait_budget > 0 ? a.wait_budget : (a.wait_budget < 0 ? 0 : kWaitBudget);
+    return a.wait_budget != 0 ? a.wait_budget : kWaitBudget;
 }
 
 // ---------------------------------------------------------------------------

@@ -69,7 +69,10 @@ enum KernelKind : int { kRefF64 = 0, kRefF32 = 1, kFastF32 = 2, kFastF64 = 3 };
 inline bool is_sweep(int kind) { return kind == kFastF32 || kind == kFastF64; }
 
 // Owned tile rows (y) of each kernel.  A sweep block also runs two halo warps.
-constexpr int kSweepRowsF32 = 12;
+#ifndef DG_SWEEP_ROWS_F32
+#define DG_SWEEP_ROWS_F32 10
+#endif
+constexpr int kSweepRowsF32 = DG_SWEEP_ROWS_F32;
 constexpr int kSweepRowsF64 = 4;
 inline int step_tile_rows(int kind) {
     switch (kind) {

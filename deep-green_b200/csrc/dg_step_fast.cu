@@ -10,7 +10,9 @@ namespace dg {
 namespace {
 template <class T> struct SweepCfg;
 template <> struct SweepCfg<float> {
-    static constexpr int TY = kSweepRowsF32, R = 5;
+    // five staged planes when they fit in shared memory, else four
+    static constexpr int TY = kSweepRowsF32;
+    static constexpr int R = sizeof(sweep::Smem<float, TY, 5>) + 1024 <= 232448 ? 5 : 4;
 };
 template <> struct SweepCfg<double> {
     static constexpr int TY = kSweepRowsF64, R = 4;

@@ -183,18 +183,19 @@ __device__ __forceinline__ void face(const V a[5], const V b[5], V gh, const K<T
     const V p2 = vfma(kk, spl<V>(-(double)k.c1), vmul(se, spl<V>(k.c1)));        // 2 p*
     const V ca = vfma(vmul(pa, vrsq(vmul(pa, ra))), spl<V>(k.sg), vabs(ua));   // c_s + |v_n|, side a
     const V cb = vfma(vmul(pb, vrsq(vmul(pb, rb))), spl<V>(k.sg), vabs(ub));
-    const V nc = vmul(vmax(ca, cb), spl<V>(-1.0));
+    const V c = vmax(ca, cb);
     V fu = vfma(smu, us, p2);
-    V fe = vmul(vfma(p2, spl<V>(2.0), se), us);
+    V fe = vmul(vadd(vadd(p2, p2), se), us);
     if constexpr (GRAV) {
         fu = vfma(sr, gh, fu);
         fe = vfma(vmul(sr, vadd(ua, ub)), gh, fe);
     }
-    F[0] = vfma(nc, vsub(rb, ra), smu);
-    F[N] = vfma(nc, vsub(mub, mua), fu);
-    F[T1] = vfma(nc, vsub(mvb, mva), vmul(smv, us));
-    F[T2] = vfma(nc, vsub(mwb, mwa), vmul(smw, us));
-    F[4] = vfma(nc, vsub(eb, ea), fe);
+    // dissipation c (U_a - U_b) with the factors of the convention above
+    F[0] = vfma(c, vsub(ra, rb), smu);
+    F[N] = vfma(c, vsub(mua, mub), fu);
+    F[T1] = vfma(c, vsub(mva, mvb), vmul(smv, us));
+    F[T2] = vfma(c, vsub(mwa, mwb), vmul(smw, us));
+    F[4] = vfma(c, vsub(ea, eb), fe);
 }
 
 // xt +- s/2
@@ -265,50 +266,47 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
         return (m != m || v != v) ? (m + v) : fmax(m, v);
     }
 
-    // Wave speed c_s + |v| of one cell of the updated state (the quantity
-    // whose maximum sets the next dt, physics.rs:186-190).
-    static __device__ __forceinline__ T speed(T r, T vx, T vy, T vz, T p, const K<T> &k) {
-        if constexpr (sizeof(T) == 4) return fast_speed(r, vx, vy, vz, p, k.gamma);
-        else return sqrt(k.gamma * p / r) + sqrt(vx * vx + vy * vy + vz * vz);
+    // Wave speeds c_s + |v| of the pair's cells in the updated state (the
+    // quantity whose maximum sets the next dt, physics.rs:186-190).  FP32:
+    // fast_speed's operation sequence on pairs (every operation rounds as
+    // there, so dt agrees bit for bit with the state reduction); FP64: IEEE
+    // square roots.
+    static __device__ __forceinline__ V speed_pair(const V q[5], const K<T> &k) {
+        if constexpr (sizeof(T) == 4) {
+            const V g = vmul(spl<V>(k.gamma), q[4]);
+            const V cs = vmul(g, vrsq(vmul(g, q[0])));
+            const V v2 = vfma(q[3], q[3], vfma(q[2], q[2], vmul(q[1], q[1])));
+            const V vm = vmul(v2, vrsq(mk(fmaxf(v2.x, 1e-30f), fmaxf(v2.y, 1e-30f))));
+            return vadd(cs, vm);
+        } else {
+            auto one = [&](T r, T vx, T vy, T vz, T p) {
+                return sqrt(k.gamma * p / r) + sqrt(vx * vx + vy * vy + vz * vz);
+            };
+            return mk(one(q[0].x, q[1].x, q[2].x, q[3].x, q[4].x), one(q[0].y, q[1].y, q[2].y, q[3].y, q[4].y));
+        }
     }
 
-    // New state of a pair: wave speed (next dt) and the store, with the
-    // ghost-cell images of cells next to a domain face.
-    static __device__ __forceinline__ void epilogue(const GridArgs<T> &a, const K<T> &k, int xu, int y, int z,
-                                                    const V u[5], bool val0, bool val1, T &smax) {
-        V q[5];
-        prim(u, q, k);
-        if (val0) smax = smax_of(smax, speed(q[0].x, q[1].x, q[2].x, q[3].x, q[4].x, k));
-        if (val1) smax = smax_of(smax, speed(q[0].y, q[1].y, q[2].y, q[3].y, q[4].y, k));
-        const bool xi = xu <= 3 || xu >= a.nx - 4;
-        const bool yi = y <= 3 || y >= a.ny - 4;
-        const bool zi = z <= 3 || z + 1 >= a.nz - 4;
-        if (!xi && !yi && !zi && val1) {
-            const long long o = ((long long)xu * a.ny + y) * a.pitch + z;
-#pragma unroll
-            for (int f = 0; f < 5; ++f) stv(a.dst + f * a.fstride + o, u[f]);
-            return;
-        }
-        int ximg[4], xflp[4], yimg[4], yflp[4];
-        const int nxi = axis_images(xu, a.nx, a.bc[0], a.bc[1], ximg, xflp);
+    // The ghost-cell images of one updated cell (all but the cell itself):
+    // the copies the reference's ghost fill makes of a cell next to a domain
+    // face (axis_images: periodic wrap, outflow copy, wall mirror with the
+    // normal momentum negated).  Rare: only cells within two of a face.
+    static __device__ __noinline__ void images(const GridArgs<T> &a, int x, int y, int z, T u0, T u1, T u2, T u3,
+                                               T u4) {
+        int ximg[4], xflp[4], yimg[4], yflp[4], zimg[4], zflp[4];
+        const int nxi = axis_images(x, a.nx, a.bc[0], a.bc[1], ximg, xflp);
         const int nyi = axis_images(y, a.ny, a.bc[2], a.bc[3], yimg, yflp);
-        for (int c = 0; c < 2; ++c) {
-            if (!(c ? val1 : val0)) continue;
-            int zimg[4], zflp[4];
-            const int nzi = axis_images(z + c, a.nz, a.bc[4], a.bc[5], zimg, zflp);
-            const T u0 = c ? u[0].y : u[0].x, u1 = c ? u[1].y : u[1].x, u2 = c ? u[2].y : u[2].x;
-            const T u3 = c ? u[3].y : u[3].x, u4 = c ? u[4].y : u[4].x;
-            for (int ix = 0; ix < nxi; ++ix)
-                for (int iy = 0; iy < nyi; ++iy)
-                    for (int iz = 0; iz < nzi; ++iz) {
-                        const long long o = ((long long)ximg[ix] * a.ny + yimg[iy]) * a.pitch + zimg[iz];
-                        a.dst[o] = u0;
-                        a.dst[a.fstride + o] = xflp[ix] ? -u1 : u1;
-                        a.dst[2 * a.fstride + o] = yflp[iy] ? -u2 : u2;
-                        a.dst[3 * a.fstride + o] = zflp[iz] ? -u3 : u3;
-                        a.dst[4 * a.fstride + o] = u4;
-                    }
-        }
+        const int nzi = axis_images(z, a.nz, a.bc[4], a.bc[5], zimg, zflp);
+        for (int ix = 0; ix < nxi; ++ix)
+            for (int iy = 0; iy < nyi; ++iy)
+                for (int iz = 0; iz < nzi; ++iz) {
+                    if (ix == 0 && iy == 0 && iz == 0) continue;   // the cell itself
+                    const long long o = ((long long)ximg[ix] * a.ny + yimg[iy]) * a.pitch + zimg[iz];
+                    a.dst[o] = u0;
+                    a.dst[a.fstride + o] = xflp[ix] ? -u1 : u1;
+                    a.dst[2 * a.fstride + o] = yflp[iy] ? -u2 : u2;
+                    a.dst[3 * a.fstride + o] = zflp[iz] ? -u3 : u3;
+                    a.dst[4 * a.fstride + o] = u4;
+                }
     }
 
     // Load a pair of staged conserved values and convert it.
@@ -369,6 +367,15 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
 
     // ---------------------------------------------------------------------
     // Owned warp: row y0 + r, lane pair at buffer columns (col, col + 1).
+    //
+    // Plane m's iteration, before the barrier: convert plane m+1; update
+    // plane m-2 (its last fluxes arrived with the barrier of plane m-1) and
+    // compute its wave speeds; slopes, prediction and the x-face flux
+    // between planes m-1 and m; publish the face states other warps need;
+    // store plane m-2.  After the barrier: the y- and z-face fluxes of plane
+    // m.  The update comes first and its stores last, so that one straight
+    // run of code interleaves its long dependency chain (loads, reciprocal,
+    // square roots) with the slopes and the prediction of plane m.
     // ---------------------------------------------------------------------
     static __device__ void run_owned(Sm &s, const GridArgs<T> &a, const Tile &t, int r, int lane, T &smax) {
         const unsigned full = 0xffffffffu;
@@ -378,11 +385,97 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
         const int y = t.y0 + r, z = t.z0 + 2 * lane;
         const bool val0 = 2 * lane < t.vz, val1 = 2 * lane + 1 < t.vz;
         const bool edge = lane == t.e;
+        const bool edge_even = edge && !t.odd;
         const bool yout = r == 0 && t.ylo == kOut;
         const bool zout = lane == 0 && t.zlo == kOut;
-        V q[5], dq[5], xtp[5], sxp[5], acc[5];
+        const bool img_y = y <= 3 || y >= a.ny - 4;
+        const bool img_z = z <= 3 || z + 1 >= a.nz - 4;
+        V q[5], dq[5], xtp[5], sxp[5], acc[5], tu[5];
 #pragma unroll
-        for (int f = 0; f < 5; ++f) q[f] = dq[f] = xtp[f] = sxp[f] = acc[f] = spl<V>(0.0);
+        for (int f = 0; f < 5; ++f) q[f] = dq[f] = xtp[f] = sxp[f] = acc[f] = tu[f] = spl<V>(0.0);
+
+        // Update of plane xu (staged index sl_idx) with the term tu: the new
+        // state and its wave speeds (stores are left to the caller).
+        auto update = [&](int xu, int sl_idx, V u[5], V &sp) {
+            const int pp = xu & 1;
+            T *sl = slot(s, sl_idx);
+#pragma unroll
+            for (int f = 0; f < 5; ++f) {
+                V tt = tu[f];
+                // its upper y flux (row above) and right edge flux (warp B)
+                if (!yout) tt = vadd(tt, ldv(&s.fy[pp][r + 1][f][2 * lane]));
+                const T fe = s.fz[pp][r][f];
+                tt.y += edge_even ? fe : T(0);
+                u[f] = vfma(spl<V>(k.sc[f]), tt, ldv(&C(sl, f, r + 2, col)));
+            }
+            V w[5];
+            prim(u, w, k);
+            sp = speed_pair(w, k);
+        };
+        // Ghost images along z of the lane's pair.  With an even interior
+        // width every pair is aligned with the faces, and the images of a
+        // pair at a z face are one pair at zt: (u[c0], u[c1]), the z
+        // momentum negated for a wall (axis_images' rules: periodic wrap,
+        // outflow copy of the first/last cell, wall mirror).  Odd widths and
+        // width 2 take the per-cell path (images()).
+        const bool even_z = ((a.nz - 4) & 1) == 0 && a.nz - 4 >= 4;   // (width 2: both faces on one pair)
+        int zt = -1, zc0 = 0, zc1 = 1;
+        bool zflip = false;
+        if (even_z && val1) {
+            if (z == 2) {
+                if (a.bc[4] == kPeriodic) { zt = a.nz - 2; }
+                else if (a.bc[4] == kOutflow) { zt = 0; zc1 = 0; }
+                else { zt = 0; zc0 = 1; zc1 = 0; zflip = true; }
+            } else if (z + 1 == a.nz - 3) {
+                if (a.bc[5] == kPeriodic) { zt = 0; }
+                else if (a.bc[5] == kOutflow) { zt = a.nz - 2; zc0 = 1; }
+                else { zt = a.nz - 2; zc0 = 1; zc1 = 0; zflip = true; }
+            }
+        }
+        const bool zslow = !even_z && img_z;
+        // the pair (or its first cell) at (x', y', z'), field 1 / 2 negated
+        // for a mirror along x / y
+        auto put = [&](int xq, int yq, const V u[5], bool s0, bool s1, bool fx, bool fy) {
+            const long long o = ((long long)xq * a.ny + yq) * a.pitch + z;
+#pragma unroll
+            for (int f = 0; f < 5; ++f) {
+                V v = u[f];
+                if ((f == 1 && fx) || (f == 2 && fy)) v = vmul(v, spl<V>(-1.0));
+                if (s1) stv(a.dst + f * a.fstride + o, v);
+                else if (s0) a.dst[f * a.fstride + o] = v.x;
+            }
+            if (zt >= 0 && s1) {
+                const long long oz = ((long long)xq * a.ny + yq) * a.pitch + zt;
+#pragma unroll
+                for (int f = 0; f < 5; ++f) {
+                    V v = mk(zc0 ? u[f].y : u[f].x, zc1 ? u[f].y : u[f].x);
+                    if ((f == 1 && fx) || (f == 2 && fy) || (f == 3 && zflip)) v = vmul(v, spl<V>(-1.0));
+                    stv(a.dst + f * a.fstride + oz, v);
+                }
+            }
+        };
+        auto store = [&](int xu, const V u[5], const V &sp, bool on) {
+            const bool s0 = on && val0, s1 = on && val1;
+            if (s0) smax = smax_of(smax, sp.x);
+            if (s1) smax = smax_of(smax, sp.y);
+            put(xu, y, u, s0, s1, false, false);
+            const bool img_x = xu <= 3 || xu >= a.nx - 4;
+            if (on && (img_x || img_y)) {
+                // boundary plane or row: the pair again at every image plane
+                // and row (uniform over the warp)
+                int ximg[4], xflp[4], yimg[4], yflp[4];
+                const int nxi = axis_images(xu, a.nx, a.bc[0], a.bc[1], ximg, xflp);
+                const int nyi = axis_images(y, a.ny, a.bc[2], a.bc[3], yimg, yflp);
+                for (int ix = 0; ix < nxi; ++ix)
+                    for (int iy = 0; iy < nyi; ++iy)
+                        if (ix || iy) put(ximg[ix], yimg[iy], u, s0, s1, xflp[ix] != 0, yflp[iy] != 0);
+            }
+            if (on && zslow) {
+                if (s0) images(a, xu, y, z, u[0].x, u[1].x, u[2].x, u[3].x, u[4].x);
+                if (s1) images(a, xu, y, z + 1, u[0].y, u[1].y, u[2].y, u[3].y, u[4].y);
+            }
+        };
+
         // prologue: planes xs-2, xs-1
         bool ok = wait_plane(s, 0, t.budget);
         if (ok && active) load_prim_pair(slot(s, 0), r + 2, col, k, q);
@@ -398,16 +491,21 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
         fence_proxy_async();
         barrier();
         if (s.abort_flag[t.xs & 1]) return;
+        bool aborted = false;
         for (int m = t.xs - 1; m <= t.xe; ++m) {
             const int l = m - t.xs + 3;
             const int pm = m & 1;
             const bool upd = m >= t.xs && m < t.xe;
-            V sy[5], sz[5], tu[5];
+            V sy[5], sz[5];
             if (!wait_plane(s, l, t.budget)) s.abort_flag[m & 1] = 1;
             if (active) {
-                V qn[5], dn[5], sx[5], xt[5];
+                V qn[5], dn[5], sx[5], xt[5], u[5], sp;
                 load_prim_pair(slot(s, l), r + 2, col, k, qn);
                 store_pb(s, (m + 1) & 1, r + 1, col, qn);
+                // update of plane m-2 (from plane xs on; earlier iterations
+                // compute on a valid slot and store nothing)
+                const bool do_upd = m - 2 >= t.xs;
+                update(m - 2, do_upd ? l - 3 : 0, u, sp);
 #pragma unroll
                 for (int f = 0; f < 5; ++f) dn[f] = vsub(qn[f], q[f]);
                 slopes_adj(s, pm, r + 1, col, q, dq, dn, nullptr, nullptr, sx, sy, sz);
@@ -435,7 +533,9 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
                     half_step(xtp, sxp, 1.0, lo);
                     half_step(xt, sx, -1.0, up);
                     face<1, false>(lo, up, spl<V>(0.0), k, fx);
-                    // lower outflow x face: plane 2 sees no x divergence
+                    // plane m-1 is complete but for its upper y flux and its
+                    // right edge flux (added at its update, two planes on); on
+                    // a lower outflow x face plane 2 sees no x divergence
                     const bool xo_prev = m - 1 == 2 && a.bc[0] == kOutflow;
                     const bool xo = m == 2 && a.bc[0] == kOutflow;
 #pragma unroll
@@ -457,7 +557,7 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
 #pragma unroll
                         for (int f = 0; f < 5; ++f) stv(&s.ytop[pm][f][2 * lane], t.yhi == kOut ? st[f] : xt[f]);
                     }
-                    if (edge && !t.odd) {
+                    if (edge_even) {
                         // the right edge face (warp B) needs the last column's states
 #pragma unroll
                         for (int f = 0; f < 5; ++f) {
@@ -468,80 +568,68 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
                 }
 #pragma unroll
                 for (int f = 0; f < 5; ++f) { q[f] = qn[f]; dq[f] = dn[f]; }
+                store(m - 2, u, sp, do_upd);
             }
             fence_proxy_async();
             barrier();
-            if (s.abort_flag[m & 1]) break;
-            if (!active) continue;
-            // ================= after the barrier =================
-            if (upd) {
-                const V *xt = xtp;
-                V dy[5];
-                if (!yout) {
-                    V lo[5], up[5], fyv[5];
+            if (s.abort_flag[m & 1]) { aborted = true; break; }
+            if (!active || !upd) continue;
+            // ================= after the barrier: y and z faces of plane m
+            const V *xt = xtp;
+            V dy[5];
+            if (!yout) {
+                V lo[5], up[5], fyv[5];
 #pragma unroll
-                    for (int f = 0; f < 5; ++f) lo[f] = ldv(&s.ypl[pm][r][f][2 * lane]);
-                    if (r == 0 && t.ylo == kWallM) {
-                        // wall ghost row: mirrored prediction of this row + its own half slope
+                for (int f = 0; f < 5; ++f) lo[f] = ldv(&s.ypl[pm][r][f][2 * lane]);
+                if (r == 0 && t.ylo == kWallM) {
+                    // wall ghost row: mirrored prediction of this row + its own half slope
 #pragma unroll
-                        for (int f = 0; f < 5; ++f) lo[f] = vadd(lo[f], mirror(xt[f], f == 2));
-                    }
-                    half_step(xt, sy, -1.0, up);
-                    face<2, false>(lo, up, spl<V>(0.0), k, fyv);
-#pragma unroll
-                    for (int f = 0; f < 5; ++f) {
-                        stv(&s.fy[pm][r][f][2 * lane], fyv[f]);
-                        dy[f] = vmul(fyv[f], spl<V>(-1.0));
-                    }
-                } else {
-#pragma unroll
-                    for (int f = 0; f < 5; ++f) dy[f] = spl<V>(0.0);
+                    for (int f = 0; f < 5; ++f) lo[f] = vadd(lo[f], mirror(xt[f], f == 2));
                 }
-                V lo[5], up[5], fzv[5];
+                half_step(xt, sy, -1.0, up);
+                face<2, false>(lo, up, spl<V>(0.0), k, fyv);
 #pragma unroll
                 for (int f = 0; f < 5; ++f) {
-                    const V U = vfma(sz[f], spl<V>(0.5), xt[f]);
-                    const V L = vfma(sz[f], spl<V>(-0.5), xt[f]);
-                    T left = __shfl_up_sync(full, U.y, 1);
-                    if (lane == 0) {
-                        left = s.zl[pm][r][f];
-                        if (t.zlo == kWallM) left += f == 3 ? -xt[f].x : xt[f].x;
-                    }
-                    lo[f] = mk(left, U.x);
-                    up[f] = L;
-                    if (edge && t.odd) {
-                        // the pair's second cell is the right ghost column
-                        T g = s.zr[pm][r][f];
-                        if (t.zhi == kWallM) g += f == 3 ? -xt[f].x : xt[f].x;
-                        if (t.zhi == kOut) g = L.x;
-                        up[f].y = g;
-                    }
+                    stv(&s.fy[pm][r][f][2 * lane], fyv[f]);
+                    dy[f] = vmul(fyv[f], spl<V>(-1.0));
                 }
-                face<3, GRAV>(lo, up, t.gh, k, fzv);
+            } else {
 #pragma unroll
-                for (int f = 0; f < 5; ++f) {
-                    T hi = __shfl_down_sync(full, fzv[f].x, 1);
-                    if (edge && !t.odd) hi = T(0);   // right edge face: added at the update
-                    V dz = vsub(mk(fzv[f].y, hi), fzv[f]);
-                    if (zout) dz.x = T(0);
-                    acc[f] = vadd(acc[f], vadd(dy[f], dz));
-                }
+                for (int f = 0; f < 5; ++f) dy[f] = spl<V>(0.0);
             }
-            if (m - 1 >= t.xs && m - 1 < t.xe) {
-                // update of plane m-1: its upper y flux (row above) and right
-                // edge flux (warp B) arrived with this barrier
-                const int pp = (m - 1) & 1;
-                V u[5];
-                T *sl = slot(s, l - 2);
+            V lo[5], up[5], fzv[5];
 #pragma unroll
-                for (int f = 0; f < 5; ++f) {
-                    V tt = tu[f];
-                    if (!yout) tt = vadd(tt, ldv(&s.fy[pp][r + 1][f][2 * lane]));
-                    if (edge && !t.odd) tt.y += s.fz[pp][r][f];
-                    u[f] = vfma(spl<V>(k.sc[f]), tt, ldv(&C(sl, f, r + 2, col)));
-                }
-                epilogue(a, k, m - 1, y, z, u, val0, val1, smax);
+            for (int f = 0; f < 5; ++f) {
+                const V U = vfma(sz[f], spl<V>(0.5), xt[f]);
+                const V L = vfma(sz[f], spl<V>(-0.5), xt[f]);
+                // the halo columns' states (broadcast loads, used by lane 0
+                // and, for an odd width, by the edge lane)
+                const T mx = f == 3 ? -xt[f].x : xt[f].x;   // wall mirror of the pair's first cell
+                T zlv = s.zl[pm][r][f];
+                if (t.zlo == kWallM) zlv += mx;
+                T zrv = s.zr[pm][r][f];
+                if (t.zhi == kWallM) zrv += mx;
+                if (t.zhi == kOut) zrv = L.x;
+                const T left = __shfl_up_sync(full, U.y, 1);
+                lo[f] = mk(lane == 0 ? zlv : left, U.x);
+                // odd width: the edge lane's second cell is the right ghost column
+                up[f] = mk(L.x, edge && t.odd ? zrv : L.y);
             }
+            face<3, GRAV>(lo, up, t.gh, k, fzv);
+#pragma unroll
+            for (int f = 0; f < 5; ++f) {
+                T hi = __shfl_down_sync(full, fzv[f].x, 1);
+                if (edge_even) hi = T(0);   // right edge face: added at the update
+                V dz = vsub(mk(fzv[f].y, hi), fzv[f]);
+                if (zout) dz.x = T(0);
+                acc[f] = vadd(acc[f], vadd(dy[f], dz));
+            }
+        }
+        // the last plane of the chunk: its fluxes arrived with the last barrier
+        if (!aborted && active && t.xe - 1 >= t.xs) {
+            V u[5], sp;
+            update(t.xe - 1, t.xe - t.xs + 1, u, sp);
+            store(t.xe - 1, u, sp, true);
         }
     }
 
@@ -659,13 +747,17 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
             fence_proxy_async();
             barrier();
             if (s.abort_flag[m & 1]) break;
-            // the slot of plane m-2 is free: stage plane m-2+R
+            // from plane xs on, the barrier frees the slot of plane m-2
+            // (staged index m - xs): stage plane m-2+R there (the first R
+            // planes were staged before the march)
             const int nl = m - t.xs + R;
-            if (lane == 0 && nl < t.np) {
-                mbar_expect_tx(&s.bar[nl % R], Sm::kBoxBytes);
-                tma_load_4d(slot(s, nl), tmap, t.z0 - 2, t.y0 - 2, t.xs - 2 + nl, 0, &s.bar[nl % R]);
+            if (m >= t.xs && nl < t.np) {
+                if (lane == 0) {
+                    mbar_expect_tx(&s.bar[nl % R], Sm::kBoxBytes);
+                    tma_load_4d(slot(s, nl), tmap, t.z0 - 2, t.y0 - 2, t.xs - 2 + nl, 0, &s.bar[nl % R]);
+                }
+                issued = nl + 1;
             }
-            if (nl < t.np) issued = nl + 1;
         }
         return issued;
     }
@@ -866,10 +958,13 @@ template <class T, int TY, int R> constexpr int smem_bytes() {
     return (int)sizeof(Smem<T, TY, R>) + 1024;
 }
 
-// Registers per thread: the whole register file for one block of 32 (TY+2)
-// threads, in the allocation granule of 8 (FP32: 144 for 448 threads).
+// Registers per thread: a block's warps are spread over the SM's four
+// sub-partitions, each with 16384 registers, so the busiest one (ceil(W/4)
+// warps) bounds them; in the allocation granule of 8, at most 255.
 template <int TY> constexpr int sweep_max_regs() {
-    return (65536 / (32 * (TY + 2))) / 8 * 8 > 255 ? 255 : (65536 / (32 * (TY + 2))) / 8 * 8;
+    constexpr int per_sub = (TY + 2 + 3) / 4;
+    constexpr int r = 16384 / (32 * per_sub) / 8 * 8;
+    return r > 255 ? 255 : r;
 }
 
 template <class T, int TY, int R, int LIM, bool GRAV>

@@ -141,7 +141,9 @@ def load(path: os.PathLike | None = None):
     global _lib
     if _lib is not None:
         return _lib
-    p = Path(path) if path else LIB_PATH
+    # DEEPGREEN_LIB names another build of the library (e.g. one compiled
+    # with different tile sizes); the default is the in-tree build
+    p = Path(path) if path else Path(os.environ.get("DEEPGREEN_LIB", LIB_PATH))
     if not p.exists():
         raise FileNotFoundError(f"{p} not built; run `make -C {PKG_ROOT}` (no CPU fallback exists)")
     lib = ctypes.CDLL(str(p))

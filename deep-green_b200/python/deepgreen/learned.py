@@ -180,6 +180,80 @@ def initial_state(kind: str, n: int, seed: int, **kw):
     raise ValueError(kind)
 
 
+def device_initial_conserved(kind: str, n: int, seed: int, device: int = 0, **kw):
+    """initial_state's fields built on the GPU and returned as the five
+    conserved totals (mass, momenta, energy; FP32 CUDA tensors of the ghosted
+    shape) for dg_set_conserved_device: the large grids of the evaluation
+    (1024^3: 43 GB of FP64 primitives) never pass through host memory.  The
+    primitives are the same functions of the cell centres as initial_state's
+    (KH noise by the same counter-based generator); they are converted to
+    totals in FP64 (calc_conserved, physics.rs:143-175) and rounded once."""
+    import torch
+    dev = torch.device("cuda", device)
+    f64 = torch.float64
+    ds = 1.0 / n
+    m = n + 4
+    c = (torch.arange(m, dtype=f64, device=dev) - 2 + 0.5) * ds
+    meta = {"kind": kind, "seed": seed}
+    if kind == "kh":
+        rng = np.random.default_rng(seed)
+        shear = kw.get("shear", rng.uniform(0.2, 0.8))
+        ratio = kw.get("ratio", rng.uniform(1.0, 4.0))
+        meta.update(shear=float(shear), ratio=float(ratio))
+        y = c.view(1, m, 1)
+        inner = (torch.abs(y - 0.5) < 0.25).expand(m, m, m)
+        rho = torch.where(inner, float(ratio), 1.0).to(f64)
+        vel = [torch.where(inner, float(shear), -float(shear)).to(f64),
+               (0.01 * torch.sin(4 * np.pi * c.view(m, 1, 1))
+                * (torch.exp(-(y - 0.25) ** 2 / 0.005) + torch.exp(-(y - 0.75) ** 2 / 0.005))).expand(m, m, m)
+               .contiguous(),
+               torch.zeros((m, m, m), dtype=f64, device=dev)]
+        # the noise of setups.kelvin_helmholtz, indexed by interior cell
+        ii = (torch.arange(m, device=dev) - 2).remainder(n).view(-1, 1, 1)
+        jj = (torch.arange(m, device=dev) - 2).remainder(n).view(1, -1, 1)
+        kk = (torch.arange(m, device=dev) - 2).remainder(n).view(1, 1, -1)
+        idx = ((ii * n + jj) * n + kk).to(torch.int64)
+        for comp in range(3):
+            vel[comp] = vel[comp] + 1e-3 * (2.0 * setups._counter_uniform_t(seed, idx, comp) - 1.0)
+        del idx
+        p = torch.full((m, m, m), 2.5, dtype=f64, device=dev)
+    elif kind == "fourier":
+        rng = np.random.default_rng(seed)
+        rho = torch.ones((m, m, m), dtype=f64, device=dev)
+        p = torch.ones((m, m, m), dtype=f64, device=dev)
+        vel = [torch.zeros((m, m, m), dtype=f64, device=dev) for _ in range(3)]
+        cn = c.cpu().numpy()
+        for _ in range(8):
+            k = np.zeros(3, dtype=np.int64)
+            while not k.any():
+                k = rng.integers(-4, 5, 3)
+            phase = rng.uniform(0.0, 2.0 * np.pi)
+            a = rng.uniform(-0.1, 0.1, 5)
+            exy = np.exp(1j * (2 * np.pi * k[0] * cn + phase))[:, None] * np.exp(1j * 2 * np.pi * k[1] * cn)[None, :]
+            ez = np.exp(1j * 2 * np.pi * k[2] * cn)
+            xr = torch.from_numpy(np.ascontiguousarray(exy.real)).to(dev)[:, :, None]
+            xi = torch.from_numpy(np.ascontiguousarray(exy.imag)).to(dev)[:, :, None]
+            zr = torch.from_numpy(np.ascontiguousarray(ez.real)).to(dev)[None, None, :]
+            zi = torch.from_numpy(np.ascontiguousarray(ez.imag)).to(dev)[None, None, :]
+            sn = xr * zi + xi * zr
+            rho += float(a[0]) * sn
+            p += float(a[1]) * sn
+            for comp in range(3):
+                vel[comp] += float(a[2 + comp]) * sn
+            del sn
+    else:
+        raise ValueError(kind)
+    vol = ds ** 3
+    cons = [(rho * vol).to(torch.float32)]
+    ke = torch.zeros_like(rho)
+    for v in vel:
+        cons.append((rho * v * vol).to(torch.float32))
+        ke += v * v
+    cons.append((vol * (0.5 * rho * ke + p / (GAMMA - 1.0))).to(torch.float32))
+    del rho, vel, p, ke
+    return [t.contiguous() for t in cons], meta
+
+
 # ---------------------------------------------------------------------------
 # Pairs
 # ---------------------------------------------------------------------------

@@ -258,8 +258,8 @@ int32_t dg_batch_enqueue(dg_batch *b, int32_t nsteps);
 int32_t dg_batch_get_dts(dg_batch *b, int32_t i, int32_t nsteps, double *dts);
 /* grid i's conserved state, ghosts filled, as dg_get_conserved */
 int32_t dg_batch_get_conserved(dg_batch *b, int32_t i, void *const cons[5]);
-/* tile rows (12, the production kernel's tile) and x-planes per work item
- * (0 = automatic) */
+/* tile rows (the production kernel's tile rows, as dg_batch_get_tiling
+ * reports them) and x-planes per work item (0 = automatic) */
 int32_t dg_batch_set_tiling(dg_batch *b, int32_t tile_rows, int32_t chunk);
 int32_t dg_batch_get_tiling(dg_batch *b, int32_t *tile_rows, int32_t *chunk, int32_t *items);
 /* times `steps` steps of each candidate tiling on the live batch, keeps the
