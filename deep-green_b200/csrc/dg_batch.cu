@@ -107,7 +107,7 @@ GridArgs<float> args_of(const dg_batch *b, int i, int parity) {
     a.nz = s.nz;
     a.pitch = s.pitch;
     a.fstride = s.fstride;
-    for (int f = 0; f < 6; ++f) a.bc[f] = s.info.bcs[f];
+    set_boundaries(a, s.info.bcs);
     a.gravity = s.info.gravity;
     a.limiter = s.info.limiter;
     a.nparts = s.nitems;
@@ -314,7 +314,7 @@ int32_t dg_batch_create(int32_t n, const dg_sim_info *infos, dg_batch **out) {
             return bfail(nullptr, DG_ERR_INVALID, "bad limiter");
         for (int a = 0; a < 3; ++a) {
             const int lo = f.bcs[2 * a], hi = f.bcs[2 * a + 1];
-            if (lo < 0 || lo > 2 || hi < 0 || hi > 2 || (lo == DG_BC_PERIODIC) != (hi == DG_BC_PERIODIC))
+            if (!valid_bc_pair(lo, hi))
                 return bfail(nullptr, DG_ERR_INVALID, "grid " + std::to_string(i) + ": bad boundary types");
         }
     }

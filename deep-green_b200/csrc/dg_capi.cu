@@ -242,9 +242,9 @@ int32_t dg_create(const dg_sim_info *info, dg_ctx **out) {
         info->rounding != DG_ROUNDING_FAST) { set_err("unknown rounding policy"); return DG_ERR_INVALID; }
     for (int a = 0; a < 3; ++a) {
         const int lo = info->bcs[2 * a], hi = info->bcs[2 * a + 1];
-        if (lo < 0 || lo > 2 || hi < 0 || hi > 2) { set_err("unknown boundary type"); return DG_ERR_INVALID; }
+        if (lo < 0 || lo > DG_BC_CONDUCTING_WALL || hi < 0 || hi > DG_BC_CONDUCTING_WALL) { set_err("unknown boundary type"); return DG_ERR_INVALID; }
         // Simulation::new (grid.rs:55-63) pairs periodic faces
-        if ((lo == DG_BC_PERIODIC) != (hi == DG_BC_PERIODIC)) { set_err("periodic faces must come in pairs"); return DG_ERR_INVALID; }
+        if (!valid_bc_pair(lo, hi)) { set_err("periodic faces must come in pairs"); return DG_ERR_INVALID; }
     }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || info->device < 0 || info->device >= ndev) {

@@ -56,7 +56,7 @@ template <class T> inline GridArgs<T> grid_args(const dg_ctx *c, const void *src
     a.nz = c->nz;
     a.pitch = c->pitch;
     a.fstride = c->fstride;
-    for (int i = 0; i < 6; ++i) a.bc[i] = c->info.bcs[i];
+    set_boundaries(a, c->info.bcs);
     a.gravity = c->info.gravity;
     a.limiter = c->info.limiter;
     a.nparts = 0;

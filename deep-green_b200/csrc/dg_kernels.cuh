@@ -47,7 +47,8 @@ template <class T> struct GridArgs {
     int nx, ny, nz;            // ghosted extents (interior + 4)
     int pitch;                 // elements between consecutive z-rows
     long long fstride;         // elements between fields
-    int bc[6];
+    int bc[6];                 // Bc per face (x-, x+, y-, y+, z-, z+)
+    int heat;                  // bit a: the lower face of axis a is a conducting wall
     int gravity;
     int limiter;               // 0 central slopes, 1 minmod
     int nparts;                // work items of this grid in a batched launch
@@ -56,6 +57,27 @@ template <class T> struct GridArgs {
     DevCtl *ctl;
     Partial *part;
 };
+
+// Boundary types of dg_sim_info (DG_BC_*) into the kernels' form.  A
+// conducting wall (DG_BC_CONDUCTING_WALL = 3, the reference CUDA variant's
+// BC::CONDUCTING_WALL) follows the wall rule for every ghost (kernels.h:327)
+// and adds a heat source to the energy flux of its face.  The reference adds
+// it at the flux of lower-cell index 1 for a lower face and n - 2 for an
+// upper face (kernels.h:561-661): only the lower face's reaches an interior
+// cell, so only lower faces set a heat bit.
+constexpr int kBcConductingWall = 3;
+inline bool valid_bc_pair(int lo, int hi) {
+    return lo >= 0 && lo <= kBcConductingWall && hi >= 0 && hi <= kBcConductingWall &&
+           (lo == kPeriodic) == (hi == kPeriodic);
+}
+template <class T> inline void set_boundaries(GridArgs<T> &a, const int32_t bcs[6]) {
+    a.heat = 0;
+    for (int f = 0; f < 6; ++f) {
+        const bool cond = bcs[f] == kBcConductingWall;
+        a.bc[f] = cond ? (int)kWall : (int)bcs[f];
+        if (cond && (f & 1) == 0) a.heat |= 1 << (f / 2);
+    }
+}
 
 // SMs of a B200 (2 dies x 74); grid sizes below are multiples of it
 constexpr int kSms = 148;

@@ -90,7 +90,7 @@ GridArgs<T> args_for(const dg_sim_info *info, const void *src, void *dst, void *
     a.nz = info->nz + 4;
     a.pitch = a.nz;
     a.fstride = (long long)a.nx * a.ny * a.nz;
-    for (int i = 0; i < 6; ++i) a.bc[i] = info->bcs[i];
+    set_boundaries(a, info->bcs);
     a.gravity = info->gravity;
     a.limiter = info->limiter;
     a.nparts = 0;
@@ -197,8 +197,7 @@ extern "C" int32_t dg_compute_step_noalloc(const dg_sim_info *info, void *cons_i
         return fail(DG_ERR_INVALID, "bad rounding policy");
     for (int ax = 0; ax < 3; ++ax) {
         const int lo = info->bcs[2 * ax], hi = info->bcs[2 * ax + 1];
-        if (lo < 0 || lo > 2 || hi < 0 || hi > 2 || (lo == DG_BC_PERIODIC) != (hi == DG_BC_PERIODIC))
-            return fail(DG_ERR_INVALID, "bad boundary types (periodic faces come in pairs)");
+        if (!valid_bc_pair(lo, hi)) return fail(DG_ERR_INVALID, "bad boundary types (periodic faces come in pairs)");
     }
     const int elem = info->precision == DG_F64 ? 8 : 4;
     if (((size_t)(info->nz + 4) * elem) % 16 != 0)

@@ -10,11 +10,10 @@
 //                   rounds exactly like the reference's scalar code, so the
 //                   GPU result equals the CPU restatement bit for bit.  Used
 //                   for FP64 and, on request, for FP32.
-//   Phys<T, false>  "fast": one reciprocal per state instead of several
-//                   divides, the ds and dt factors folded into one update
-//                   scale, fused multiply-adds.  Differs from the reference's
-//                   rounding at the level of the unit roundoff.  The FP32
-//                   production path.
+//   Phys<T, false>  "fast": the conversion of a state to primitives with one
+//                   reciprocal and fused multiply-adds, as the fused-arithmetic
+//                   sweep kernel (dg_sweep_impl.cuh) computes it; used by the
+//                   reductions and conversions that must agree with it.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -22,7 +21,25 @@
 
 namespace dg {
 
+// Boundary types in the kernels (DG_BC_*): a conducting wall (DG_BC_CONDUCTING_WALL)
+// reaches them as kWall plus a heat-source flag (GridArgs::heat).
 enum Bc : int { kPeriodic = 0, kOutflow = 1, kWall = 2 };
+
+// Conducting-wall heat per unit volume, Q / V, of the reference's CUDA flux
+// kernel (src/cu/include/kernels.h:561-575) in its operation order, with its
+// constants (constants.h:63-66: RS = 287, T_OUT_KELVIN = 273, VOUT_MS = 0;
+// wall thickness d = 0.008 and conductivity kappa = 0.2 as float literals)
+// and t_in = p / (RS rho) of the face's lower cell (its extrapolated state).
+template <class T> __host__ __device__ __forceinline__ T wall_heat(T rho, T p, T ds) {
+    const T rs = T(287.0f), t_out = T(273.0f), vout = T(0.0f);
+    const T t_in = p / (rs * rho);
+    const T hc_out = T(10.0f) - vout + T(10.0f) * sqrt(vout);
+    const T S = ds * ds;
+    const T V = ds * ds * ds;
+    const T d = T(0.008f), kappa = T(0.2f);
+    const T Q = (t_out - t_in) * (S / ((d / kappa) + (T(1.0f) / hc_out)));
+    return Q / V;
+}
 
 // Runtime constants of one grid, derived once on the host in precision T.
 template <class T> struct Consts {
@@ -40,8 +57,22 @@ template <class T> struct Consts {
     T g;         // gravity acceleration (globals.rs:7)
 };
 
+// The fast policy's FP32 reciprocal and reciprocal square root: the
+// hardware approximations without the subnormal range handling (the states
+// never reach subnormal densities or pressures), one instruction each.
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float rsqrt_approx(float x) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 template <class T> __device__ __forceinline__ T fast_rcp(T x);
-template <> __device__ __forceinline__ float fast_rcp<float>(float x) { return __fdividef(1.0f, x); }
+template <> __device__ __forceinline__ float fast_rcp<float>(float x) { return rcp_approx(x); }
 template <> __device__ __forceinline__ double fast_rcp<double>(double x) { return 1.0 / x; }
 
 // minmod slope limiter (an addition of this library; the reference uses
@@ -64,15 +95,15 @@ __device__ __forceinline__ float max_nan(float a, float b) {
 
 // Fast-policy wave speed c_s + |v| of one primitive state (the quantity
 // whose maximum sets dt, physics.rs:186-190): sqrt(gamma p / rho) as
-// g*rsqrt(g*rho) with g = gamma p, |v| as v2*rsqrt(v2).  The fast kernels
+// g*rsqrt(g*rho) with g = gamma p, |v| as v2*rsqrt(v2) (rsqrt_approx).  The fast kernels
 // take dt = CFL * ds / max(speed), the same minimum as CFL * min(ds/speed)
 // without a divide per cell.  Explicit _rn operations: every kernel that
 // calls this rounds the same way.
 __device__ __forceinline__ float fast_speed(float rho, float vx, float vy, float vz, float p, float gamma) {
     const float g = __fmul_rn(gamma, p);
-    const float cs = __fmul_rn(g, rsqrtf(__fmul_rn(g, rho)));
+    const float cs = __fmul_rn(g, rsqrt_approx(__fmul_rn(g, rho)));
     const float v2 = __fmaf_rn(vz, vz, __fmaf_rn(vy, vy, __fmul_rn(vx, vx)));
-    const float vm = __fmul_rn(v2, rsqrtf(fmaxf(v2, 1e-30f)));
+    const float vm = __fmul_rn(v2, rsqrt_approx(fmaxf(v2, 1e-30f)));
     return __fadd_rn(cs, vm);
 }
 
@@ -123,8 +154,11 @@ template <class T> struct Phys<T, true> {
     // the upper cell (xu, gu).  n = 1, 2, 3: index of the normal velocity.
     // The result includes the final *ds (physics.rs:401-405).  klow: z index
     // of the lower cell, for the gravity term (z faces only, grav != 0).
+    // heat: the face is the first face of a lower conducting wall; its
+    // energy flux takes Q / V after the advective part (kernels.h:561-575).
     static __device__ __forceinline__ void face(const T xl[5], const T gl[5], const T xu[5], const T gu[5], int n,
-                                                int grav, int klow, int nz, const Consts<T> &k, T F[5]) {
+                                                int grav, int klow, int nz, const Consts<T> &k, T F[5],
+                                                bool heat = false) {
         const int t1 = n == 1 ? 2 : 1, t2 = n == 3 ? 2 : 3;
         const T half = k.half_ds;
         const T rl = xu[0] - gu[0] * half;
@@ -150,6 +184,7 @@ template <class T> struct Phys<T, true> {
         T f2 = mx * my / rho_star;
         T f3 = mx * mz / rho_star;
         T f4 = (en_star + p_star) * (mx / rho_star);
+        if (heat) f4 += wall_heat(xl[0], xl[4], k.ds);
         if (grav) {
             const T h = (T(nz) - T(2.0) * T(2)) * k.ds - (T(klow) - T(2.0)) * k.ds;
             f1 += T(1.0) * rho_star * k.g * h;
@@ -181,8 +216,9 @@ template <class T> struct Phys<T, true> {
 // Fast
 // ---------------------------------------------------------------------------
 template <class T> struct Phys<T, false> {
-    // Same operation sequence as the packed FP32 step kernel's epilogue
-    // (dg_fast_impl.cuh), so dt agrees bit for bit between the two.
+    // Same operation sequence as the sweep kernel's conversion of the
+    // updated state (dg_sweep_impl.cuh prim), so dt agrees bit for bit
+    // between the state reduction and the step's fused reduction.
     static __device__ __forceinline__ void prim(const T u[5], T w[5], const Consts<T> &k) {
         const T ir = fast_rcp(u[0]);   // 1 / (rho V)
         const T rho = u[0] * k.inv_vol;
@@ -193,67 +229,6 @@ template <class T> struct Phys<T, false> {
         w[2] = vy;
         w[3] = vz;
         w[4] = fma(T(-0.5) * rho, v2, u[4] * k.inv_vol) * k.gm1;
-    }
-
-    template <int LIM> static __device__ __forceinline__ T slope(T qm, T q0, T qp, const Consts<T> &k) {
-        if (LIM == 0) return (qp - qm) * k.inv_2ds;
-        return minmod((q0 - qm) * k.inv_ds, (qp - q0) * k.inv_ds);
-    }
-
-    static __device__ __forceinline__ void predict(const T w[5], const T gx[5], const T gy[5], const T gz[5], T dt,
-                                                   const Consts<T> &k, T out[5]) {
-        const T rho = w[0], vx = w[1], vy = w[2], vz = w[3], p = w[4];
-        const T h = T(0.5) * dt;
-        const T ir = fast_rcp(rho);
-        const T div = gx[1] + gy[2] + gz[3];
-        out[0] = rho - h * (vx * gx[0] + vy * gy[0] + vz * gz[0] + rho * div);
-        out[1] = vx - h * (vx * gx[1] + vy * gy[1] + vz * gz[1] + ir * gx[4]);
-        out[2] = vy - h * (vx * gx[2] + vy * gy[2] + vz * gz[2] + ir * gy[4]);
-        out[3] = vz - h * (vx * gx[3] + vy * gy[3] + vz * gz[3] + ir * gz[4]);
-        out[4] = p - h * (k.gamma * p * div + vx * gx[4] + vy * gy[4] + vz * gz[4]);
-    }
-
-    // Same flux as the reference policy, re-associated; WITHOUT the final
-    // *ds (folded into the update scale dt*ds*ds).
-    static __device__ __forceinline__ void face(const T xl[5], const T gl[5], const T xu[5], const T gu[5], int n,
-                                                int grav, int klow, int nz, const Consts<T> &k, T F[5]) {
-        const int t1 = n == 1 ? 2 : 1, t2 = n == 3 ? 2 : 3;
-        const T half = k.half_ds;
-        // a: lower side of the face, b: upper side
-        const T ra = xl[0] + gl[0] * half, rb = xu[0] - gu[0] * half;
-        const T ua = xl[n] + gl[n] * half, ub = xu[n] - gu[n] * half;
-        const T va = xl[t1] + gl[t1] * half, vb = xu[t1] - gu[t1] * half;
-        const T wa = xl[t2] + gl[t2] * half, wb = xu[t2] - gu[t2] * half;
-        const T pa = xl[4] + gl[4] * half, pb = xu[4] - gu[4] * half;
-        const T ea = T(0.5) * ra * (ua * ua + va * va + wa * wa) + pa * k.inv_gm1;
-        const T eb = T(0.5) * rb * (ub * ub + vb * vb + wb * wb) + pb * k.inv_gm1;
-        const T mua = ra * ua, mva = ra * va, mwa = ra * wa;
-        const T mub = rb * ub, mvb = rb * vb, mwb = rb * wb;
-        const T rs = T(0.5) * (ra + rb);
-        const T mu = T(0.5) * (mua + mub), mv = T(0.5) * (mva + mvb), mw = T(0.5) * (mwa + mwb);
-        const T es = T(0.5) * (ea + eb);
-        const T irs = fast_rcp(rs);
-        const T us = mu * irs;
-        const T ps = k.gm1 * (es - T(0.5) * (mu * mu + mv * mv + mw * mw) * irs);
-        const T ca = sqrt(k.gamma * pa * fast_rcp(ra)) + fabs(ua);
-        const T cb = sqrt(k.gamma * pb * fast_rcp(rb)) + fabs(ub);
-        const T hc = T(0.5) * fmax(ca, cb);
-        T fu = mu * us + ps, fe = (es + ps) * us;
-        if (grav) {
-            const T gh = k.g * (T(nz - 4) * k.ds - T(klow - 2) * k.ds);
-            fu += rs * gh;
-            fe += T(0.5) * rs * (ua + ub) * gh;
-        }
-        F[0] = mu - hc * (rb - ra);
-        F[n] = fu - hc * (mub - mua);
-        F[t1] = mv * us - hc * (mvb - mva);
-        F[t2] = mw * us - hc * (mwb - mwa);
-        F[4] = fe - hc * (eb - ea);
-    }
-
-    static __device__ __forceinline__ T update(T u, T fxh, T fxl, T fyh, T fyl, T fzh, T fzl, T dt,
-                                               const Consts<T> &k) {
-        return u - (dt * k.ds * k.ds) * ((fxh - fxl) + (fyh - fyl) + (fzh - fzl));
     }
 };
 

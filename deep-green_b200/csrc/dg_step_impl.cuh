@@ -133,8 +133,9 @@ struct StepKernel {
         }
     }
 
-    // y-face flux between rectangle cells (sy-1, sz) [lower] and (sy, sz).
-    static __device__ __forceinline__ void yface(S &s, int sy, int sz, const Consts<T> &k, T F[5]) {
+    // y-face flux between rectangle cells (sy-1, sz) [lower] and (sy, sz);
+    // heat: the face of a lower conducting wall.
+    static __device__ __forceinline__ void yface(S &s, int sy, int sz, const Consts<T> &k, T F[5], bool heat) {
         T xl[5], gl[5], xu[5], gu[5];
         const int rl = ridx(sy - 1, sz), ru = ridx(sy, sz);
 #pragma unroll
@@ -144,7 +145,7 @@ struct StepKernel {
             xu[f] = s.xt[f * S::kRect + ru];
             gu[f] = s.gy[f * S::kRect + ru];
         }
-        Ph::face(xl, gl, xu, gu, 2, 0, 0, 0, k, F);
+        Ph::face(xl, gl, xu, gu, 2, 0, 0, 0, k, F, heat);
     }
 
     // z-face flux between rectangle cells (sy, sz-1) and (sy, sz); klow is
@@ -159,7 +160,7 @@ struct StepKernel {
             xu[f] = s.xt[f * S::kRect + ru];
             gu[f] = s.gz[f * S::kRect + ru];
         }
-        Ph::face(xl, gl, xu, gu, 3, a.gravity, klow, a.nz, a.k, F);
+        Ph::face(xl, gl, xu, gu, 3, a.gravity, klow, a.nz, a.k, F, klow == 1 && (a.heat & 4));
     }
 
     static __device__ void run(const GridArgs<T> &a, const CUtensorMap *tmap, int chunk, unsigned char *raw) {
@@ -302,7 +303,7 @@ struct StepKernel {
                         xt_cur[1] = -xt_cur[1];
                     }
                 }
-                Ph::face(xt_prev, gx_prev, xt_cur, gx_cur, 1, 0, 0, 0, k, fx_hi);
+                Ph::face(xt_prev, gx_prev, xt_cur, gx_cur, 1, 0, 0, 0, k, fx_hi, m == 2 && (a.heat & 1));
             }
             __syncthreads();               // S2: predicted rectangle ready; slot of plane m-1 free
 
@@ -320,14 +321,14 @@ struct StepKernel {
             if (plane_upd) {
                 T *fyb = s.fy[m & 1], *fzb = s.fz[m & 1];
                 T F[5];
-                yface(s, ly + 1, lz + 1, k, F);
+                yface(s, ly + 1, lz + 1, k, F, y0 + ly == 2 && (a.heat & 2));
 #pragma unroll
                 for (int f = 0; f < 5; ++f) fyb[(f * (TY + 1) + ly) * kTZ + lz] = F[f];
                 zface(s, ly + 1, lz + 1, a, gzo - 1, F);
 #pragma unroll
                 for (int f = 0; f < 5; ++f) fzb[(f * TY + ly) * (kTZ + 1) + lz] = F[f];
                 if (ly == 0) {
-                    yface(s, TY + 1, lz + 1, k, F);
+                    yface(s, TY + 1, lz + 1, k, F, false);
 #pragma unroll
                     for (int f = 0; f < 5; ++f) fyb[(f * (TY + 1) + TY) * kTZ + lz] = F[f];
                 } else if (ly == 1 && lz < TY) {

@@ -85,9 +85,9 @@ __device__ __forceinline__ float2 mk(float a, float b) { return make_float2(a, b
 __device__ __forceinline__ double2 mk(double a, double b) { return make_double2(a, b); }
 
 // 1/x of both cells: the fast policy's reciprocal (Phys<T, false>::prim).
-__device__ __forceinline__ float2 vrcp(float2 a) { return make_float2(__fdividef(1.0f, a.x), __fdividef(1.0f, a.y)); }
+__device__ __forceinline__ float2 vrcp(float2 a) { return make_float2(rcp_approx(a.x), rcp_approx(a.y)); }
 __device__ __forceinline__ double2 vrcp(double2 a) { return make_double2(1.0 / a.x, 1.0 / a.y); }
-__device__ __forceinline__ float2 vrsq(float2 a) { return make_float2(rsqrtf(a.x), rsqrtf(a.y)); }
+__device__ __forceinline__ float2 vrsq(float2 a) { return make_float2(rsqrt_approx(a.x), rsqrt_approx(a.y)); }
 __device__ __forceinline__ double2 vrsq(double2 a) { return make_double2(rsqrt(a.x), rsqrt(a.y)); }
 __device__ __forceinline__ float2 vmax(float2 a, float2 b) { return make_float2(fmaxf(a.x, b.x), fmaxf(a.y, b.y)); }
 __device__ __forceinline__ double2 vmax(double2 a, double2 b) { return make_double2(fmax(a.x, b.x), fmax(a.y, b.y)); }
@@ -122,9 +122,19 @@ template <int LIM, class S> __device__ __forceinline__ S slope1(S dm, S dp) {
 
 // Per-grid constants of the kernel in the pair type.
 template <class T> struct K {
-    T inv_vol, gamma, gm1, kp, c1, sg, hd;
+    T inv_vol, gamma, gm1, kp, c1, sg;
+    T iv_h;    // inv_vol / 2
+    T nh4;     // -4 hd, hd = dt / (2 ds): the predictor's factor on products of halves
     T sc[5];   // update scale per field: -dt ds^2 / 2 (mass, momenta), / 4 (energy)
+    T hq4;     // conducting wall: 4 Q/V per kelvin of (273 - t_in), the energy flux's scale
 };
+
+// Conducting-wall heat of one cell in the energy flux's scale (4 Q/V,
+// wall_heat's formula with its constant factor folded into k.hq4); xr, xp:
+// rho/2 and p/2 of the face's lower cell, whose quotient is t_in * RS.
+template <class T> __device__ __forceinline__ T heat4(T xr, T xp, const K<T> &k) {
+    return (T(273.0f) - xp / (T(287.0f) * xr)) * k.hq4;
+}
 
 // Conserved totals -> primitives (calc_primitives, physics.rs:112-140), the
 // fast policy's operation sequence (the same as Phys<T, false>::prim, so the
@@ -141,21 +151,43 @@ template <class V, class T> __device__ __forceinline__ void prim(const V u[5], V
     w[4] = vmul(vfma(vmul(spl<V>(-0.5), rho), v2, vmul(u[4], spl<V>(k.inv_vol))), spl<V>(k.gm1));
 }
 
-// Half-step predictor (extrapolate_primitives_t, physics.rs:251-278) with
-// cell-unit slopes; hd = dt / (2 ds).
+// Half primitives: the march works on q/2 (and hence on half slopes s/2 from
+// their differences), so that the face states xt -+ s/2 are plain sums.
+// Every quantity is the full one scaled by a power of two, and the
+// predictor below scales back exactly: results equal those of the full-size
+// formulas bit for bit.  prim_half is prim's operation sequence on halves:
+// 1/(2M), rho/2, v/2, |v|^2/4 and p/2 = (E/(2V) - 2 (rho/2)|v|^2/4)(gamma-1).
+template <class V, class T> __device__ __forceinline__ void prim_half(const V u[5], V w[5], const K<T> &k) {
+    const V irh = vrcp(vadd(u[0], u[0]));
+    const V rho = vmul(u[0], spl<V>(k.iv_h));
+    const V vx = vmul(u[1], irh), vy = vmul(u[2], irh), vz = vmul(u[3], irh);
+    const V v2 = vfma(vz, vz, vfma(vy, vy, vmul(vx, vx)));
+    w[0] = rho;
+    w[1] = vx;
+    w[2] = vy;
+    w[3] = vz;
+    const V t = vfma(vadd(rho, rho), v2, vmul(u[4], spl<V>(-(double)k.iv_h)));
+    w[4] = vmul(t, spl<V>(-(double)k.gm1));
+}
+
+// Half-step predictor (extrapolate_primitives_t, physics.rs:251-278) on half
+// primitives qh and half slopes (cell units): returns the full predicted
+// state.  Every product of two halves is a quarter of the full product, so
+// the sums are quarters and the factor is -4 hd (hd = dt / (2 ds)).
 template <class V, class T>
-__device__ __forceinline__ void predict(const V w[5], const V sx[5], const V sy[5], const V sz[5], const K<T> &k,
+__device__ __forceinline__ void predict(const V qh[5], const V sx[5], const V sy[5], const V sz[5], const K<T> &k,
                                         V out[5]) {
-    const V rho = w[0], vx = w[1], vy = w[2], vz = w[3], p = w[4];
-    const V nh = spl<V>(-(double)k.hd);
-    const V ir = vrcp(rho);
+    const V rho = vadd(qh[0], qh[0]), vx = vadd(qh[1], qh[1]), vy = vadd(qh[2], qh[2]);
+    const V vz = vadd(qh[3], qh[3]), p = vadd(qh[4], qh[4]);
+    const V nh = spl<V>(k.nh4);
+    const V ir = vrcp(vadd(rho, rho));   // 1 / (4 rho_h)
     const V div = vadd(vadd(sx[1], sy[2]), sz[3]);
-    out[0] = vfma(nh, vfma(rho, div, vfma(vz, sz[0], vfma(vy, sy[0], vmul(vx, sx[0])))), rho);
-    out[1] = vfma(nh, vfma(ir, sx[4], vfma(vz, sz[1], vfma(vy, sy[1], vmul(vx, sx[1])))), vx);
-    out[2] = vfma(nh, vfma(ir, sy[4], vfma(vz, sz[2], vfma(vy, sy[2], vmul(vx, sx[2])))), vy);
-    out[3] = vfma(nh, vfma(ir, sz[4], vfma(vz, sz[3], vfma(vy, sy[3], vmul(vx, sx[3])))), vz);
-    const V gp = vmul(spl<V>(k.gamma), p);
-    out[4] = vfma(nh, vfma(vz, sz[4], vfma(vy, sy[4], vfma(vx, sx[4], vmul(gp, div)))), p);
+    out[0] = vfma(nh, vfma(qh[0], div, vfma(qh[3], sz[0], vfma(qh[2], sy[0], vmul(qh[1], sx[0])))), rho);
+    out[1] = vfma(nh, vfma(ir, sx[4], vfma(qh[3], sz[1], vfma(qh[2], sy[1], vmul(qh[1], sx[1])))), vx);
+    out[2] = vfma(nh, vfma(ir, sy[4], vfma(qh[3], sz[2], vfma(qh[2], sy[2], vmul(qh[1], sx[2])))), vy);
+    out[3] = vfma(nh, vfma(ir, sz[4], vfma(qh[3], sz[3], vfma(qh[2], sy[3], vmul(qh[1], sx[3])))), vz);
+    const V gp = vmul(spl<V>(k.gamma), qh[4]);
+    out[4] = vfma(nh, vfma(qh[3], sz[4], vfma(qh[2], sy[4], vfma(qh[1], sx[4], vmul(gp, div)))), p);
 }
 
 // Rusanov face flux (calc_flux_reconstruction, physics.rs:338-400): a is the
@@ -198,10 +230,10 @@ __device__ __forceinline__ void face(const V a[5], const V b[5], V gh, const K<T
     F[4] = vfma(c, vsub(ea, eb), fe);
 }
 
-// xt +- s/2
-template <class V> __device__ __forceinline__ void half_step(const V xt[5], const V s[5], double sign, V out[5]) {
+// xt + s/2 (sign > 0) or xt - s/2: with half slopes hs = s/2, a sum
+template <class V> __device__ __forceinline__ void half_step(const V xt[5], const V hs[5], double sign, V out[5]) {
 #pragma unroll
-    for (int f = 0; f < 5; ++f) out[f] = vfma(s[f], spl<V>(0.5 * sign), xt[f]);
+    for (int f = 0; f < 5; ++f) out[f] = sign > 0 ? vadd(xt[f], hs[f]) : vsub(xt[f], hs[f]);
 }
 
 // Boundary modes of a tile side.
@@ -314,14 +346,14 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
         V u[5];
 #pragma unroll
         for (int f = 0; f < 5; ++f) u[f] = ldv(&C(sl, f, ry, cz));
-        prim(u, q, k);
+        prim_half(u, q, k);
     }
     // Two staged cells that are not adjacent (columns c0, c1 of row ry).
     static __device__ __forceinline__ void load_prim_split(T *sl, int ry, int c0, int c1, const K<T> &k, V q[5]) {
         V u[5];
 #pragma unroll
         for (int f = 0; f < 5; ++f) u[f] = mk(C(sl, f, ry, c0), C(sl, f, ry, c1));
-        prim(u, q, k);
+        prim_half(u, q, k);
     }
     static __device__ __forceinline__ void store_pb(Sm &s, int par, int row, int col, const V q[5]) {
 #pragma unroll
@@ -350,6 +382,14 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
     // Block-wide barrier reached from the three roles' own code (bar.sync
     // counts arrivals, not call sites; every role takes the same sequence).
     static __device__ __forceinline__ void barrier() { asm volatile("bar.sync 0;" ::: "memory"); }
+
+    // Plane nx-3 with a non-periodic upper x face: the owned warps stash the
+    // ghost rule's operands in the y-state slot of parity (nx-2) & 1, which
+    // the row above reads until the end of plane nx-4's second phase.  Every
+    // role takes one more barrier at the start of that plane.
+    static __device__ __forceinline__ bool upper_stash(const GridArgs<T> &a, int m) {
+        return m == a.nx - 3 && a.bc[1] != kPeriodic;
+    }
 
     // Geometry and constants of one work item, shared by the three roles.
     struct Tile {
@@ -388,11 +428,17 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
         const bool edge_even = edge && !t.odd;
         const bool yout = r == 0 && t.ylo == kOut;
         const bool zout = lane == 0 && t.zlo == kOut;
+        const bool zheat = lane == 0 && t.zlo == kWallM && (a.heat & 4);
         const bool img_y = y <= 3 || y >= a.ny - 4;
         const bool img_z = z <= 3 || z + 1 >= a.nz - 4;
-        V q[5], dq[5], xtp[5], sxp[5], acc[5], tu[5];
+        // carried along the march: lox, the lower state of the x face ahead
+        // (xt + s/2 of the previous plane); acc, the previous plane's flux
+        // balance so far; tu, the update term of the plane before it.  The
+        // own cell's primitives of the current and the previous plane are
+        // read back from the primitive buffer.
+        V lox[5], acc[5], tu[5];
 #pragma unroll
-        for (int f = 0; f < 5; ++f) q[f] = dq[f] = xtp[f] = sxp[f] = acc[f] = tu[f] = spl<V>(0.0);
+        for (int f = 0; f < 5; ++f) lox[f] = acc[f] = tu[f] = spl<V>(0.0);
 
         // Update of plane xu (staged index sl_idx) with the term tu: the new
         // state and its wave speeds (stores are left to the caller).
@@ -476,16 +522,18 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
             }
         };
 
-        // prologue: planes xs-2, xs-1
+        // prologue: planes xs-2, xs-1 (the own row of both into the buffer)
         bool ok = wait_plane(s, 0, t.budget);
-        if (ok && active) load_prim_pair(slot(s, 0), r + 2, col, k, q);
+        if (ok && active) {
+            V q0[5];
+            load_prim_pair(slot(s, 0), r + 2, col, k, q0);
+            store_pb(s, t.xs & 1, r + 1, col, q0);
+        }
         ok = ok && wait_plane(s, 1, t.budget);
         if (ok && active) {
-            V qn[5];
-            load_prim_pair(slot(s, 1), r + 2, col, k, qn);
-            store_pb(s, (t.xs - 1) & 1, r + 1, col, qn);
-#pragma unroll
-            for (int f = 0; f < 5; ++f) { dq[f] = vsub(qn[f], q[f]); q[f] = qn[f]; }
+            V q1[5];
+            load_prim_pair(slot(s, 1), r + 2, col, k, q1);
+            store_pb(s, (t.xs - 1) & 1, r + 1, col, q1);
         }
         if (!ok) s.abort_flag[t.xs & 1] = 1;
         fence_proxy_async();
@@ -496,12 +544,20 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
             const int l = m - t.xs + 3;
             const int pm = m & 1;
             const bool upd = m >= t.xs && m < t.xe;
-            V sy[5], sz[5];
+            V sy[5], sz[5], xtc[5];
+            if (upper_stash(a, m)) barrier();
             if (!wait_plane(s, l, t.budget)) s.abort_flag[m & 1] = 1;
             if (active) {
-                V qn[5], dn[5], sx[5], xt[5], u[5], sp;
+                V q[5], dq[5], qn[5], dn[5], sx[5], xt[5], u[5], sp;
+                // the own cell at planes m and m-1 (this thread's entries), read
+                // before the conversion of plane m+1 replaces plane m-1's
+#pragma unroll
+                for (int f = 0; f < 5; ++f) {
+                    q[f] = ldv(&s.pb[pm][f][r + 1][col]);
+                    dq[f] = vsub(q[f], ldv(&s.pb[pm ^ 1][f][r + 1][col]));
+                }
                 load_prim_pair(slot(s, l), r + 2, col, k, qn);
-                store_pb(s, (m + 1) & 1, r + 1, col, qn);
+                store_pb(s, pm ^ 1, r + 1, col, qn);
                 // update of plane m-2 (from plane xs on; earlier iterations
                 // compute on a valid slot and store nothing)
                 const bool do_upd = m - 2 >= t.xs;
@@ -510,28 +566,45 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
                 for (int f = 0; f < 5; ++f) dn[f] = vsub(qn[f], q[f]);
                 slopes_adj(s, pm, r + 1, col, q, dq, dn, nullptr, nullptr, sx, sy, sz);
                 predict(q, sx, sy, sz, k, xt);
-                if (m >= t.xs) {
-                    // ghost rules of the x faces: a wall's ghost plane 1 takes the
-                    // mirrored prediction of plane 2; the upper ghost plane takes
-                    // the last plane's state (outflow) or its mirror (wall)
-                    if (m == 2 && a.bc[0] == kWall) {
+                // ghost rules of the x faces (rare planes): a wall's ghost
+                // plane 1 takes the mirrored prediction of plane 2 with its
+                // own slope; the upper ghost plane takes the last plane's state
+                // and slope (outflow) or its mirrored prediction with its own
+                // slope (wall).  The operands wait one plane in the own row's
+                // slot of the y-state buffer of the parity no plane publishes
+                // meanwhile: ypl[0] before plane 2 publishes, ypl[(nx-2) & 1]
+                // after plane nx-4 was read (upper_stash's barrier) and with
+                // no upper ghost publish.
+                const bool wall_lo = a.bc[0] == kWall, hi_rule = a.bc[1] != kPeriodic;
+                T *stash = &s.ypl[m == 1 ? 0 : (a.nx - 2) & 1][r + 1][0][2 * lane];
+                if ((m == 1 && wall_lo) || (m == a.nx - 3 && hi_rule)) {
 #pragma unroll
-                        for (int f = 0; f < 5; ++f) xtp[f] = xt[f];
-                        xtp[1] = mirror(xtp[1], true);
+                    for (int f = 0; f < 5; ++f) {
+                        // lower wall: plane 1's slope; upper outflow: xt - s/2;
+                        // upper wall: the mirrored xt
+                        const V v = m == 1 ? sx[f]
+                                           : (a.bc[1] == kOutflow ? vsub(xt[f], sx[f]) : mirror(xt[f], f == 1));
+                        stv(stash + f * kTileZ, v);
                     }
-                    if (m == a.nx - 2) {
-                        if (a.bc[1] == kOutflow) {
+                }
+                if (m >= t.xs) {
+                    V lo[5], up[5], fx[5];
+                    half_step(xt, sx, -1.0, up);
 #pragma unroll
-                            for (int f = 0; f < 5; ++f) { xt[f] = xtp[f]; sx[f] = sxp[f]; }
-                        } else if (a.bc[1] == kWall) {
+                    for (int f = 0; f < 5; ++f) lo[f] = lox[f];
+                    if (m == 2 && wall_lo) {
+                        const T *st0 = &s.ypl[0][r + 1][0][2 * lane];
 #pragma unroll
-                            for (int f = 0; f < 5; ++f) xt[f] = xtp[f];
-                            xt[1] = mirror(xt[1], true);
+                        for (int f = 0; f < 5; ++f) lo[f] = vadd(mirror(xt[f], f == 1), ldv(st0 + f * kTileZ));
+                    }
+                    if (m == a.nx - 2 && hi_rule) {
+                        const T *st1 = &s.ypl[(a.nx - 2) & 1][r + 1][0][2 * lane];
+#pragma unroll
+                        for (int f = 0; f < 5; ++f) {
+                            const V v = ldv(st1 + f * kTileZ);
+                            up[f] = a.bc[1] == kOutflow ? v : vsub(v, sx[f]);
                         }
                     }
-                    V lo[5], up[5], fx[5];
-                    half_step(xtp, sxp, 1.0, lo);
-                    half_step(xt, sx, -1.0, up);
                     face<1, false>(lo, up, spl<V>(0.0), k, fx);
                     // plane m-1 is complete but for its upper y flux and its
                     // right edge flux (added at its update, two planes on); on
@@ -543,9 +616,16 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
                         tu[f] = xo_prev ? acc[f] : vadd(acc[f], fx[f]);
                         acc[f] = xo ? spl<V>(0.0) : vmul(fx[f], spl<V>(-1.0));
                     }
+                    if (m == 2 && (a.heat & 1)) {
+                        // conducting lower x face: its heat enters plane 2
+                        // (the ghost plane's state mirrors plane 2's)
+                        acc[4].x -= heat4(xt[0].x, xt[4].x, k);
+                        acc[4].y -= heat4(xt[0].y, xt[4].y, k);
+                    }
                 }
+                half_step(xt, sx, 1.0, lox);
 #pragma unroll
-                for (int f = 0; f < 5; ++f) { xtp[f] = xt[f]; sxp[f] = sx[f]; }
+                for (int f = 0; f < 5; ++f) xtc[f] = xt[f];
                 if (upd) {
                     V st[5];
                     half_step(xt, sy, 1.0, st);
@@ -561,13 +641,11 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
                         // the right edge face (warp B) needs the last column's states
 #pragma unroll
                         for (int f = 0; f < 5; ++f) {
-                            s.zeu[pm][r][f] = xt[f].y + T(0.5) * sz[f].y;
-                            s.zex[pm][r][f] = t.zhi == kOut ? xt[f].y - T(0.5) * sz[f].y : xt[f].y;
+                            s.zeu[pm][r][f] = xt[f].y + sz[f].y;
+                            s.zex[pm][r][f] = t.zhi == kOut ? xt[f].y - sz[f].y : xt[f].y;
                         }
                     }
                 }
-#pragma unroll
-                for (int f = 0; f < 5; ++f) { q[f] = qn[f]; dq[f] = dn[f]; }
                 store(m - 2, u, sp, do_upd);
             }
             fence_proxy_async();
@@ -575,7 +653,7 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
             if (s.abort_flag[m & 1]) { aborted = true; break; }
             if (!active || !upd) continue;
             // ================= after the barrier: y and z faces of plane m
-            const V *xt = xtp;
+            const V *xt = xtc;
             V dy[5];
             if (!yout) {
                 V lo[5], up[5], fyv[5];
@@ -593,6 +671,11 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
                     stv(&s.fy[pm][r][f][2 * lane], fyv[f]);
                     dy[f] = vmul(fyv[f], spl<V>(-1.0));
                 }
+                if (r == 0 && t.ylo == kWallM && (a.heat & 2)) {
+                    // conducting lower y face (the ghost row mirrors row 2)
+                    dy[4].x -= heat4(xt[0].x, xt[4].x, k);
+                    dy[4].y -= heat4(xt[0].y, xt[4].y, k);
+                }
             } else {
 #pragma unroll
                 for (int f = 0; f < 5; ++f) dy[f] = spl<V>(0.0);
@@ -600,8 +683,8 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
             V lo[5], up[5], fzv[5];
 #pragma unroll
             for (int f = 0; f < 5; ++f) {
-                const V U = vfma(sz[f], spl<V>(0.5), xt[f]);
-                const V L = vfma(sz[f], spl<V>(-0.5), xt[f]);
+                const V U = vadd(xt[f], sz[f]);
+                const V L = vsub(xt[f], sz[f]);
                 // the halo columns' states (broadcast loads, used by lane 0
                 // and, for an odd width, by the edge lane)
                 const T mx = f == 3 ? -xt[f].x : xt[f].x;   // wall mirror of the pair's first cell
@@ -622,6 +705,8 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
                 if (edge_even) hi = T(0);   // right edge face: added at the update
                 V dz = vsub(mk(fzv[f].y, hi), fzv[f]);
                 if (zout) dz.x = T(0);
+                // conducting lower z face: the heat of the first column
+                if (f == 4 && zheat) dz.x -= heat4(xt[0].x, xt[4].x, k);
                 acc[f] = vadd(acc[f], vadd(dy[f], dz));
             }
         }
@@ -689,6 +774,7 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
             const int l = m - t.xs + 3;
             const int pm = m & 1;
             const bool upd = m >= t.xs && m < t.xe;
+            if (upper_stash(a, m)) barrier();
             if (!wait_plane(s, l, t.budget)) s.abort_flag[m & 1] = 1;
             V qn[5], q2n[5], qtn[5], dn[5], dtn[5];
 #pragma unroll
@@ -709,7 +795,7 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
                         half_step(xt, sy, 1.0, st);
                     } else {
 #pragma unroll
-                        for (int f = 0; f < 5; ++f) st[f] = vmul(sy[f], spl<V>(0.5));
+                        for (int f = 0; f < 5; ++f) st[f] = sy[f];
                     }
 #pragma unroll
                     for (int f = 0; f < 5; ++f) stv(&s.ypl[pm][0][f][2 * lane], st[f]);
@@ -730,7 +816,7 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
                     predict(qt, sx, sy, sz, k, xt);
 #pragma unroll
                     for (int f = 0; f < 5; ++f) {
-                        const T hz0 = T(0.5) * sz[f].x, hz1 = T(0.5) * sz[f].y;
+                        const T hz0 = sz[f].x, hz1 = sz[f].y;   // half slopes
                         s.zl[pm][lane][f] = t.zlo == kWallM ? hz0 : xt[f].x + hz0;
                         s.zr[pm][lane][f] = t.zhi == kWallM ? -hz1 : xt[f].y - hz1;
                     }
@@ -796,6 +882,7 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
             const int l = m - t.xs + 3;
             const int pm = m & 1;
             const bool upd = m >= t.xs && m < t.xe;
+            if (upper_stash(a, m)) barrier();
             if (!wait_plane(s, l, t.budget)) s.abort_flag[m & 1] = 1;
             V qn[5], q2n[5], dn[5];
             load_prim_pair(slot(s, l), br + 1, col, k, qn);
@@ -811,7 +898,7 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
                     half_step(xt, sy, -1.0, lb);
                 } else {
 #pragma unroll
-                    for (int f = 0; f < 5; ++f) lb[f] = vmul(sy[f], spl<V>(-0.5));
+                    for (int f = 0; f < 5; ++f) lb[f] = vmul(sy[f], spl<V>(-1.0));
                 }
             }
 #pragma unroll
@@ -888,11 +975,15 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
         t.k.kp = T(2) * a.k.inv_gm1;
         t.k.c1 = T(0.5) * a.k.gm1;
         t.k.sg = (T)sqrt((double)a.k.gamma);
-        t.k.hd = T(0.5) * dt * a.k.inv_ds;
+        t.k.iv_h = T(0.5) * a.k.inv_vol;
+        t.k.nh4 = T(-2) * dt * a.k.inv_ds;   // -4 dt / (2 ds)
         {
             const T scale = dt * a.k.ds * a.k.ds;
             t.k.sc[0] = t.k.sc[1] = t.k.sc[2] = t.k.sc[3] = T(-0.5) * scale;
             t.k.sc[4] = T(-0.25) * scale;
+            // wall_heat's factor S / (d/kappa + 1/hc_out) / V, times 4
+            const T ds = a.k.ds;
+            t.k.hq4 = T(4) * ((ds * ds) / ((T(0.008f) / T(0.2f)) + (T(1.0f) / T(10.0f)))) / (ds * ds * ds);
         }
         t.gh = t.ghe = spl<V>(0.0);
         if constexpr (GRAV) {

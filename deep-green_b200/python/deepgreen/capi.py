@@ -24,6 +24,7 @@ DG_ERR_TIMEOUT = -4
 DG_ERR_NO_DEVICE = -5
 
 PERIODIC, OUTFLOW, WALL = 0, 1, 2
+CONDUCTING_WALL = 3   # DG_BC_CONDUCTING_WALL: a wall with the heat source of the reference's CUDA variant
 LIMITER_NONE, LIMITER_MINMOD = 0, 1
 F32, F64 = 0, 1
 ROUNDING_DEFAULT, ROUNDING_REFERENCE, ROUNDING_FAST = 0, 1, 2

@@ -24,6 +24,8 @@ class BoundaryType(IntEnum):
     PERIODIC = capi.PERIODIC
     OUTFLOW = capi.OUTFLOW
     WALL = capi.WALL
+    # the reference's CUDA variant only (src/cu/include/constants.h:44)
+    CONDUCTING_WALL = capi.CONDUCTING_WALL
 
 
 @dataclass

@@ -54,6 +54,18 @@ extern "C" {
 #define DG_BC_PERIODIC 0
 #define DG_BC_OUTFLOW 1
 #define DG_BC_WALL 2
+/* Opt-in, from the reference's CUDA variant (src/cu/include/constants.h:44
+ * BC::CONDUCTING_WALL, the source term of src/cu/include/kernels.h:559-661):
+ * a wall whose ghosts follow DG_BC_WALL's rule and whose face conducts heat
+ * between the gas and an outside at 273 K through a wall of thickness 0.008
+ * and conductivity 0.2 (outside film coefficient 10, gas constant 287, the
+ * reference's constants).  The energy flux through the face gets
+ * Q / V = (273 - p/(287 rho)) * (ds^2 / (0.008/0.2 + 1/10)) / ds^3 before
+ * the dissipation term, p and rho of the ghost cell's extrapolated state.
+ * As in the reference, which adds the term at the flux of lower-cell index
+ * 1 on a lower face and n - 2 on an upper face, only a LOWER face's heat
+ * reaches the interior: an upper conducting face acts as a plain wall. */
+#define DG_BC_CONDUCTING_WALL 3
 
 /* slope limiter: NONE = the reference's central slopes (physics.rs:198-215);
  * MINMOD is an addition of this library */

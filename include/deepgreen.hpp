@@ -41,7 +41,13 @@ struct Error : std::runtime_error {
     Error(int32_t c, const std::string &msg) : std::runtime_error(msg), code(c) {}
 };
 
-enum class BoundaryType : int32_t { PERIODIC = DG_BC_PERIODIC, OUTFLOW = DG_BC_OUTFLOW, WALL = DG_BC_WALL };
+// CONDUCTING_WALL: the reference's CUDA variant only (src/cu/include/constants.h:44)
+enum class BoundaryType : int32_t {
+    PERIODIC = DG_BC_PERIODIC,
+    OUTFLOW = DG_BC_OUTFLOW,
+    WALL = DG_BC_WALL,
+    CONDUCTING_WALL = DG_BC_CONDUCTING_WALL
+};
 
 // globals.rs:3-8 (f32 in the reference)
 inline constexpr double GAMMA = 5.0 / 3.0;

@@ -45,7 +45,7 @@ dgo_ctx *dgo_create(const dgo_info *info, int32_t precision) {
     for (int a = 0; a < 3; ++a) {
         /* Simulation::new asserts periodic pairs (grid.rs:55-63). */
         const int lo = info->bcs[2 * a], hi = info->bcs[2 * a + 1];
-        if (lo < 0 || lo > 2 || hi < 0 || hi > 2) return NULL;
+        if (lo < 0 || lo > 3 || hi < 0 || hi > 3) return NULL;
         if ((lo == DGO_PERIODIC) != (hi == DGO_PERIODIC)) return NULL;
     }
     dgo_ctx *c = (dgo_ctx *)calloc(1, sizeof(dgo_ctx));

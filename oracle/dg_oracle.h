@@ -24,7 +24,10 @@
  * Parameters that the reference hard-codes as statics (globals.rs:3-8:
  * GAMMA, CFL, G) are runtime fields here.  One addition that the reference
  * does not have is switchable and off by default: a minmod slope limiter
- * (limiter = 1).  Gravity follows physics.rs:366-372.
+ * (limiter = 1).  Gravity follows physics.rs:366-372.  The conducting wall
+ * (DGO_CONDUCTING_WALL) exists only in the reference's CUDA variant
+ * (src/cu/include/kernels.h:559-661); it is restated onto this path as
+ * that code applies it (see flux_sweep).
  *
  * PARITY UNPINNED: the reference ships no tests, golden vectors or stored
  * outputs, and none of its implementations can be built or run in this
@@ -47,8 +50,11 @@
 extern "C" {
 #endif
 
-/* BoundaryType, grid.rs:23-28 (same order). */
-enum { DGO_PERIODIC = 0, DGO_OUTFLOW = 1, DGO_WALL = 2 };
+/* BoundaryType, grid.rs:23-28 (same order), plus the CUDA variant's
+ * conducting wall (src/cu/include/constants.h:44 BC::CONDUCTING_WALL): a
+ * wall whose ghosts follow the wall rule (src/cu/include/kernels.h:327) and
+ * whose flux gets a heat source (kernels.h:559-661; see flux_sweep). */
+enum { DGO_PERIODIC = 0, DGO_OUTFLOW = 1, DGO_WALL = 2, DGO_CONDUCTING_WALL = 3 };
 
 /* Array groups of SimulationGrid, grid.rs:111-118. */
 enum { DGO_PRIM = 0, DGO_XTR = 1, DGO_CONS = 2, DGO_GRAD = 3, DGO_FLUX = 4 };

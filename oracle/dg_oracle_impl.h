@@ -116,7 +116,7 @@ static void FN(apply_bc)(const FN(state) *s, REAL *a, int comp) {
                 FN(copy_slice)(s, a, comp, axis, m - 1, 3, 0);
             }
             break;
-        default: /* WALL */
+        default: /* WALL, CONDUCTING_WALL */
             break;
         }
     }
@@ -129,7 +129,9 @@ static void FN(apply_bc)(const FN(state) *s, REAL *a, int comp) {
 static void FN(handle_walls)(const FN(state) *s, REAL *q[5]) {
     const int n[3] = {s->nx, s->ny, s->nz};
     for (int face = 0; face < 6; ++face) {
-        if (s->info.bcs[face] != DGO_WALL) continue;
+        /* the CUDA variant fills a conducting wall's ghosts by the wall
+         * rule (src/cu/include/kernels.h:327) */
+        if (s->info.bcs[face] != DGO_WALL && s->info.bcs[face] != DGO_CONDUCTING_WALL) continue;
         const int axis = face / 2, upper = face & 1, m = n[axis];
         const int d0 = upper ? m - 2 : 1, s0 = upper ? m - 3 : 2;
         const int d1 = upper ? m - 1 : 0, s1 = upper ? m - 4 : 3;
@@ -257,10 +259,33 @@ static void FN(extrapolate)(FN(state) *s, REAL dt) {
     }
 }
 
+/* Heat conducted through a conducting wall, per unit volume: Q / V of the
+ * CUDA variant's flux kernel (src/cu/include/kernels.h:561-575), with its
+ * constants (constants.h:63-66: RS = 287, T_OUT_KELVIN = 273, VOUT_MS = 0;
+ * wall thickness d = 0.008, conductivity kappa = 0.2 as float literals) and
+ * t_in = p / (RS rho) of the face's lower cell. */
+static REAL FN(wall_heat)(REAL rho, REAL p, REAL ds) {
+    const REAL rs = (REAL)287.0f, t_out = (REAL)273.0f, vout = (REAL)0.0f;
+    const REAL t_in = p / (rs * rho);
+    const REAL hc_out = (REAL)10.0f - vout + (REAL)10.0f * SQRT(vout);
+    const REAL S = ds * ds;
+    const REAL V = ds * ds * ds;
+    const REAL d = (REAL)0.008f, kappa = (REAL)0.2f;
+    const REAL Q = (t_out - t_in) * (S / ((d / kappa) + ((REAL)1.0f / hc_out)));
+    return Q / V;
+}
+
 /* physics.rs:284-409 for sweep direction `dim`.  The caller passes the
  * arrays permuted so that slot 1 holds the normal component
  * (compute_step, physics.rs:616-677); `fo` are the output flux arrays in
- * the same permuted order. */
+ * the same permuted order.  Conducting walls: the CUDA variant adds Q / V
+ * to the energy flux of every face whose lower-cell index is 1 on the axis
+ * of a lower conducting face, or n - 2 on the axis of an upper one, in each
+ * of the three sweeps, after the advective flux and before gravity and the
+ * dissipation (kernels.h:561-661; its bcs order is x-, y-, z-, x+, y+, z+,
+ * mapped here onto this path's x-, x+, y-, y+, z-, z+).  Only the normal
+ * flux at a lower wall's first face reaches an interior cell; the others
+ * touch ghost cells only. */
 static void FN(flux_sweep)(FN(state) *s, int dim, REAL *fo[5], REAL *const gi[5], REAL *const xi[5]) {
     const REAL ds = (REAL)s->info.ds;
     const REAL gam = (REAL)s->info.gamma;
@@ -268,6 +293,8 @@ static void FN(flux_sweep)(FN(state) *s, int dim, REAL *fo[5], REAL *const gi[5]
     const int nx = s->nx, ny = s->ny, nz = s->nz;
     const int par = s->mode == DGO_ALL_PARALLEL;
     const int grav = s->info.gravity && dim == 2;
+    int heat = 0;
+    for (int f = 0; f < 6; ++f) heat |= s->info.bcs[f] == DGO_CONDUCTING_WALL;
     const size_t off = dim == 0 ? (size_t)ny * nz : (dim == 1 ? (size_t)nz : 1);
     const REAL *rho = xi[0], *vx = xi[1], *vy = xi[2], *vz = xi[3], *p = xi[4];
     const REAL *drho = gi[0], *dvx = gi[1], *dvy = gi[2], *dvz = gi[3], *dp = gi[4];
@@ -303,6 +330,15 @@ static void FN(flux_sweep)(FN(state) *s, int dim, REAL *fo[5], REAL *const gi[5]
                 fo[2][o] = mx * my / rho_star;
                 fo[3][o] = mx * mz / rho_star;
                 fo[4][o] = (en_star + p_star) * (mx / rho_star);
+                if (heat) {
+                    const int idx[3] = {i, j, k}, nn[3] = {nx, ny, nz};
+                    for (int a = 0; a < 3; ++a)   /* lower faces x, y, z */
+                        if (s->info.bcs[2 * a] == DGO_CONDUCTING_WALL && idx[a] == 1)
+                            fo[4][o] += FN(wall_heat)(rho[c], p[c], ds);
+                    for (int a = 0; a < 3; ++a)   /* upper faces */
+                        if (s->info.bcs[2 * a + 1] == DGO_CONDUCTING_WALL && idx[a] == nn[a] - 2)
+                            fo[4][o] += FN(wall_heat)(rho[c], p[c], ds);
+                }
                 if (grav) {
                     const REAL h = ((REAL)nz - (REAL)2.0 * (REAL)2) * ds - ((REAL)k - (REAL)2.0) * ds;
                     fo[1][o] += (REAL)1.0 * rho_star * G * h;

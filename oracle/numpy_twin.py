@@ -21,7 +21,7 @@ from __future__ import annotations
 
 import numpy as np
 
-PERIODIC, OUTFLOW, WALL = 0, 1, 2
+PERIODIC, OUTFLOW, WALL, CONDUCTING_WALL = 0, 1, 2, 3
 
 
 def _sl(axis: int, idx):
@@ -73,7 +73,7 @@ class TwinState:
     def _walls(self, q):
         """handle_walls: mirror two interior slices, negate normal velocity."""
         for face, bc in enumerate(self.bcs):
-            if bc != WALL:
+            if bc not in (WALL, CONDUCTING_WALL):
                 continue
             ax, up = divmod(face, 2)
             m = self.n[ax]
@@ -183,6 +183,8 @@ class TwinState:
             f2 = mx * my / rs
             f3 = mx * mz / rs
             f4 = (es + ps) * (mx / rs)
+            if CONDUCTING_WALL in self.bcs:
+                f4 = self._wall_heat(f4, X[0][c_sl], X[4][c_sl])
             if self.gravity and dim == 2:
                 nz = self.n[2]
                 k = np.arange(1, nz - 1, dtype=self.dtype)[None, None, :]
@@ -201,6 +203,29 @@ class TwinState:
             ]
         for slot, src in enumerate(perm):
             self.flux[src][c_sl + (dim,)] = out[slot] * ds
+
+    def _wall_heat(self, f4, rho, p):
+        """Conducting walls (src/cu/include/kernels.h:561-661): Q / V added to
+        the energy flux of the faces whose lower cell has index 1 on a lower
+        conducting face's axis, or n - 2 on an upper one's, lower faces first;
+        t_in = p / (RS rho) of that lower cell."""
+        T = self.dtype.type
+        ds = self.ds
+        t_in = p / (T(np.float32(287.0)) * rho)
+        hc = T(np.float32(10.0)) - T(0.0) + T(np.float32(10.0)) * np.sqrt(T(0.0))
+        S = ds * ds
+        V = ds * ds * ds
+        d, kappa = T(np.float32(0.008)), T(np.float32(0.2))
+        Q = (T(np.float32(273.0)) - t_in) * (S / ((d / kappa) + (T(np.float32(1.0)) / hc)))
+        q = Q / V
+        for up in (0, 1):
+            for ax in range(3):
+                if self.bcs[2 * ax + up] != CONDUCTING_WALL:
+                    continue
+                pos = f4.shape[ax] - 1 if up else 0   # cell index n - 2 or 1
+                sl = _sl(ax, pos)
+                f4[sl] = f4[sl] + q[sl]
+        return f4
 
     def _add_fluxes(self, dt):
         c = (slice(1, -1),) * 3

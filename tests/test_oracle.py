@@ -48,6 +48,70 @@ def test_oracle_gravity_matches_twin():
         np.testing.assert_array_equal(o.conserved()[f][INTERIOR], t.cons[f][INTERIOR])
 
 
+C = 3   # conducting wall (the reference's CUDA variant)
+
+
+def hot_gas(shape, seed):
+    """Air-like state (rho ~ 1.2, p ~ 4e5, so t_in ~ 1200 K against the
+    wall's 273 K) with smooth noise: the conducting walls cool it at a rate
+    that stays small per step."""
+    prim = random_primitives(shape, seed)
+    return [prim[0] * 1.2, prim[1] * 50.0, prim[2] * 50.0, prim[3] * 50.0, prim[4] * 4e5]
+
+
+@pytest.mark.parametrize("bcs", [(C, W, P, P, O, O), (W, C, C, C, P, P), (C,) * 6, (O, C, P, P, C, W)])
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_oracle_conducting_wall_matches_numpy_twin_bitwise(bcs, dtype):
+    shape = (6, 5, 7)
+    prim = hot_gas(shape, 17)
+    o = pyoracle.Oracle(shape, 0.05, bcs, gamma=1.4, cfl=0.4, limiter=1, dtype=dtype)
+    o.set_primitives([a.astype(dtype) for a in prim])
+    t = numpy_twin.TwinState(shape, 0.05, bcs, 1.4, 0.4, dtype=dtype, limiter=1)
+    for f in range(5):
+        t.prim[f][...] = prim[f].astype(dtype)
+    t.calc_conserved()
+    t._prim_ghosts(t.prim)
+    for _ in range(3):
+        assert o.step(1)[0] == t.compute_step()
+    for f in range(5):
+        np.testing.assert_array_equal(o.conserved()[f][INTERIOR], t.cons[f][INTERIOR])
+
+
+def _one_step(bcs, prim, shape):
+    o = pyoracle.Oracle(shape, 0.05, bcs, gamma=1.4, cfl=0.4, limiter=1)
+    o.set_primitives(prim)
+    dt = o.step(1)[0]
+    cons = o.conserved()
+    o.close()
+    return dt, cons
+
+
+def test_conducting_wall_heat_reaches_only_the_first_cells_of_a_lower_face():
+    """One step: a conducting lower x face changes only the energy of the
+    first interior plane, by dt ds^2 Q/V (cooling of the hot gas); an upper
+    conducting face adds its heat on a ghost face (kernels.h:616-627 tests
+    i == NX-2), so the interior equals the plain wall's bit for bit."""
+    shape = (6, 5, 7)
+    prim = hot_gas(shape, 3)
+    dt_w, wall = _one_step((W, W, P, P, O, O), prim, shape)
+    dt_c, lo = _one_step((C, W, P, P, O, O), prim, shape)
+    dt_u, up = _one_step((W, C, P, P, O, O), prim, shape)
+    assert dt_w == dt_c == dt_u
+    for f in range(5):
+        np.testing.assert_array_equal(up[f][INTERIOR], wall[f][INTERIOR])
+    for f in range(4):
+        np.testing.assert_array_equal(lo[f][INTERIOR], wall[f][INTERIOR])
+    d = (lo[4] - wall[4])[INTERIOR]
+    assert np.all(d[1:] == 0)
+    assert np.all(d[0] < 0)   # the wall (273 K) cools the gas
+    # size: dt ds ds (Q / V), Q from the ghost cell's extrapolated state,
+    # bounded by the first cell's cell-centred temperature within the step
+    ds = 0.05
+    t_in = prim[4][2:-2, 2:-2, 2:-2][0] / (287.0 * prim[0][2:-2, 2:-2, 2:-2][0])
+    q = (273.0 - t_in) * (ds * ds / (0.008 / 0.2 + 0.1)) / ds ** 3
+    np.testing.assert_allclose(d[0], dt_c * ds * ds * q, rtol=0.05)
+
+
 def test_golden_fixtures_reproduce():
     import sys
     from pathlib import Path

@@ -312,3 +312,47 @@ def test_sweep_fp64_gravity_and_kh64():
     assert max(errs[0], errs[1], errs[4]) <= 1e-12, errs
     assert max(errs[2], errs[3]) <= 1e-11, errs
     np.testing.assert_allclose(dts, ref_dts, rtol=1e-12)   # dt follows the amplified noise as well
+
+
+# ---------------------------------------------------------------------------
+# Conducting walls (DG_BC_CONDUCTING_WALL, the reference CUDA variant's heat
+# source, src/cu/include/kernels.h:559-661) on every kernel: the reference
+# rounding bit for bit against the oracle of the same precision, the sweep
+# at the FP32 / FP64 tolerances.  A hot gas (t_in ~ 1200 K against the
+# wall's 273 K) makes the heat term visible: the oracle with plain walls
+# differs from the one with conducting walls far beyond the tolerances.
+# ---------------------------------------------------------------------------
+C = capi.CONDUCTING_WALL
+COND_BCS = [(C, W, C, O, C, C), (W, C, P, P, C, O), (C, C, C, C, C, C)]
+
+
+def _hot_gas(shape, seed):
+    prim = random_primitives(shape, seed)
+    return [prim[0] * 1.2, prim[1] * 50.0, prim[2] * 50.0, prim[3] * 50.0, prim[4] * 4e5]
+
+
+@pytest.mark.parametrize("bcs", COND_BCS)
+@pytest.mark.parametrize("precision,dtype", [(capi.F64, np.float64), (capi.F32, np.float32)])
+def test_conducting_wall_reference_rounding_bitwise(bcs, precision, dtype):
+    shape = (13, 11, 45)
+    prim = _hot_gas(shape, 41)
+    _, ref_dts, ref = oracle_run(shape, 0.05, bcs, prim, 5, dtype=dtype)
+    _, dts, cons = gpu_run(shape, 0.05, bcs, prim, 5, precision, rounding=capi.ROUNDING_REFERENCE, chunk=3)
+    np.testing.assert_array_equal(dts, ref_dts)
+    for f in range(5):
+        np.testing.assert_array_equal(cons[f][INTERIOR], ref[f][INTERIOR], err_msg=f"field {f}")
+
+
+@pytest.mark.parametrize("shape", [(13, 11, 45), (9, 30, 100)])
+@pytest.mark.parametrize("bcs", COND_BCS)
+@pytest.mark.parametrize("precision", [capi.F64, capi.F32])
+def test_conducting_wall_sweep(shape, bcs, precision):
+    prim = _hot_gas(shape, 43)
+    _, ref_dts, ref = oracle_run(shape, 0.05, bcs, prim, 5)
+    _, dts, cons = gpu_run(shape, 0.05, bcs, prim, 5, precision, chunk=4, rounding=capi.ROUNDING_FAST)
+    assert_parity(cons, ref, dts, ref_dts, precision, f"{shape} {bcs}")
+    # the heat term matters at these tolerances
+    plain = tuple(W if b == C else b for b in bcs)
+    _, _, ref_plain = oracle_run(shape, 0.05, plain, prim, 5)
+    assert rel_l1(ref_plain[4], ref[4]) > 100 * TOL[precision]
+
