@@ -311,7 +311,7 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-STEP_KERNEL = "dg::sweep::sweep_step_kernel<float, 10, 5, 1, false>"
+STEP_KERNEL = "dg::sweep::sweep_step_kernel<float, 14, 4, 1, false>"
 
 
 def timed_steps(ctx, steps, warmup, local, world, barrier):

@@ -41,8 +41,7 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long budget) {
     if (budget < 0) return false;
     const uint32_t addr = smem_u32(bar);
-    const long long t0 = clock64();
-    while (true) {
+    auto try_wait = [&]() {
         uint32_t ok;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -51,7 +50,12 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long l
             : "=r"(ok)
             : "r"(addr), "r"(parity)
             : "memory");
-        if (ok) return true;
+        return ok != 0;
+    };
+    if (try_wait()) return true;   // the usual case: no clock reads
+    const long long t0 = clock64();
+    while (true) {
+        if (try_wait()) return true;
         if (clock64() - t0 > budget) return false;
     }
 }

@@ -92,7 +92,7 @@ inline bool is_sweep(int kind) { return kind == kFastF32 || kind == kFastF64; }
 
 // Owned tile rows (y) of each kernel.  A sweep block also runs two halo warps.
 #ifndef DG_SWEEP_ROWS_F32
-#define DG_SWEEP_ROWS_F32 10
+#define DG_SWEEP_ROWS_F32 14
 #endif
 constexpr int kSweepRowsF32 = DG_SWEEP_ROWS_F32;
 constexpr int kSweepRowsF64 = 4;

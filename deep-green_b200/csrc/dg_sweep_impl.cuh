@@ -341,6 +341,52 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
                 }
     }
 
+    // An updated pair (or its first cell) at (xq, yq, z), and for a lane at
+    // a z face of an even-width grid its z-image pair at zt (cells zc0, zc1
+    // of the pair; field 3 negated for a wall); fields 1 / 2 negated for a
+    // mirror along x / y.
+    static __device__ __forceinline__ void put(const GridArgs<T> &a, int xq, int yq, int z, const V u[5], bool s0,
+                                               bool s1, bool fx, bool fy, int zt, int zc0, int zc1, bool zflip) {
+        const long long o = ((long long)xq * a.ny + yq) * a.pitch + z;
+        if (s1) {
+#pragma unroll
+            for (int f = 0; f < 5; ++f) {
+                const bool neg = (f == 1 && fx) || (f == 2 && fy);
+                stv(a.dst + f * a.fstride + o, neg ? vmul(u[f], spl<V>(-1.0)) : u[f]);
+            }
+            if (zt >= 0) {
+                const long long oz = ((long long)xq * a.ny + yq) * a.pitch + zt;
+#pragma unroll
+                for (int f = 0; f < 5; ++f) {
+                    V v = mk(zc0 ? u[f].y : u[f].x, zc1 ? u[f].y : u[f].x);
+                    if ((f == 1 && fx) || (f == 2 && fy) || (f == 3 && zflip)) v = vmul(v, spl<V>(-1.0));
+                    stv(a.dst + f * a.fstride + oz, v);
+                }
+            }
+        } else if (s0) {
+#pragma unroll
+            for (int f = 0; f < 5; ++f) {
+                const bool neg = (f == 1 && fx) || (f == 2 && fy);
+                a.dst[f * a.fstride + o] = neg ? -u[f].x : u[f].x;
+            }
+        }
+    }
+
+    // The x / y ghost images of an updated pair next to an x or y face
+    // (boundary planes and rows only): the pair again at every image plane
+    // and row, with its z images (put).  Inlined: a call in the march
+    // constrains the register allocation of the whole loop.
+    static __device__ __forceinline__ void xy_images(const GridArgs<T> &a, int xu, int y, int z, V u0, V u1, V u2, V u3,
+                                                  V u4, bool s0, bool s1, int zt, int zc0, int zc1, bool zflip) {
+        const V u[5] = {u0, u1, u2, u3, u4};
+        int ximg[4], xflp[4], yimg[4], yflp[4];
+        const int nxi = axis_images(xu, a.nx, a.bc[0], a.bc[1], ximg, xflp);
+        const int nyi = axis_images(y, a.ny, a.bc[2], a.bc[3], yimg, yflp);
+        for (int ix = 0; ix < nxi; ++ix)
+            for (int iy = 0; iy < nyi; ++iy)
+                if (ix || iy) put(a, ximg[ix], yimg[iy], z, u, s0, s1, xflp[ix] != 0, yflp[iy] != 0, zt, zc0, zc1, zflip);
+    }
+
     // Load a pair of staged conserved values and convert it.
     static __device__ __forceinline__ void load_prim_pair(T *sl, int ry, int cz, const K<T> &k, V q[5]) {
         V u[5];
@@ -479,43 +525,13 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
             }
         }
         const bool zslow = !even_z && img_z;
-        // the pair (or its first cell) at (x', y', z'), field 1 / 2 negated
-        // for a mirror along x / y
-        auto put = [&](int xq, int yq, const V u[5], bool s0, bool s1, bool fx, bool fy) {
-            const long long o = ((long long)xq * a.ny + yq) * a.pitch + z;
-#pragma unroll
-            for (int f = 0; f < 5; ++f) {
-                V v = u[f];
-                if ((f == 1 && fx) || (f == 2 && fy)) v = vmul(v, spl<V>(-1.0));
-                if (s1) stv(a.dst + f * a.fstride + o, v);
-                else if (s0) a.dst[f * a.fstride + o] = v.x;
-            }
-            if (zt >= 0 && s1) {
-                const long long oz = ((long long)xq * a.ny + yq) * a.pitch + zt;
-#pragma unroll
-                for (int f = 0; f < 5; ++f) {
-                    V v = mk(zc0 ? u[f].y : u[f].x, zc1 ? u[f].y : u[f].x);
-                    if ((f == 1 && fx) || (f == 2 && fy) || (f == 3 && zflip)) v = vmul(v, spl<V>(-1.0));
-                    stv(a.dst + f * a.fstride + oz, v);
-                }
-            }
-        };
         auto store = [&](int xu, const V u[5], const V &sp, bool on) {
             const bool s0 = on && val0, s1 = on && val1;
             if (s0) smax = smax_of(smax, sp.x);
             if (s1) smax = smax_of(smax, sp.y);
-            put(xu, y, u, s0, s1, false, false);
+            put(a, xu, y, z, u, s0, s1, false, false, zt, zc0, zc1, zflip);
             const bool img_x = xu <= 3 || xu >= a.nx - 4;
-            if (on && (img_x || img_y)) {
-                // boundary plane or row: the pair again at every image plane
-                // and row (uniform over the warp)
-                int ximg[4], xflp[4], yimg[4], yflp[4];
-                const int nxi = axis_images(xu, a.nx, a.bc[0], a.bc[1], ximg, xflp);
-                const int nyi = axis_images(y, a.ny, a.bc[2], a.bc[3], yimg, yflp);
-                for (int ix = 0; ix < nxi; ++ix)
-                    for (int iy = 0; iy < nyi; ++iy)
-                        if (ix || iy) put(ximg[ix], yimg[iy], u, s0, s1, xflp[ix] != 0, yflp[iy] != 0);
-            }
+            if (on && (img_x || img_y)) xy_images(a, xu, y, z, u[0], u[1], u[2], u[3], u[4], s0, s1, zt, zc0, zc1, zflip);
             if (on && zslow) {
                 if (s0) images(a, xu, y, z, u[0].x, u[1].x, u[2].x, u[3].x, u[4].x);
                 if (s1) images(a, xu, y, z + 1, u[0].y, u[1].y, u[2].y, u[3].y, u[4].y);

@@ -36,7 +36,7 @@ def make_batch(shapes, seed=2024, limiter=capi.LIMITER_MINMOD, bcs=(capi.OUTFLOW
 
 def signature(shapes, device_name):
     # the tiling candidates belong to the kernel: its name is part of the key
-    h = hashlib.sha1(json.dumps([sorted(shapes), device_name, "sweep10"]).encode()).hexdigest()[:16]
+    h = hashlib.sha1(json.dumps([sorted(shapes), device_name, "sweep14"]).encode()).hexdigest()[:16]
     return h
 
 

@@ -351,8 +351,18 @@ def test_conducting_wall_sweep(shape, bcs, precision):
     _, ref_dts, ref = oracle_run(shape, 0.05, bcs, prim, 5)
     _, dts, cons = gpu_run(shape, 0.05, bcs, prim, 5, precision, chunk=4, rounding=capi.ROUNDING_FAST)
     assert_parity(cons, ref, dts, ref_dts, precision, f"{shape} {bcs}")
-    # the heat term matters at these tolerances
+    # the heat term itself, on the first layer of each lower conducting
+    # face: the kernel's energy change against plain walls is the oracle's
+    # (the term is ~1e-3 of the layer's energy over these steps, far above
+    # either precision's error)
     plain = tuple(W if b == C else b for b in bcs)
     _, _, ref_plain = oracle_run(shape, 0.05, plain, prim, 5)
-    assert rel_l1(ref_plain[4], ref[4]) > 100 * TOL[precision]
+    for ax in range(3):
+        if bcs[2 * ax] != C:
+            continue
+        layer = tuple(slice(2, 3) if a == ax else slice(2, -2) for a in range(3))
+        d_ref = ref[4][layer] - ref_plain[4][layer]
+        d_gpu = cons[4][layer] - ref_plain[4][layer]
+        assert np.abs(d_ref).sum() > 1e-4 * np.abs(ref[4][layer]).sum()
+        assert np.abs(d_gpu - d_ref).sum() <= 1e-2 * np.abs(d_ref).sum(), f"axis {ax}"
 

@@ -77,10 +77,10 @@ def test_noalloc_matches_context_entry_point_two_calls(precision, rounding, limi
     assert lib.dg_noalloc_status(0, ctypes.byref(flags)) == capi.DG_OK
     assert flags.value == 0
     for call in range(2):
-        assert dts[call] == ref_dts[call], (call, dts[call], ref_dts[call])
         for f in range(5):
             np.testing.assert_array_equal(outs[call][f][INTERIOR], ref[call][f][INTERIOR],
                                           err_msg=f"call {call} field {f}")
+        assert dts[call] == ref_dts[call], (call, dts[call], ref_dts[call])
         errs = [rel_l1(outs[call][f], ref[call][f]) for f in range(5)]
         assert max(errs) <= TOL[precision], (call, errs)
 
