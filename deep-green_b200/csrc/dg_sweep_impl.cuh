@@ -300,16 +300,14 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
 
     // Wave speeds c_s + |v| of the pair's cells in the updated state (the
     // quantity whose maximum sets the next dt, physics.rs:186-190).  FP32:
-    // fast_speed's operation sequence on pairs (every operation rounds as
-    // there, so dt agrees bit for bit with the state reduction); FP64: IEEE
+    // the state reduction's own scalar function (fast_speed), so that dt
+    // agrees bit for bit with it; the packed form of the same operations
+    // did not (one unit in the last place on some cells).  FP64: IEEE
     // square roots.
     static __device__ __forceinline__ V speed_pair(const V q[5], const K<T> &k) {
         if constexpr (sizeof(T) == 4) {
-            const V g = vmul(spl<V>(k.gamma), q[4]);
-            const V cs = vmul(g, vrsq(vmul(g, q[0])));
-            const V v2 = vfma(q[3], q[3], vfma(q[2], q[2], vmul(q[1], q[1])));
-            const V vm = vmul(v2, vrsq(mk(fmaxf(v2.x, 1e-30f), fmaxf(v2.y, 1e-30f))));
-            return vadd(cs, vm);
+            return mk(fast_speed(q[0].x, q[1].x, q[2].x, q[3].x, q[4].x, k.gamma),
+                      fast_speed(q[0].y, q[1].y, q[2].y, q[3].y, q[4].y, k.gamma));
         } else {
             auto one = [&](T r, T vx, T vy, T vz, T p) {
                 return sqrt(k.gamma * p / r) + sqrt(vx * vx + vy * vy + vz * vz);
@@ -321,8 +319,10 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
     // The ghost-cell images of one updated cell (all but the cell itself):
     // the copies the reference's ghost fill makes of a cell next to a domain
     // face (axis_images: periodic wrap, outflow copy, wall mirror with the
-    // normal momentum negated).  Rare: only cells within two of a face.
-    static __device__ __noinline__ void images(const GridArgs<T> &a, int x, int y, int z, T u0, T u1, T u2, T u3,
+    // normal momentum negated).  Rare: only cells within two of a face of a
+    // grid of odd width.  Inlined like xy_images (a call in the march costs
+    // more than the larger code).
+    static __device__ __forceinline__ void images(const GridArgs<T> &a, int x, int y, int z, T u0, T u1, T u2, T u3,
                                                T u4) {
         int ximg[4], xflp[4], yimg[4], yflp[4], zimg[4], zflp[4];
         const int nxi = axis_images(x, a.nx, a.bc[0], a.bc[1], ximg, xflp);
