@@ -394,8 +394,8 @@ def run_ours(args, world, rank, local):
         cons, ds, bcs = device_initial_state(case, n, dev)
         c = capi.Context((n, n, n), ds, bcs, gamma=GAMMA, cfl=CFL, limiter=capi.LIMITER_MINMOD,
                          precision=capi.F32, device=local)
+        torch.cuda.synchronize()   # the fields are complete before the library's stream copies them
         c.set_conserved_device([x.data_ptr() for x in cons])
-        torch.cuda.synchronize()
         return c, cons
 
     ctx, cons = make(args.case)
@@ -561,8 +561,8 @@ def run_learned(args, world, rank, local):
     net, norm, ps, tr = lw.training(128, traj, 8, 20, 40, 2000, 8, 64, 1e-3, 0, log=quiet)
     del ps
     torch.cuda.empty_cache()
-    cases = [lw.evaluate_truth(net, norm, "kh", 9001, 256, 400, log=quiet, shear=0.5, ratio=2.0),
-             lw.evaluate_truth(net, norm, "fourier", 9002, 256, 400, log=quiet)]
+    cases = [lw.evaluate_truth(net, norm, "kh", 9001, 256, 400, log=quiet, train_n=128, shear=0.5, ratio=2.0),
+             lw.evaluate_truth(net, norm, "fourier", 9002, 256, 400, log=quiet, train_n=128)]
     # the network alone at the corrector's shape: 264^3 input -> 256^3 fluxes
     dev = torch.device("cuda", local)
     feat = torch.zeros((1, 264, 264, 264, 16), dtype=torch.bfloat16, device=dev)
@@ -593,7 +593,8 @@ def run_learned(args, world, rank, local):
                     "cases": [{k: c[k] for k in ("kind", "t_end", "l1_density", "l1_density_plain_512_at_256",
                                                   "seconds", "steps", "corrector",
                                                   "criterion_learned_within_1p5x_of_plain_512",
-                                                  "time_ratio_plain_512_over_learned_256", "time_to_l1")}
+                                                  "time_ratio_plain_512_over_learned_256", "time_to_l1",
+                                                  "by_method_at_256")}
                               for c in cases]},
         "time_ratio_plain_512_over_learned_256": [c["time_ratio_plain_512_over_learned_256"] for c in cases],
         "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 8},
@@ -662,6 +663,7 @@ def run_snapshot(args, world, rank, local):
     cons, ds, bcs = device_initial_state("sod", n, dev)
     ctx = capi.Context((n, n, n), ds, bcs, gamma=GAMMA, cfl=CFL, limiter=capi.LIMITER_MINMOD,
                        precision=capi.F32, device=local)
+    torch.cuda.synchronize()   # the fields are complete before the library's stream copies them
     ctx.set_conserved_device([c.data_ptr() for c in cons])
     del cons
     ctx.enqueue_steps(max(args.warmup, 1))

@@ -450,7 +450,10 @@ int32_t dg_get_conserved_device(dg_ctx *c, void *const cons[5]) {
     if (!c->has_state) return fail(c, DG_ERR_NO_STATE, "no state set");
     int r;
     if ((r = use_device(c)) != DG_OK) return r;
-    return copy_out(c, cons, c->buf[c->cur], cudaMemcpyDeviceToDevice);
+    if ((r = copy_out(c, cons, c->buf[c->cur], cudaMemcpyDeviceToDevice)) != DG_OK) return r;
+    // the destination belongs to the caller's streams: return after the copies
+    DG_CUDA(c, cudaStreamSynchronize(c->stream));
+    return DG_OK;
 }
 
 int32_t dg_get_primitives(dg_ctx *c, void *const prim[5]) {

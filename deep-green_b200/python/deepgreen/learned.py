@@ -251,7 +251,11 @@ def device_initial_conserved(kind: str, n: int, seed: int, device: int = 0, **kw
         ke += v * v
     cons.append((vol * (0.5 * rho * ke + p / (GAMMA - 1.0))).to(torch.float32))
     del rho, vel, p, ke
-    return [t.contiguous() for t in cons], meta
+    out = [t.contiguous() for t in cons]
+    # dg_set_conserved_device copies on the context's own (non-blocking)
+    # stream: the fields must be complete before they are handed over
+    torch.cuda.synchronize(dev)
+    return out, meta
 
 
 # ---------------------------------------------------------------------------

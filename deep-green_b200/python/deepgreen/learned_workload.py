@@ -127,7 +127,23 @@ def _density_l1_device(ctx, ref):
     return float((ai - bi).abs().sum() / bi.abs().sum())
 
 
-def evaluate_truth(net, norm, kind, seed, n_coarse, fine_steps, log=print, threshold=0.02, **kw):
+def resolution_norm(norm, n_train, n_eval, order=2):
+    """The normalisation of a network trained on n_train^3 coarse grids, with
+    its output scale moved to n_eval^3.  Per step the correction is the
+    coarse step's truncation error, which for smooth flow shrinks like
+    dt ds^2 ~ ds^3 (second order in space, dt ~ ds), while the network's
+    dominant input, the change over the step, shrinks like dt ~ ds: a network
+    that responds in proportion to its inputs over-corrects by
+    (n_eval / n_train)^order with order = 2.  The output scale is multiplied
+    by (n_train / n_eval)^order."""
+    s = learned.Norm.from_dict(norm.to_dict())
+    f = (n_train / n_eval) ** order
+    for c in range(16):
+        s.out_std[c] = s.out_std[c] * f
+    return s
+
+
+def evaluate_truth(net, norm, kind, seed, n_coarse, fine_steps, log=print, threshold=0.02, train_n=None, **kw):
     """The learned-vs-plain comparison against a plain solve at FOUR times the
     coarse resolution (1024^3 for the 256^3 workload), which serves as the
     truth for every method, including the 512^3 plain solve.
@@ -139,7 +155,11 @@ def evaluate_truth(net, norm, kind, seed, n_coarse, fine_steps, log=print, thres
     with the truth summed to its own resolution, and the 512^3 solution also
     at the 256^3 resolution, where the workload's criterion compares it with
     the corrected 256^3 solve (error within 1.5x).  Time to L1 <= threshold:
-    the fastest method whose density error is within the threshold."""
+    the fastest method whose density error is within the threshold.  With
+    train_n (the coarse resolution of the training pairs) the corrected
+    solves at other resolutions run twice: with the trained normalisation
+    ("learned_n") and with its output scale moved to n (resolution_norm,
+    "learned_rs_n")."""
     import torch
     n1, n2, n4 = n_coarse, 2 * n_coarse, 4 * n_coarse
     cons, meta = learned.device_initial_conserved(kind, n4, seed, **kw)
@@ -153,13 +173,17 @@ def evaluate_truth(net, norm, kind, seed, n_coarse, fine_steps, log=print, thres
         plain[n] = learned.grid(n)
         learned.coarsen(prev, plain[n])
         prev = plain[n]
+    # corrected solves: (name, resolution, normalisation)
+    variants = [(f"learned_{n}", n, norm) for n in (n1, n1 // 2)]
+    if train_n:
+        variants += [(f"learned_rs_{n}", n, resolution_norm(norm, train_n, n)) for n in (n1, n1 // 2) if n != train_n]
     corr = {}
-    for n in (n1, n1 // 2):
-        corr[n] = learned.grid(n)
-        learned.coarsen(plain[2 * n], corr[n])
+    for name, n, _ in variants:
+        corr[name] = learned.grid(n)
+        learned.coarsen(plain[2 * n], corr[name])
     # corrected steps on scratch grids outside the clocks: the network's
     # workspace and launch attributes are set up once per shape
-    for n in corr:
+    for n in (n1, n1 // 2):
         w = learned.grid(n)
         learned.coarsen(plain[2 * n], w)
         cw = learned.Corrector(w, net, norm)
@@ -182,13 +206,13 @@ def evaluate_truth(net, norm, kind, seed, n_coarse, fine_steps, log=print, thres
     for n in sizes[1:]:
         steps[f"plain_{n}"], times[f"plain_{n}"] = learned.solve_to_time(plain[n], t_end)
     stats = {}
-    for n in corr:
-        cor = learned.Corrector(corr[n], net, norm)
-        steps[f"learned_{n}"], times[f"learned_{n}"] = learned.solve_to_time(corr[n], t_end, corrector=cor)
+    for name, n, nm in variants:
+        cor = learned.Corrector(corr[name], net, nm)
+        steps[name], times[name] = learned.solve_to_time(corr[name], t_end, corrector=cor)
         st = cor.stats()
-        stats[f"learned_{n}"] = {"fallback_step_rate": st["fallback_steps"] / max(1, st["steps"]),
-                                 "masked_cell_rate": st["masked_cells"] / max(1, st["cells"]),
-                                 "max_drift": st["max_drift"]}
+        stats[name] = {"fallback_step_rate": st["fallback_steps"] / max(1, st["steps"]),
+                       "masked_cell_rate": st["masked_cells"] / max(1, st["cells"]),
+                       "max_drift": st["max_drift"]}
         cor.close()
     # the truth summed to every resolution
     ref, prev = {}, truth
@@ -198,8 +222,8 @@ def evaluate_truth(net, norm, kind, seed, n_coarse, fine_steps, log=print, thres
         prev = ref[n]
     truth.close()
     err = {f"plain_{n}": _density_l1_device(plain[n], ref[n]) for n in sizes}
-    for n in corr:
-        err[f"learned_{n}"] = _density_l1_device(corr[n], ref[n])
+    for name, n, _ in variants:
+        err[name] = _density_l1_device(corr[name], ref[n])
     c512 = learned.grid(n1)
     learned.coarsen(plain[n2], c512)
     err_512_at_256 = _density_l1_device(c512, ref[n1])
@@ -216,6 +240,11 @@ def evaluate_truth(net, norm, kind, seed, n_coarse, fine_steps, log=print, thres
         "time_ratio_plain_512_over_learned_256": times[f"plain_{n2}"] / times[f"learned_{n1}"],
         "time_to_l1": {"threshold": threshold, "meeting": meeting, "fastest": best,
                        "fastest_seconds": meeting.get(best) if best else None},
+        # every corrected solve at the workload's resolution against the criterion
+        "by_method_at_256": {name: {"l1_density": err[name],
+                                    "within_1p5x_of_plain_512_at_256": err[name] <= 1.5 * err_512_at_256,
+                                    "time_ratio_plain_512_over_it": times[f"plain_{n2}"] / times[name]}
+                             for name, n, _ in variants if n == n1},
     })
     for g in list(plain.values()) + list(corr.values()) + list(ref.values()) + [c512]:
         g.close()
@@ -261,8 +290,9 @@ def main(argv=None):
         del ps
     if not args.no_eval and args.truth:
         out["evaluation_truth"] = [
-            evaluate_truth(net, norm, "kh", 9001, cfg["eval_n"], cfg["fine_steps"], shear=0.5, ratio=2.0),
-            evaluate_truth(net, norm, "fourier", 9002, cfg["eval_n"], cfg["fine_steps"]),
+            evaluate_truth(net, norm, "kh", 9001, cfg["eval_n"], cfg["fine_steps"], train_n=cfg["n_coarse"],
+                           shear=0.5, ratio=2.0),
+            evaluate_truth(net, norm, "fourier", 9002, cfg["eval_n"], cfg["fine_steps"], train_n=cfg["n_coarse"]),
         ]
     if not args.no_eval:
         out["evaluation"] = [

@@ -146,7 +146,11 @@ int32_t dg_conservation_sums(dg_ctx *ctx, double out[5]);
 
 /* Device-pointer variants of dg_set_conserved / dg_get_conserved for
  * callers that keep the fields in their own CUDA allocations (same layout
- * as the host arrays; ordered on the context's stream). */
+ * as the host arrays).  The copies run on the context's stream, a
+ * non-blocking stream that does not order against the caller's streams:
+ * work that writes the source fields must be complete when
+ * dg_set_conserved_device is called.  Both calls return after their copies
+ * finished. */
 int32_t dg_set_conserved_device(dg_ctx *ctx, const void *const cons[5]);
 int32_t dg_get_conserved_device(dg_ctx *ctx, void *const cons[5]);
 
