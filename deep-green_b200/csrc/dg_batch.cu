@@ -504,7 +504,7 @@ int32_t dg_batch_autotune(dg_batch *b, int32_t steps, int32_t *tile_rows, int32_
     B_CUDA(b, cudaMemcpyAsync(save_ctl, b->ctl, b->n * sizeof(DevCtl), cudaMemcpyDeviceToDevice, b->stream));
     const unsigned long long steps0 = b->steps;
     const int rows_cand[1] = {kTY};
-    const int chunk_cand[5] = {16, 24, 32, 64, 128};
+    const int chunk_cand[6] = {16, 24, 32, 64, 128, 256};
     double best = 1e30;
     int best_rows = b->tile_rows, best_chunk = b->chunk;
     cudaEvent_t e0, e1;

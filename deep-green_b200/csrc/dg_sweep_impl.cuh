@@ -591,52 +591,68 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
                 // meanwhile: ypl[0] before plane 2 publishes, ypl[(nx-2) & 1]
                 // after plane nx-4 was read (upper_stash's barrier) and with
                 // no upper ghost publish.
-                const bool wall_lo = a.bc[0] == kWall, hi_rule = a.bc[1] != kPeriodic;
-                T *stash = &s.ypl[m == 1 ? 0 : (a.nx - 2) & 1][r + 1][0][2 * lane];
-                if ((m == 1 && wall_lo) || (m == a.nx - 3 && hi_rule)) {
-#pragma unroll
-                    for (int f = 0; f < 5; ++f) {
-                        // lower wall: plane 1's slope; upper outflow: xt - s/2;
-                        // upper wall: the mirrored xt
-                        const V v = m == 1 ? sx[f]
-                                           : (a.bc[1] == kOutflow ? vsub(xt[f], sx[f]) : mirror(xt[f], f == 1));
-                        stv(stash + f * kTileZ, v);
-                    }
-                }
-                if (m >= t.xs) {
-                    V lo[5], up[5], fx[5];
-                    half_step(xt, sx, -1.0, up);
-#pragma unroll
-                    for (int f = 0; f < 5; ++f) lo[f] = lox[f];
-                    if (m == 2 && wall_lo) {
-                        const T *st0 = &s.ypl[0][r + 1][0][2 * lane];
-#pragma unroll
-                        for (int f = 0; f < 5; ++f) lo[f] = vadd(mirror(xt[f], f == 1), ldv(st0 + f * kTileZ));
-                    }
-                    if (m == a.nx - 2 && hi_rule) {
-                        const T *st1 = &s.ypl[(a.nx - 2) & 1][r + 1][0][2 * lane];
+                // planes next to an x face (ghost rules, their stash, the
+                // lower outflow face, heat) take the full path; the others
+                // one test
+                if (m > 3 && m < a.nx - 3) {
+                    if (m >= t.xs) {
+                        V up[5], fx[5];
+                        half_step(xt, sx, -1.0, up);
+                        face<1, false>(lox, up, spl<V>(0.0), k, fx);
 #pragma unroll
                         for (int f = 0; f < 5; ++f) {
-                            const V v = ldv(st1 + f * kTileZ);
-                            up[f] = a.bc[1] == kOutflow ? v : vsub(v, sx[f]);
+                            tu[f] = vadd(acc[f], fx[f]);
+                            acc[f] = vmul(fx[f], spl<V>(-1.0));
                         }
                     }
-                    face<1, false>(lo, up, spl<V>(0.0), k, fx);
-                    // plane m-1 is complete but for its upper y flux and its
-                    // right edge flux (added at its update, two planes on); on
-                    // a lower outflow x face plane 2 sees no x divergence
-                    const bool xo_prev = m - 1 == 2 && a.bc[0] == kOutflow;
-                    const bool xo = m == 2 && a.bc[0] == kOutflow;
-#pragma unroll
-                    for (int f = 0; f < 5; ++f) {
-                        tu[f] = xo_prev ? acc[f] : vadd(acc[f], fx[f]);
-                        acc[f] = xo ? spl<V>(0.0) : vmul(fx[f], spl<V>(-1.0));
+                } else {
+                    const bool wall_lo = a.bc[0] == kWall, hi_rule = a.bc[1] != kPeriodic;
+                    T *stash = &s.ypl[m == 1 ? 0 : (a.nx - 2) & 1][r + 1][0][2 * lane];
+                    if ((m == 1 && wall_lo) || (m == a.nx - 3 && hi_rule)) {
+    #pragma unroll
+                        for (int f = 0; f < 5; ++f) {
+                            // lower wall: plane 1's slope; upper outflow: xt - s/2;
+                            // upper wall: the mirrored xt
+                            const V v = m == 1 ? sx[f]
+                                               : (a.bc[1] == kOutflow ? vsub(xt[f], sx[f]) : mirror(xt[f], f == 1));
+                            stv(stash + f * kTileZ, v);
+                        }
                     }
-                    if (m == 2 && (a.heat & 1)) {
-                        // conducting lower x face: its heat enters plane 2
-                        // (the ghost plane's state mirrors plane 2's)
-                        acc[4].x -= heat4(xt[0].x, xt[4].x, k);
-                        acc[4].y -= heat4(xt[0].y, xt[4].y, k);
+                    if (m >= t.xs) {
+                        V lo[5], up[5], fx[5];
+                        half_step(xt, sx, -1.0, up);
+    #pragma unroll
+                        for (int f = 0; f < 5; ++f) lo[f] = lox[f];
+                        if (m == 2 && wall_lo) {
+                            const T *st0 = &s.ypl[0][r + 1][0][2 * lane];
+    #pragma unroll
+                            for (int f = 0; f < 5; ++f) lo[f] = vadd(mirror(xt[f], f == 1), ldv(st0 + f * kTileZ));
+                        }
+                        if (m == a.nx - 2 && hi_rule) {
+                            const T *st1 = &s.ypl[(a.nx - 2) & 1][r + 1][0][2 * lane];
+    #pragma unroll
+                            for (int f = 0; f < 5; ++f) {
+                                const V v = ldv(st1 + f * kTileZ);
+                                up[f] = a.bc[1] == kOutflow ? v : vsub(v, sx[f]);
+                            }
+                        }
+                        face<1, false>(lo, up, spl<V>(0.0), k, fx);
+                        // plane m-1 is complete but for its upper y flux and its
+                        // right edge flux (added at its update, two planes on); on
+                        // a lower outflow x face plane 2 sees no x divergence
+                        const bool xo_prev = m - 1 == 2 && a.bc[0] == kOutflow;
+                        const bool xo = m == 2 && a.bc[0] == kOutflow;
+    #pragma unroll
+                        for (int f = 0; f < 5; ++f) {
+                            tu[f] = xo_prev ? acc[f] : vadd(acc[f], fx[f]);
+                            acc[f] = xo ? spl<V>(0.0) : vmul(fx[f], spl<V>(-1.0));
+                        }
+                        if (m == 2 && (a.heat & 1)) {
+                            // conducting lower x face: its heat enters plane 2
+                            // (the ghost plane's state mirrors plane 2's)
+                            acc[4].x -= heat4(xt[0].x, xt[4].x, k);
+                            acc[4].y -= heat4(xt[0].y, xt[4].y, k);
+                        }
                     }
                 }
                 half_step(xt, sx, 1.0, lox);
