@@ -52,6 +52,12 @@ def test_create_rejects_bad_configurations_without_gpu_work():
     info.bcs[0], info.bcs[1] = capi.PERIODIC, capi.OUTFLOW   # unpaired periodic face (grid.rs:55-63)
     assert lib.dg_create(ctypes.byref(info), ctypes.byref(h)) == capi.DG_ERR_INVALID
     assert not h.value
+    info.bcs[0], info.bcs[1] = capi.PERIODIC, capi.CONDUCTING_WALL   # a conducting wall is no periodic face
+    assert lib.dg_create(ctypes.byref(info), ctypes.byref(h)) == capi.DG_ERR_INVALID
+    info.bcs[0], info.bcs[1] = 4, 4                                   # no such boundary type
+    assert lib.dg_create(ctypes.byref(info), ctypes.byref(h)) == capi.DG_ERR_INVALID
+    assert b"boundary" in lib.dg_last_error(None)
+    assert not h.value
 
 
 def _bad_info(**kw):
@@ -101,3 +107,31 @@ def test_batch_create_rejects_bad_grids_without_gpu_work():
     assert lib.dg_batch_create(2, infos, ctypes.byref(h)) == capi.DG_ERR_INVALID
     assert b"grid 1" in lib.dg_batch_last_error(None)
     assert lib.dg_batch_create(0, infos, ctypes.byref(h)) == capi.DG_ERR_INVALID
+
+
+def test_bench_traffic_figure_belongs_to_the_benchmarked_kernel():
+    """The bench reports roofline.traffic only from a capture of the kernel
+    it times; the committed summary must name that instantiation."""
+    import json
+    from pathlib import Path
+    import bench
+    d = json.loads((Path(__file__).resolve().parent.parent / "profiles" / "step_traffic.json").read_text())
+    assert d["kernel"] == bench.STEP_KERNEL
+    assert 40 <= d["dram_bytes_per_cell"] < 60
+    assert bench.ncu_traffic_per_launch(bench.STEP_KERNEL, 512) == d["dram_bytes_per_cell"] * 512 ** 3
+    assert bench.ncu_traffic_per_launch("another kernel", 512) is None
+
+
+def test_resolution_norm_scales_only_the_output_scale():
+    from deepgreen import learned
+    from deepgreen.learned_workload import resolution_norm
+    n = learned.Norm.identity()
+    for c in range(16):
+        n.in_mean[c], n.in_inv_std[c], n.out_std[c] = 0.1 * c, 1.0 + c, 2.0 + c
+    r = resolution_norm(n, 128, 256)
+    for c in range(16):
+        assert r.in_mean[c] == n.in_mean[c] and r.in_inv_std[c] == n.in_inv_std[c]
+        assert abs(r.out_std[c] - 0.25 * n.out_std[c]) <= 1e-6 * n.out_std[c]
+    same = resolution_norm(n, 128, 128)
+    assert all(same.out_std[c] == n.out_std[c] for c in range(16))
+
