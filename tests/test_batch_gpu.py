@@ -53,6 +53,29 @@ def test_batch_equals_single_grid_runs_bitwise(chunk):
             np.testing.assert_array_equal(got[f][INTERIOR], cons[f][INTERIOR], err_msg=f"grid {i} field {f}")
 
 
+def test_batch_conducting_walls_equal_single_grid_bitwise():
+    """A conducting-wall grid (DG_BC_CONDUCTING_WALL, hot gas) beside a plain
+    one in a batch: both equal their single-grid runs bit for bit."""
+    from conftest import random_primitives
+    C = capi.CONDUCTING_WALL
+    specs, prims = [], []
+    for sh, b, seed in (((13, 11, 45), (C, W, C, O, C, C), 41), ((9, 12, 20), (O,) * 6, 42)):
+        pr = random_primitives(sh, seed)
+        prims.append([pr[0] * 1.2, pr[1] * 50.0, pr[2] * 50.0, pr[3] * 50.0, pr[4] * 4e5])
+        specs.append({"shape": sh, "ds": 0.05, "bcs": b, "limiter": 1})
+    bt = capi.Batch(specs)
+    for i, p in enumerate(prims):
+        bt.set_primitives(i, p)
+    steps = 5
+    bt.step(steps)
+    for i, (sp, pr) in enumerate(zip(specs, prims)):
+        dts, cons = _single(sp, pr, steps)
+        np.testing.assert_array_equal(bt.get_dts(i, steps), dts, err_msg=f"grid {i}")
+        got = bt.get_conserved(i)
+        for f in range(5):
+            np.testing.assert_array_equal(got[f][INTERIOR], cons[f][INTERIOR], err_msg=f"grid {i} field {f}")
+
+
 def test_batch_matches_fp64_oracle():
     bt, specs, prims = _batch()
     bt.step(5)
