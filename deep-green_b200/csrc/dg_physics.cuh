@@ -25,6 +25,14 @@ namespace dg {
 // reaches them as kWall plus a heat-source flag (GridArgs::heat).
 enum Bc : int { kPeriodic = 0, kOutflow = 1, kWall = 2 };
 
+// Lower-cell index whose gravity height a z face's flux carries.  The
+// reference copies the flux of face nz-3 into face 1 on a periodic z axis
+// (apply_boundary_conditions4 on the fluxes, boundaries.rs:113-118): the
+// first interior cell's lower face carries the top face's gravity term.
+__host__ __device__ __forceinline__ int grav_klow(int klow, int nz, int bc_zlo) {
+    return klow == 1 && bc_zlo == kPeriodic ? nz - 3 : klow;
+}
+
 // Conducting-wall heat per unit volume, Q / V, of the reference's CUDA flux
 // kernel (src/cu/include/kernels.h:561-575) in its operation order, with its
 // constants (constants.h:63-66: RS = 287, T_OUT_KELVIN = 273, VOUT_MS = 0;

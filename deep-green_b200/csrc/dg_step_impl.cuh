@@ -160,7 +160,7 @@ struct StepKernel {
             xu[f] = s.xt[f * S::kRect + ru];
             gu[f] = s.gz[f * S::kRect + ru];
         }
-        Ph::face(xl, gl, xu, gu, 3, a.gravity, klow, a.nz, a.k, F, klow == 1 && (a.heat & 4));
+        Ph::face(xl, gl, xu, gu, 3, a.gravity, grav_klow(klow, a.nz, a.bc[4]), a.nz, a.k, F, klow == 1 && (a.heat & 4));
     }
 
     static __device__ void run(const GridArgs<T> &a, const CUtensorMap *tmap, int chunk, unsigned char *raw) {

@@ -31,7 +31,9 @@
 // states, fluxes; boundaries.rs:5-195 and handle_walls :197-407 applied to
 // them in compute_step, physics.rs:595-681), as composed rules:
 //   periodic: ghosts are computed like interior cells from the ghost
-//             primitives (the ghost layers hold the wrapped copies);
+//             primitives (the ghost layers hold the wrapped copies); the
+//             lower z boundary face carries the top face's gravity height
+//             (the reference copies that face's flux, grav_klow);
 //   outflow:  a ghost takes the adjacent interior cell's slopes and
 //             prediction, and the lower face repeats the next face's flux,
 //             so the first interior cell sees no divergence along that axis;
@@ -1019,7 +1021,7 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
         }
         t.gh = t.ghe = spl<V>(0.0);
         if constexpr (GRAV) {
-            t.gh = mk(grav_h(a, t.z0 + 2 * lane - 1), grav_h(a, t.z0 + 2 * lane));
+            t.gh = mk(grav_h(a, grav_klow(t.z0 + 2 * lane - 1, a.nz, a.bc[4])), grav_h(a, t.z0 + 2 * lane));
             const T g1 = grav_h(a, t.z0 + t.vz - 1);
             t.ghe = mk(g1, g1);
         }

@@ -366,3 +366,67 @@ def test_conducting_wall_sweep(shape, bcs, precision):
         assert np.abs(d_ref).sum() > 1e-4 * np.abs(ref[4][layer]).sum()
         assert np.abs(d_gpu - d_ref).sum() <= 1e-2 * np.abs(d_ref).sum(), f"axis {ax}"
 
+
+# ---------------------------------------------------------------------------
+# Seeded random configurations: shapes from 2 to 90 cells per axis (ragged
+# tiles in y and z, odd and even widths, several x chunks), every boundary
+# combination the reference allows (periodic faces in pairs, conducting
+# walls included), both limiters, gravity on or off; the FP64 sweep build at
+# 1e-12 and the FP32 build at 1e-5 against the FP64 oracle
+# ---------------------------------------------------------------------------
+def _random_config(rng):
+    shape = tuple(int(v) for v in rng.integers(2, 91, 3))
+    bcs = []
+    for _ in range(3):
+        if rng.random() < 0.3:
+            bcs += [P, P]
+        else:
+            bcs += [int(rng.choice([O, W, C])), int(rng.choice([O, W, C]))]
+    return shape, tuple(bcs), int(rng.integers(0, 2)), bool(rng.random() < 0.3), int(rng.integers(1, 6))
+
+
+@pytest.mark.parametrize("case", range(12))
+def test_sweep_random_configurations(case):
+    rng = np.random.default_rng(9000 + case)
+    shape, bcs, lim, grav, chunk = _random_config(rng)
+    prim = random_primitives(shape, 9100 + case)
+    if C in bcs:
+        prim = _hot_gas(shape, 9100 + case)
+    _, ref_dts, ref = oracle_run(shape, 0.05, bcs, prim, 4, limiter=lim, gravity=grav)
+    for precision in (capi.F64, capi.F32):
+        _, dts, cons = gpu_run(shape, 0.05, bcs, prim, 4, precision, limiter=lim, gravity=grav, chunk=chunk,
+                               rounding=capi.ROUNDING_FAST)
+        assert_parity(cons, ref, dts, ref_dts, precision, f"{shape} {bcs} lim {lim} grav {grav} chunk {chunk}")
+
+
+@pytest.mark.parametrize("case", range(12))
+def test_reference_rounding_random_configurations(case):
+    """The same configurations on the reference-rounding kernel: bit for bit
+    against the FP64 oracle."""
+    rng = np.random.default_rng(9000 + case)
+    shape, bcs, lim, grav, chunk = _random_config(rng)
+    prim = _hot_gas(shape, 9100 + case) if C in bcs else random_primitives(shape, 9100 + case)
+    _, ref_dts, ref = oracle_run(shape, 0.05, bcs, prim, 4, limiter=lim, gravity=grav)
+    _, dts, cons = gpu_run(shape, 0.05, bcs, prim, 4, capi.F64, limiter=lim, gravity=grav, chunk=chunk,
+                           rounding=capi.ROUNDING_REFERENCE)
+    np.testing.assert_array_equal(dts, ref_dts)
+    for f in range(5):
+        np.testing.assert_array_equal(cons[f][INTERIOR], ref[f][INTERIOR], err_msg=f"field {f}")
+
+
+def test_gravity_with_periodic_z():
+    """Gravity on a periodic z axis: the reference copies the flux of the top
+    face (nz-3) into the first cell's lower face, gravity term included."""
+    shape = (9, 10, 6)
+    prim = random_primitives(shape, 77)
+    bcs = (P,) * 6
+    _, ref_dts, ref = oracle_run(shape, 0.05, bcs, prim, 5, gravity=True)
+    for precision, rounding in ((capi.F64, capi.ROUNDING_REFERENCE), (capi.F64, capi.ROUNDING_FAST),
+                                (capi.F32, capi.ROUNDING_DEFAULT)):
+        _, dts, cons = gpu_run(shape, 0.05, bcs, prim, 5, precision, gravity=True, rounding=rounding)
+        if rounding == capi.ROUNDING_REFERENCE:
+            for f in range(5):
+                np.testing.assert_array_equal(cons[f][INTERIOR], ref[f][INTERIOR])
+        else:
+            assert_parity(cons, ref, dts, ref_dts, precision, f"rounding {rounding}")
+
