@@ -116,3 +116,44 @@ def test_batch_workload_generator_is_seeded():
     b = batch.grid_shapes(64, seed=7)
     assert a == b and len(a) == 64
     assert all(32 <= x <= 160 for sh in a for x in sh)
+
+
+@pytest.mark.parametrize("trial", range(4))
+def test_random_batches_equal_single_grid_runs_bitwise(trial):
+    """Seeded random batches: 2-8 grids of 2-60 cells per axis, every
+    boundary type, both limiters, gravity on some, a random x-chunk; each
+    grid equals its single-grid run bit for bit."""
+    from conftest import random_primitives
+    C = capi.CONDUCTING_WALL
+    rng = np.random.default_rng(40000 + trial)
+    specs, prims = [], []
+    for i in range(int(rng.integers(2, 9))):
+        shape = tuple(int(v) for v in rng.integers(2, 60, 3))
+        bcs = []
+        for _ in range(3):
+            bcs += [P, P] if rng.random() < 0.3 else [int(rng.choice([O, W, C])), int(rng.choice([O, W, C]))]
+        spec = {"shape": shape, "ds": 0.05, "bcs": tuple(bcs), "limiter": int(rng.integers(0, 2)),
+                "gravity": bool(rng.random() < 0.4)}
+        pr = random_primitives(shape, 50000 + 10 * trial + i)
+        if C in bcs:
+            pr = [pr[0] * 1.2, pr[1] * 50.0, pr[2] * 50.0, pr[3] * 50.0, pr[4] * 4e5]
+        specs.append(spec)
+        prims.append(pr)
+    steps, chunk = int(rng.integers(1, 7)), int(rng.choice([0, 8, 16, 64]))
+    bt = capi.Batch(specs)
+    for i, pr in enumerate(prims):
+        bt.set_primitives(i, pr)
+    rows, _, _ = bt.tiling()
+    bt.set_tiling(rows, chunk)
+    bt.step(steps)
+    for i, (sp, pr) in enumerate(zip(specs, prims)):
+        ctx = capi.Context(sp["shape"], 0.05, sp["bcs"], gamma=1.4, cfl=0.4, gravity=sp["gravity"],
+                           limiter=sp["limiter"], precision=capi.F32)
+        ctx.set_primitives(pr)
+        dts = ctx.compute_step(steps)
+        cons = ctx.get_conserved()
+        np.testing.assert_array_equal(bt.get_dts(i, steps), dts, err_msg=f"grid {i}")
+        got = bt.get_conserved(i)
+        for f in range(5):
+            np.testing.assert_array_equal(got[f][INTERIOR], cons[f][INTERIOR], err_msg=f"grid {i} field {f}")
+
