@@ -118,8 +118,17 @@ double dgo_calc_timestep(dgo_ctx *c) {
 
 int32_t dgo_compute_step(dgo_ctx *c, int32_t nsteps, double *dts) {
     for (int32_t s = 0; s < nsteps; ++s) {
-        double dt = c->d ? compute_step_f64(c->d) : (double)compute_step_f32(c->f);
+        double dt = c->d ? compute_step_f64(c->d, NULL) : (double)compute_step_f32(c->f, NULL);
         if (dts) dts[s] = dt;
+    }
+    return 0;
+}
+
+int32_t dgo_compute_step_given_dts(dgo_ctx *c, int32_t nsteps, const double *dts) {
+    if (!dts) return -1;
+    for (int32_t s = 0; s < nsteps; ++s) {
+        if (c->d) compute_step_f64(c->d, &dts[s]);
+        else compute_step_f32(c->f, &dts[s]);
     }
     return 0;
 }

@@ -29,15 +29,25 @@
  * (src/cu/include/kernels.h:559-661); it is restated onto this path as
  * that code applies it (see flux_sweep).
  *
- * PARITY UNPINNED: the reference ships no tests, golden vectors or stored
- * outputs, and none of its implementations can be built or run in this
- * environment (no Rust toolchain or crates, no gfortran, no warp, and the
- * CUDA path needs HighFive/HDF5).  This oracle is cross-checked against an
- * independent NumPy restatement (oracle/numpy_twin.py), against physics
- * invariants (uniform states, conservation, axis symmetry) and against the
- * mathematics (the Sod tube converges to the exact Riemann solution, the
- * periodic isentropic vortex returns after one period), not against
- * reference outputs.
+ * PARITY PINNED against the reference's own code where it can run here.
+ * The Rust path cannot be built (no Rust toolchain or crates), and the
+ * reference ships no tests or stored outputs.  Its CUDA variant's kernels
+ * (src/cu/include/kernels.h) do run here, compiled for the host by
+ * oracle/refcu on the reference's own configuration headers; their outputs
+ * are the golden vectors tests/golden/refcu_cases.npz.  Given the same dt,
+ * this oracle is bit for bit equal to them in FP64 on the KHI configuration
+ * (periodic, 5 steps) and the TRB configuration (walls, gravity), within
+ * 2e-15 on the Sod configuration (whose ds is not a power of two: the CUDA
+ * gradient multiplies by 1/(2 ds) where the Rust one divides), and in FP32
+ * bit for bit except one last-place unit of mass (a double literal in the
+ * CUDA mass flux); its own dt is within one last-place unit of theirs.
+ * Two parts of the Rust path have no counterpart there and stay pinned only
+ * by the independent NumPy restatement (oracle/numpy_twin.py) and by
+ * physics checks: the ghost rules of the derived arrays (gradients,
+ * predicted states, fluxes; boundaries.rs applied in compute_step), which
+ * the CUDA variant does not apply, so the first interior layer at a wall
+ * or outflow face differs between the two variants by design; and the
+ * minmod limiter, this project's addition.
  *
  * Build: make -C oracle   (gcc, -O2 -fopenmp -ffp-contract=off)
  */
@@ -93,6 +103,11 @@ double dgo_calc_timestep(dgo_ctx *ctx);
 /* physics.rs:595; runs nsteps steps, dt of each step written to dts[]
  * (may be NULL).  Returns 0. */
 int32_t dgo_compute_step(dgo_ctx *ctx, int32_t nsteps, double *dts);
+/* compute_step with each step's dt taken from dts[] (converted to the
+ * context's precision) instead of calc_timestep: compares the rest of the
+ * step with an implementation whose dt rounds differently (the reference's
+ * CUDA variant, whose CFL * DELTA is a float product).  -1 if dts is NULL. */
+int32_t dgo_compute_step_given_dts(dgo_ctx *ctx, int32_t nsteps, const double *dts);
 
 #ifdef __cplusplus
 }

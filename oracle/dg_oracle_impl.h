@@ -380,11 +380,12 @@ static void FN(add_fluxes)(FN(state) *s, REAL dt) {
             }
 }
 
-/* physics.rs:595-681 */
-static REAL FN(compute_step)(FN(state) *s) {
+/* physics.rs:595-681.  dt_given: NULL, or the step's dt to use in place
+ * of calc_timestep's (dgo_compute_step_given_dts). */
+static REAL FN(compute_step)(FN(state) *s, const double *dt_given) {
     FN(calc_primitives)(s);
     FN(update_prim_ghosts)(s, s->prim);
-    const REAL dt = FN(calc_timestep)(s);
+    const REAL dt = dt_given ? (REAL)*dt_given : FN(calc_timestep)(s);
     for (int f = 0; f < 5; ++f) FN(calc_gradients)(s, s->prim[f], s->grad[f]);
     for (int f = 0; f < 5; ++f) FN(apply_bc)(s, s->grad[f], 3);
     FN(extrapolate)(s, dt);

@@ -4,9 +4,10 @@ TEST INFRASTRUCTURE ONLY (checker, never the product path).
 
 Written separately from the C oracle (``dg_oracle_impl.h``) and in a
 different style: whole-array slicing instead of index loops.  The two
-readings of the Rust source are compared with each other in the tests,
-because the reference has no stored outputs to pin either of them
-(parity unpinned).
+readings of the Rust source are compared with each other in the tests.
+The C oracle is further pinned against the reference's CUDA kernels run on
+the host (dg_oracle.h); this reading is what pins the parts those kernels
+lack (the ghost rules of the derived arrays).
 
 Reference lines restated (paths within deep-green):
   src/rs/src/physics.rs: calc_primitives 109-141, calc_conserved 143-175,

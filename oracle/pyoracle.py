@@ -2,7 +2,7 @@
 
 TEST INFRASTRUCTURE ONLY: loaded by the tests, the smoke check and the
 CPU-baseline leg of the benchmark, as the checker; never by the product.
-PARITY UNPINNED (see dg_oracle.h).
+Parity: pinned against the reference's own kernels (see dg_oracle.h).
 """
 from __future__ import annotations
 
@@ -51,6 +51,9 @@ def load():
         lib.dgo_calc_timestep.restype = ctypes.c_double
         lib.dgo_compute_step.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]
         lib.dgo_compute_step.restype = ctypes.c_int32
+        lib.dgo_compute_step_given_dts.argtypes = [ctypes.c_void_p, ctypes.c_int32,
+                                                   ctypes.POINTER(ctypes.c_double)]
+        lib.dgo_compute_step_given_dts.restype = ctypes.c_int32
         _lib = lib
     return _lib
 
@@ -108,6 +111,13 @@ class Oracle:
         dts = np.zeros(max(nsteps, 1), dtype=np.float64)
         self.lib.dgo_compute_step(self.h, int(nsteps), dts.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
         return dts[:nsteps]
+
+    def step_given_dts(self, dts):
+        """Steps with the given dt per step in place of calc_timestep's."""
+        d = np.ascontiguousarray(dts, dtype=np.float64)
+        rc = self.lib.dgo_compute_step_given_dts(self.h, int(d.size), d.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        if rc != 0:
+            raise ValueError("dgo_compute_step_given_dts failed")
 
     def conserved(self):
         return [self.field(CONS, f).copy() for f in range(5)]

@@ -1,0 +1,3 @@
+// driver_types.h (host shim) -- TEST INFRASTRUCTURE ONLY; see cuda_runtime.h.
+#pragma once
+#include "cuda_runtime.h"
