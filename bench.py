@@ -53,6 +53,17 @@ correction) on an n^3 periodic KH state with random network weights.
 stream, device->host copy rate, the step time while a copy is in flight,
 and the file write rate.
 
+--case refcuda: the reference's own CUDA solver on the same GPU, as the
+same-box comparator.  oracle/refcu builds its src/cu sources (physics.hpp's
+compute_step and kernels, unchanged; spdlog, HighFive and NVTX stubbed) for
+sm_100a on its TRB configuration header (ini_files/trb.h: 124 x 124 x 252
+interior cells, walls, gravity, FP32); that program sets up the reference's
+own rising-bubble state, runs its stock time step and reports its time.
+This library then steps the same state on the same configuration: the
+first step is compared field by field with the reference's, and K steps
+are timed both as one enqueued sequence (device time) and as the
+reference's loop runs (one call per step, dt read back each step).
+
 --impl reference times the reference's CPU algorithm (the oracle port; the
 Rust crate cannot be built on this image) on the same workload and metric.
 Multi-GPU (torchrun): independent replicas, one 512^3 grid per rank
@@ -89,7 +100,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=512, help="interior cells per axis")
-    ap.add_argument("--case", default="sod", choices=["sod", "vortex", "batch64", "learned", "netfwd", "snapshot", "corrector"])
+    ap.add_argument("--case", default="sod", choices=["sod", "vortex", "batch64", "learned", "netfwd", "snapshot", "corrector",
+                                                          "refcuda"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -809,6 +821,104 @@ def run_corrector(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+REFCUDA = ROOT / "oracle" / "_ref" / "refcu" / "refcu_gpu_trb"
+# ini_files/trb.h, as the program built from it reports it
+TRB = {"n": (128, 128, 256), "ds": 1.0, "gamma": float(np.float32(5.0 / 3.0)), "cfl": float(np.float32(0.2)),
+       "g": float(np.float32(-9.81))}
+
+
+def run_refcuda(args, world, rank, local):
+    """The reference's CUDA solver (built from its sources for this GPU) and
+    this library on the reference's TRB configuration, same state, same GPU."""
+    if rank != 0:
+        return
+    import ctypes
+    import tempfile
+
+    import torch
+    from deepgreen import capi
+    base = {"case": "refcuda", "metric": METRIC, "unit": UNIT}
+    if not REFCUDA.exists():
+        print(json.dumps({**base, "unavailable": "oracle/_ref/refcu/refcu_gpu_trb not built "
+                          "(make -C oracle/refcu needs the reference sources)"}), flush=True)
+        return
+    torch.cuda.set_device(local)
+    n = TRB["n"]
+    cells = int(np.prod(n))
+    interior = tuple(k - 4 for k in n)
+    with tempfile.TemporaryDirectory() as d:
+        state = Path(d) / "state.bin"
+        with ClockSampler(local) as rclk:
+            out = subprocess.run([str(REFCUDA), str(max(args.warmup, 1)), str(args.steps), str(state)],
+                                 capture_output=True, text=True, timeout=900)
+        if out.returncode != 0:
+            print(json.dumps({**base, "unavailable": f"reference program exited {out.returncode}: "
+                              f"{out.stderr.strip()[-200:]}"}), flush=True)
+            return
+        ref = json.loads(out.stdout.strip().splitlines()[-1])
+        raw = state.read_bytes()
+    fields = cells * 4
+    prim = [np.frombuffer(raw[f * fields:(f + 1) * fields], np.float32).reshape(n) for f in range(5)]
+    ref_dt1 = float(np.frombuffer(raw[5 * fields:5 * fields + 8], np.float64)[0])
+    off = 5 * fields + 8
+    ref_cons = [np.frombuffer(raw[off + f * fields:off + (f + 1) * fields], np.float32).reshape(n)
+                for f in range(5)]
+    walls = (2,) * 6
+    ctx = capi.Context(interior, TRB["ds"], walls, gamma=TRB["gamma"], cfl=TRB["cfl"], g=TRB["g"], gravity=True,
+                       limiter=capi.LIMITER_NONE, precision=capi.F32, device=local)
+    ctx.set_primitives(prim)
+    dt1 = float(ctx.compute_step(1)[0])
+    got = ctx.get_conserved()
+    # every interior cell but the first layer at each wall, where the CUDA
+    # variant (no ghost rules for its derived arrays) and the Rust path differ
+    reg = (slice(3, n[0] - 3), slice(3, n[1] - 3), slice(3, n[2] - 3))
+    names = ("mass", "mom_x", "mom_y", "mom_z", "energy")
+    errs = {}
+    for f, nm in enumerate(names):
+        a = np.asarray(got[f], np.float64)[reg]
+        b = np.asarray(ref_cons[f], np.float64)[reg]
+        den = np.abs(b).sum()
+        errs[nm] = float(np.abs(a - b).sum() / den) if den > 0 else float(np.abs(a - b).sum())
+    # timing from the reference's initial state again
+    ctx.set_primitives(prim)
+    ms, clocks = timed_steps(ctx, args.steps, max(args.warmup, 1), local, 1, lambda: None)
+    ctx.set_primitives(prim)
+    dtbuf = (ctypes.c_double * 1)()
+    for _ in range(max(args.warmup, 1)):
+        ctx._check(ctx.lib.dg_compute_step(ctx.h, 1, dtbuf))
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        ctx._check(ctx.lib.dg_compute_step(ctx.h, 1, dtbuf))
+    e1.record(stream)
+    e1.synchronize()
+    loop_ms = e0.elapsed_time(e1)
+    ctx.close()
+    icells = int(np.prod(interior))
+    value = icells * args.steps / (ms * 1e-3) / 1e9
+    loop_value = icells * args.steps / (loop_ms * 1e-3) / 1e9
+    line = {
+        **base, "impl": "ours", "value": value, "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 1),
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "none", "vs_baseline": None,
+        "dtype": "f32", "data": "the reference's TRB set-up (init_trb, physics.hpp), produced by its own program",
+        "config": {"workload": "trb_124x124x252_walls_gravity_fp32_central",
+                   "configuration_header": "src/cu/ini_files/trb.h", "grid": list(interior), "ghosts": 2,
+                   "inputs_vs_L2": "two state buffers of 8.4e7 B each: 1.7e8 B touched per step > L2"},
+        "reference_cuda": {"value": ref["gcups"], "ms_per_step": ref["ms_per_step"], "unit": UNIT,
+                           "path": "EULERCFD::compute_step (physics.hpp:336-490), the reference's sources "
+                                   "built for sm_100a; CUDA events around its calls", "clocks": rclk.summary()},
+        "ours_host_loop": {"value": loop_value, "ms_per_step": loop_ms / args.steps,
+                           "path": "dg_compute_step(ctx, 1, &dt) per step, dt read back each step, "
+                                   "as the reference's loop reads it"},
+        "speedup_device": value / ref["gcups"], "speedup_host_loop": loop_value / ref["gcups"],
+        "parity_step1": {"rel_l1": errs, "max": max(errs.values()), "dt_rel": abs(dt1 - ref_dt1) / ref_dt1,
+                         "region": "interior minus the first layer at each wall"},
+        "clocks": clocks, "gpu_launches": args.steps,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup()
@@ -825,6 +935,8 @@ def main():
             run_snapshot(args, world, rank, local)
         elif args.case == "corrector":
             run_corrector(args, world, rank, local)
+        elif args.case == "refcuda":
+            run_refcuda(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:

@@ -1,4 +1,5 @@
-// highfive/highfive.hpp (host shim) -- TEST INFRASTRUCTURE ONLY.  The
+// highfive/highfive.hpp (stub) -- TEST INFRASTRUCTURE ONLY (HighFive and
+// HDF5 are not installed here).  The
 // reference's Grid::store writes HDF5 files through HighFive; the checker
 // never calls it, so only the names it uses are declared.
 #pragma once

@@ -1,5 +1,5 @@
-// spdlog/spdlog.h (host shim) -- TEST INFRASTRUCTURE ONLY: the log calls that
-// the reference's solver headers make are no-ops.
+// spdlog/spdlog.h (stub) -- TEST INFRASTRUCTURE ONLY: the log calls that the
+// reference's solver headers make are no-ops.
 #pragma once
 namespace spdlog {
 template <class... A> void critical(A &&...) {}
