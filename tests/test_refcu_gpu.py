@@ -65,3 +65,64 @@ def test_production_kernel_against_reference_kernels(name, precision):
     err = np.abs(got.astype(np.float64) - ref).sum(axis=1) / np.abs(ref).sum(axis=1)
     print(name, "FP64" if precision == capi.F64 else "FP32", "rel-L1 per field", err)
     assert err.max() <= (1e-12 if precision == capi.F64 else 1e-5), (name, err)
+
+
+REFCUDA = Path(__file__).resolve().parents[1] / "oracle" / "_ref" / "refcu" / "refcu_gpu_trb"
+
+
+@pytest.mark.skipif(not REFCUDA.exists(), reason="the reference's GPU program is not built "
+                    "(make -C oracle/refcu needs the reference sources)")
+def test_reference_gpu_program_and_ours_against_fp64_oracle():
+    """The reference's CUDA solver built for this GPU (its TRB set-up, one
+    step) and this library's FP32 step from the same state, each against the
+    FP64 oracle given the same dt, on the interior minus the first wall
+    layer.  The rising bubble starts near hydrostatic balance, so the
+    z momentum after one step is a small residual of cancelling pressure and
+    gravity terms: there both FP32 results carry a relative error near 2e-3
+    (measured: the reference 1.69e-3, this library 1.70e-3), and this
+    library's must stay within 5 % of the reference's own.  The transverse
+    momenta are zero in both FP32 results and round-off noise in FP64, so
+    their relative error is 1 for both."""
+    import subprocess
+    import tempfile
+
+    import pyoracle
+    n = (128, 128, 256)
+    cells = int(np.prod(n))
+    with tempfile.TemporaryDirectory() as d:
+        state = Path(d) / "state.bin"
+        subprocess.run([str(REFCUDA), "1", "1", str(state)], check=True, capture_output=True, timeout=600)
+        raw = state.read_bytes()
+    fb = cells * 4
+    prim = [np.frombuffer(raw[f * fb:(f + 1) * fb], np.float32).reshape(n) for f in range(5)]
+    dt1 = float(np.frombuffer(raw[5 * fb:5 * fb + 8], np.float64)[0])
+    off = 5 * fb + 8
+    ref_gpu = [np.frombuffer(raw[off + f * fb:off + (f + 1) * fb], np.float32).reshape(n) for f in range(5)]
+    cfg = rc.CONFIGS["trb"]
+    interior = tuple(k - 4 for k in n)
+    o = pyoracle.Oracle(interior, cfg["DELTA"], rc.bcs_dg(cfg), gamma=cfg["GAMMA"], cfl=rc.cfl_eff(cfg),
+                        limiter=0, gravity=True, g=cfg["G"], dtype=np.float64, threads=pyoracle.ALL_PARALLEL)
+    o.set_primitives([np.asarray(a, np.float64) for a in prim])
+    o.step_given_dts([dt1])
+    truth = o.conserved()
+    o.close()
+    ctx = capi.Context(interior, cfg["DELTA"], rc.bcs_dg(cfg), gamma=cfg["GAMMA"], cfl=rc.cfl_eff(cfg),
+                       g=cfg["G"], gravity=True, limiter=capi.LIMITER_NONE, precision=capi.F32)
+    ctx.set_primitives(prim)
+    dts = ctx.compute_step(1)
+    ours = ctx.get_conserved()
+    ctx.close()
+    assert abs(dts[0] - dt1) <= np.finfo(np.float32).eps * dt1
+    reg = rc.region(cfg)
+
+    def rel(a, f):
+        b = np.asarray(truth[f], np.float64)[reg]
+        den = np.abs(b).sum()
+        diff = np.abs(np.asarray(a, np.float64)[reg] - b).sum()
+        return float(diff / den) if den > 0 else float(diff)
+    e_ref = [rel(ref_gpu[f], f) for f in range(5)]
+    e_ours = [rel(ours[f], f) for f in range(5)]
+    print("reference GPU FP32 vs FP64 oracle", e_ref)
+    print("this library FP32 vs FP64 oracle ", e_ours)
+    for f in range(5):
+        assert e_ours[f] <= max(1e-5, 1.05 * e_ref[f]), (f, e_ours, e_ref)
