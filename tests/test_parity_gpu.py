@@ -385,6 +385,23 @@ def _random_config(rng):
     return shape, tuple(bcs), int(rng.integers(0, 2)), bool(rng.random() < 0.3), int(rng.integers(1, 6))
 
 
+@pytest.mark.parametrize("bcs,lim,grav", [((P,) * 6, 1, False), ((W, O, P, P, O, W), 0, True),
+                                          ((O, W, W, O, W, O), 1, True), ((P, P, O, W, P, P), 1, False)])
+def test_sweep_interior_tiles(bcs, lim, grav):
+    """Grids wide enough to hold interior tiles (full tiles two cells clear
+    of every y and z face, three or more tiles per axis) beside boundary and
+    ragged tiles, as the random configurations (at most 90 cells per axis)
+    do not: the FP64 build (4-row tiles) within 1e-12 and FP32 (14-row
+    tiles) within 1e-5 of the oracle."""
+    shape = (11, 47, 198)
+    prim = random_primitives(shape, 777 + lim + 2 * grav)
+    _, ref_dts, ref = oracle_run(shape, 0.05, bcs, prim, 4, limiter=lim, gravity=grav)
+    for precision in (capi.F64, capi.F32):
+        _, dts, cons = gpu_run(shape, 0.05, bcs, prim, 4, precision, limiter=lim, gravity=grav, chunk=5,
+                               rounding=capi.ROUNDING_FAST)
+        assert_parity(cons, ref, dts, ref_dts, precision, f"{bcs} lim {lim} grav {grav}")
+
+
 @pytest.mark.parametrize("case", range(12))
 def test_sweep_random_configurations(case):
     rng = np.random.default_rng(9000 + case)
