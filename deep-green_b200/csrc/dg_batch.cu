@@ -34,7 +34,9 @@ constexpr int kCombos = 4;           // (limiter, gravity) pairs; one launch eac
 int combo_of(const dg_sim_info &f) { return (f.limiter ? 1 : 0) + (f.gravity ? 2 : 0); }
 
 struct GridSlot {
-    dg_sim_info info;
+    dg_sim_info info;        // as stored: sizes and boundaries along the stored axes
+    int perm[3];             // stored axis d is the caller's axis perm[d]
+    int cn[3];               // the caller's ghosted sizes (x, y, z)
     int nx, ny, nz, pitch;
     long long fstride;
     size_t state_bytes;
@@ -297,10 +299,95 @@ int check_timeouts(dg_batch *b) {
 
 }  // namespace
 
+namespace {
+
+// Orientation of a grid stored with DG_BATCH_REORIENT: the axis order
+// (stored x, y, z = caller axes perm[0..2]) with the fewest padded cells --
+// z widths round up to the tile's 64 columns, y to its rows, x not at all,
+// and each x plane pays a little for the planes a work item re-stages --
+// z kept in place for a grid with gravity (it acts along z).  Ties keep the
+// caller's order.
+void choose_orientation(const dg_sim_info &f, bool reorient, int perm[3]) {
+    perm[0] = 0; perm[1] = 1; perm[2] = 2;
+    if (!reorient) return;
+    const long long n[3] = {f.nx, f.ny, f.nz};
+    auto cost = [&](const int p[3]) {
+        const long long y = (n[p[1]] + kTY - 1) / kTY * kTY, z = (n[p[2]] + kTZs - 1) / kTZs * kTZs;
+        return (n[p[0]] + 6) * y * z;
+    };
+    static const int perms[6][3] = {{0, 1, 2}, {1, 0, 2}, {0, 2, 1}, {2, 0, 1}, {1, 2, 0}, {2, 1, 0}};
+    long long best = cost(perm);
+    for (const auto &p : perms) {
+        if (f.gravity && p[2] != 2) continue;
+        const long long c = cost(p);
+        if (c < best) { best = c; perm[0] = p[0]; perm[1] = p[1]; perm[2] = p[2]; }
+    }
+}
+
+// Copies 5 fields between the caller's layout (dense, ghosted sizes cn,
+// velocity / momentum components along the caller's axes) and the stored
+// one (pitched, axes permuted by perm, components likewise).  TO_STORED:
+// caller -> stored; else stored -> caller.  One thread per destination cell.
+template <bool TO_STORED>
+__global__ void permute_fields(const float *src, float *dst, int cn0, int cn1, int cn2, int p0, int p1, int p2,
+                               int pitch, long long fstride) {
+    const int cn[3] = {cn0, cn1, cn2}, p[3] = {p0, p1, p2};
+    const long long ncaller = (long long)cn0 * cn1 * cn2;
+    const int sn0 = cn[p0], sn1 = cn[p1], sn2 = cn[p2];
+    const long long nstored = (long long)sn0 * sn1 * sn2;
+    const long long total = TO_STORED ? nstored : ncaller;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 5 * total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int f = (int)(t / total);
+        const long long c = t % total;
+        int s[3], q[3];   // stored and caller coordinates
+        if (TO_STORED) {
+            s[2] = (int)(c % sn2);
+            s[1] = (int)(c / sn2 % sn1);
+            s[0] = (int)(c / ((long long)sn2 * sn1));
+            for (int d = 0; d < 3; ++d) q[p[d]] = s[d];
+        } else {
+            q[2] = (int)(c % cn2);
+            q[1] = (int)(c / cn2 % cn1);
+            q[0] = (int)(c / ((long long)cn2 * cn1));
+            for (int d = 0; d < 3; ++d) s[d] = q[p[d]];
+        }
+        // stored component 1 + d is the caller's component 1 + p[d]
+        const int fs = f, fc = (f >= 1 && f <= 3) ? 1 + p[f - 1] : f;
+        const long long ci = ((long long)q[0] * cn1 + q[1]) * cn2 + q[2];
+        const long long si = ((long long)s[0] * sn1 + s[1]) * pitch + s[2];
+        if (TO_STORED) dst[fs * fstride + si] = src[fc * ncaller + ci];
+        else dst[fc * ncaller + ci] = src[fs * fstride + si];
+    }
+}
+
+int launch_permute(dg_batch *b, const GridSlot &s, bool to_stored, const float *src, float *dst) {
+    const long long cells = 5LL * s.cn[0] * s.cn[1] * s.cn[2];
+    const int threads = 256;
+    const int blocks = (int)std::min<long long>((cells + threads - 1) / threads, 148LL * 16);
+    if (to_stored)
+        permute_fields<true><<<blocks, threads, 0, b->stream>>>(src, dst, s.cn[0], s.cn[1], s.cn[2], s.perm[0],
+                                                                s.perm[1], s.perm[2], s.pitch, s.fstride);
+    else
+        permute_fields<false><<<blocks, threads, 0, b->stream>>>(src, dst, s.cn[0], s.cn[1], s.cn[2], s.perm[0],
+                                                                 s.perm[1], s.perm[2], s.pitch, s.fstride);
+    B_CUDA(b, cudaGetLastError());
+    return DG_OK;
+}
+
+bool identity(const GridSlot &s) { return s.perm[0] == 0 && s.perm[1] == 1 && s.perm[2] == 2; }
+
+}  // namespace
+
 extern "C" {
 
 int32_t dg_batch_create(int32_t n, const dg_sim_info *infos, dg_batch **out) {
+    return dg_batch_create_ex(n, infos, 0, out);
+}
+
+int32_t dg_batch_create_ex(int32_t n, const dg_sim_info *infos, uint32_t flags, dg_batch **out) {
     if (!out) return bfail(nullptr, DG_ERR_INVALID, "null out");
+    if (flags & ~(uint32_t)DG_BATCH_REORIENT) return bfail(nullptr, DG_ERR_INVALID, "unknown batch flags");
     *out = nullptr;
     if (n < 1 || !infos) return bfail(nullptr, DG_ERR_INVALID, "need at least one grid");
     for (int i = 0; i < n; ++i) {
@@ -328,10 +415,21 @@ int32_t dg_batch_create(int32_t n, const dg_sim_info *infos, dg_batch **out) {
     size_t total = 0;
     for (int i = 0; i < n; ++i) {
         GridSlot &s = b->g[i];
-        s.info = infos[i];
-        s.nx = infos[i].nx + 4;
-        s.ny = infos[i].ny + 4;
-        s.nz = infos[i].nz + 4;
+        const dg_sim_info &f = infos[i];
+        choose_orientation(f, (flags & DG_BATCH_REORIENT) != 0, s.perm);
+        const int cn[3] = {f.nx, f.ny, f.nz};
+        s.info = f;
+        s.info.nx = cn[s.perm[0]];
+        s.info.ny = cn[s.perm[1]];
+        s.info.nz = cn[s.perm[2]];
+        for (int d = 0; d < 3; ++d) {
+            s.info.bcs[2 * d] = f.bcs[2 * s.perm[d]];
+            s.info.bcs[2 * d + 1] = f.bcs[2 * s.perm[d] + 1];
+            s.cn[d] = cn[d] + 4;
+        }
+        s.nx = s.info.nx + 4;
+        s.ny = s.info.ny + 4;
+        s.nz = s.info.nz + 4;
         s.pitch = (s.nz + 31) / 32 * 32;
         s.fstride = (long long)s.nx * s.ny * s.pitch;
         s.state_bytes = ((size_t)5 * s.fstride * 4 + 255) / 256 * 256;
@@ -397,11 +495,22 @@ int32_t dg_batch_set_primitives(dg_batch *b, int32_t i, const void *const prim[5
     GridSlot &s = b->g[i];
     const int cur = (int)(b->steps & 1);
     void *stage = s.buf[1 - cur];
-    const size_t row = (size_t)s.nz * 4;
-    for (int f = 0; f < 5; ++f) {
+    for (int f = 0; f < 5; ++f)
         if (!prim[f]) return bfail(b, DG_ERR_INVALID, "null field");
-        B_CUDA(b, cudaMemcpy2DAsync(static_cast<char *>(stage) + (size_t)f * s.fstride * 4, (size_t)s.pitch * 4,
-                                    prim[f], row, row, (size_t)s.nx * s.ny, cudaMemcpyHostToDevice, b->stream));
+    if (identity(s)) {
+        const size_t row = (size_t)s.nz * 4;
+        for (int f = 0; f < 5; ++f)
+            B_CUDA(b, cudaMemcpy2DAsync(static_cast<char *>(stage) + (size_t)f * s.fstride * 4, (size_t)s.pitch * 4,
+                                        prim[f], row, row, (size_t)s.nx * s.ny, cudaMemcpyHostToDevice, b->stream));
+    } else {
+        // the caller's fields, dense, into the other buffer, then permuted
+        // into the stored layout
+        const size_t cells = (size_t)s.cn[0] * s.cn[1] * s.cn[2];
+        float *raw = static_cast<float *>(s.buf[cur]);
+        for (int f = 0; f < 5; ++f)
+            B_CUDA(b, cudaMemcpyAsync(raw + f * cells, prim[f], cells * 4, cudaMemcpyHostToDevice, b->stream));
+        const int r = launch_permute(b, s, true, raw, static_cast<float *>(stage));
+        if (r != DG_OK) return r;
     }
     GridArgs<float> a = args_of(b, i, cur);
     a.part = b->part;
@@ -451,11 +560,22 @@ int32_t dg_batch_get_conserved(dg_batch *b, int32_t i, void *const cons[5]) {
     B_CUDA(b, cudaSetDevice(b->device));
     const GridSlot &s = b->g[i];
     const char *src = static_cast<const char *>(s.buf[b->steps & 1]);
-    const size_t row = (size_t)s.nz * 4;
-    for (int f = 0; f < 5; ++f) {
+    for (int f = 0; f < 5; ++f)
         if (!cons[f]) return bfail(b, DG_ERR_INVALID, "null field");
-        B_CUDA(b, cudaMemcpy2DAsync(cons[f], row, src + (size_t)f * s.fstride * 4, (size_t)s.pitch * 4, row,
-                                    (size_t)s.nx * s.ny, cudaMemcpyDeviceToHost, b->stream));
+    if (identity(s)) {
+        const size_t row = (size_t)s.nz * 4;
+        for (int f = 0; f < 5; ++f)
+            B_CUDA(b, cudaMemcpy2DAsync(cons[f], row, src + (size_t)f * s.fstride * 4, (size_t)s.pitch * 4, row,
+                                        (size_t)s.nx * s.ny, cudaMemcpyDeviceToHost, b->stream));
+    } else {
+        // permuted back into the caller's layout in the other buffer (which
+        // the next step overwrites), then copied out dense
+        const size_t cells = (size_t)s.cn[0] * s.cn[1] * s.cn[2];
+        float *raw = static_cast<float *>(s.buf[1 - (b->steps & 1)]);
+        const int r = launch_permute(b, s, false, reinterpret_cast<const float *>(src), raw);
+        if (r != DG_OK) return r;
+        for (int f = 0; f < 5; ++f)
+            B_CUDA(b, cudaMemcpyAsync(cons[f], raw + f * cells, cells * 4, cudaMemcpyDeviceToHost, b->stream));
     }
     B_CUDA(b, cudaStreamSynchronize(b->stream));
     return DG_OK;
@@ -544,6 +664,12 @@ int32_t dg_batch_autotune(dg_batch *b, int32_t steps, int32_t *tile_rows, int32_
     if (chunk) *chunk = best_chunk;
     if (ms_per_step) *ms_per_step = best;
     return check_timeouts(b);
+}
+
+int32_t dg_batch_get_orientation(dg_batch *b, int32_t i, int32_t axes[3]) {
+    if (!b || !axes || i < 0 || i >= b->n) return bfail(b, DG_ERR_INVALID, "bad argument");
+    for (int d = 0; d < 3; ++d) axes[d] = b->g[i].perm[d];
+    return DG_OK;
 }
 
 int32_t dg_batch_get_stream(dg_batch *b, void **stream) {

@@ -21,30 +21,33 @@ def grid_shapes(n_grids=64, lo=32, hi=160, seed=2024):
     return [tuple(int(round(v)) for v in row) for row in e]
 
 
-def make_batch(shapes, seed=2024, limiter=capi.LIMITER_MINMOD, bcs=(capi.OUTFLOW,) * 6, device=0):
-    """A Batch with grid i holding riemann_random(shapes[i], seed + i)."""
+def make_batch(shapes, seed=2024, limiter=capi.LIMITER_MINMOD, bcs=(capi.OUTFLOW,) * 6, device=0, reorient=False):
+    """A Batch with grid i holding riemann_random(shapes[i], seed + i)
+    (reorient: capi.Batch's stored-axis choice)."""
     specs, prims = [], []
     for i, sh in enumerate(shapes):
         prim, ds, b = setups.riemann_random(sh, seed + i, bcs=bcs)
         specs.append({"shape": sh, "ds": ds, "bcs": b, "limiter": limiter})
         prims.append(prim)
-    bt = capi.Batch(specs, device=device)
+    bt = capi.Batch(specs, device=device, reorient=reorient)
     for i, p in enumerate(prims):
         bt.set_primitives(i, p)
     return bt, specs, prims
 
 
-def signature(shapes, device_name):
-    # the tiling candidates belong to the kernel: its name is part of the key
-    h = hashlib.sha1(json.dumps([sorted(shapes), device_name, "sweep14"]).encode()).hexdigest()[:16]
+def signature(shapes, device_name, reorient=False):
+    # the tiling candidates belong to the kernel: its name is part of the key,
+    # and so is the stored layout
+    key = [sorted(shapes), device_name, "sweep14"] + (["reoriented"] if reorient else [])
+    h = hashlib.sha1(json.dumps(key).encode()).hexdigest()[:16]
     return h
 
 
-def tuned(bt, shapes, device_name, cache_path=None, steps=3):
+def tuned(bt, shapes, device_name, cache_path=None, steps=3, reorient=False):
     """Tiling for this batch: from the JSON cache if present, else timed by
     dg_batch_autotune and stored."""
     path = Path(cache_path or os.environ.get("DG_AUTOTUNE_CACHE", Path.home() / ".cache" / "deepgreen_tuning.json"))
-    key = signature(shapes, device_name)
+    key = signature(shapes, device_name, reorient)
     cache = {}
     if path.exists():
         try:

@@ -28,6 +28,7 @@ CONDUCTING_WALL = 3   # DG_BC_CONDUCTING_WALL: a wall with the heat source of th
 LIMITER_NONE, LIMITER_MINMOD = 0, 1
 F32, F64 = 0, 1
 ROUNDING_DEFAULT, ROUNDING_REFERENCE, ROUNDING_FAST = 0, 1, 2
+BATCH_REORIENT = 1  # dg_batch_create_ex flag
 STATUS_NONFINITE = 0x1
 STATUS_TIMEOUT = 0x2
 SNAP_PRIMITIVES, SNAP_CONSERVED = 0x1, 0x2
@@ -91,6 +92,8 @@ SIGNATURES = {
                                ctypes.POINTER(ctypes.c_void_p), ctypes.c_uint64, ctypes.c_char_p],
     "dg_snapshot_last_error": [_P],
     "dg_batch_create": [_I, ctypes.POINTER(SimInfo), ctypes.POINTER(ctypes.c_void_p)],
+    "dg_batch_create_ex": [_I, ctypes.POINTER(SimInfo), ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p)],
+    "dg_batch_get_orientation": [_P, _I, ctypes.POINTER(_I)],
     "dg_batch_destroy": [_P],
     "dg_batch_set_primitives": [_P, _I, _PP5],
     "dg_batch_step": [_P, _I],
@@ -292,9 +295,11 @@ class Context:
 class Batch:
     """Owner of one dg_batch: independent grids stepped by one launch per
     step.  ``specs`` is a list of dicts with keys shape, ds, bcs and
-    optionally gamma, cfl, limiter, g, gravity."""
+    optionally gamma, cfl, limiter, g, gravity.  ``reorient``: let the
+    library store each grid with its axes in the order that pads its tiles
+    least (DG_BATCH_REORIENT); inputs and outputs keep the caller's layout."""
 
-    def __init__(self, specs, device=0):
+    def __init__(self, specs, device=0, reorient=False):
         self.lib = load()
         self.n = len(specs)
         arr = (SimInfo * self.n)()
@@ -317,7 +322,7 @@ class Batch:
             self.shapes.append(tuple(int(x) + 4 for x in sp["shape"]))
         self.infos = arr
         h = ctypes.c_void_p()
-        rc = self.lib.dg_batch_create(self.n, arr, ctypes.byref(h))
+        rc = self.lib.dg_batch_create_ex(self.n, arr, BATCH_REORIENT if reorient else 0, ctypes.byref(h))
         if rc != DG_OK:
             raise DgError(rc, self.lib.dg_last_error(None).decode())
         self.h = h
@@ -360,6 +365,12 @@ class Batch:
         out = [np.empty(self.shapes[i], dtype=np.float32) for _ in range(5)]
         self._check(self.lib.dg_batch_get_conserved(self.h, int(i), _ptrs(out)))
         return out
+
+    def orientation(self, i):
+        """Caller axes (0 x, 1 y, 2 z) of grid i's stored x, y, z."""
+        axes = (_I * 3)()
+        self._check(self.lib.dg_batch_get_orientation(self.h, int(i), axes))
+        return tuple(axes)
 
     def set_tiling(self, tile_rows, chunk=0):
         self._check(self.lib.dg_batch_set_tiling(self.h, int(tile_rows), int(chunk)))

@@ -263,6 +263,20 @@ const char *dg_snapshot_last_error(const dg_snapshot *snap);
  * kernel (precision DG_F32, rounding DEFAULT); all grids on one device. */
 typedef struct dg_batch dg_batch;
 int32_t dg_batch_create(int32_t n, const dg_sim_info *infos, dg_batch **out);
+/* Creation flags of dg_batch_create_ex. */
+enum {
+    /* Each grid may be stored with its axes permuted: the order with the
+     * fewest padded cells (z rounds up to the kernel's 64-column tiles, y to
+     * its rows, x not at all); z stays z for a grid with gravity.  Inputs
+     * and outputs keep the caller's layout (permuted on the device).  A
+     * permuted grid's step equals the caller-order step up to rounding (its
+     * flux balance adds the axes in another order), not bit for bit. */
+    DG_BATCH_REORIENT = 1
+};
+/* dg_batch_create with flags (0: dg_batch_create). */
+int32_t dg_batch_create_ex(int32_t n, const dg_sim_info *infos, uint32_t flags, dg_batch **out);
+/* Stored axis d of grid i is the caller's axis axes[d] (0 x, 1 y, 2 z). */
+int32_t dg_batch_get_orientation(dg_batch *b, int32_t i, int32_t axes[3]);
 int32_t dg_batch_destroy(dg_batch *b);
 /* grid i's state from host primitives, as dg_set_primitives */
 int32_t dg_batch_set_primitives(dg_batch *b, int32_t i, const void *const prim[5]);
