@@ -303,17 +303,17 @@ namespace {
 
 // Orientation of a grid stored with DG_BATCH_REORIENT: the axis order
 // (stored x, y, z = caller axes perm[0..2]) with the fewest padded cells --
-// z widths round up to the tile's 64 columns, y to its rows, x not at all,
-// and each x plane pays a little for the planes a work item re-stages --
-// z kept in place for a grid with gravity (it acts along z).  Ties keep the
-// caller's order.
+// z widths round up to the tile's 64 columns, y to its rows, x not at all
+// (charging short x axes for the planes a work item re-stages measured
+// slower on the batch64 workload) -- z kept in place for a grid with
+// gravity (it acts along z).  Ties keep the caller's order.
 void choose_orientation(const dg_sim_info &f, bool reorient, int perm[3]) {
     perm[0] = 0; perm[1] = 1; perm[2] = 2;
     if (!reorient) return;
     const long long n[3] = {f.nx, f.ny, f.nz};
     auto cost = [&](const int p[3]) {
         const long long y = (n[p[1]] + kTY - 1) / kTY * kTY, z = (n[p[2]] + kTZs - 1) / kTZs * kTZs;
-        return (n[p[0]] + 6) * y * z;
+        return n[p[0]] * y * z;
     };
     static const int perms[6][3] = {{0, 1, 2}, {1, 0, 2}, {0, 2, 1}, {2, 0, 1}, {1, 2, 0}, {2, 1, 0}};
     long long best = cost(perm);

@@ -160,10 +160,10 @@ def test_random_batches_equal_single_grid_runs_bitwise(trial):
 
 
 # Shapes whose tiles pad less in another axis order (z widths just over 64,
-# wide y, a short z), a conducting y face that is stored along z, and a
+# wide y, a short z), a conducting x face that is stored along z, and a
 # gravity grid.
 RE_SHAPES = [(40, 9, 70), (8, 33, 12), (70, 20, 30), (5, 6, 70), (30, 66, 9), (9, 33, 8)]
-RE_BCS = [(O,) * 6, (P,) * 6, (W, W, O, O, P, P), (O, W, P, P, W, O), (O, O, 3, W, W, O), (P, P, O, O, W, W)]
+RE_BCS = [(O,) * 6, (P,) * 6, (W, W, O, O, P, P), (O, W, P, P, W, O), (3, W, O, O, W, O), (P, P, O, O, W, W)]
 
 
 def _re_batch(reorient):
