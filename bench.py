@@ -9,11 +9,12 @@ cells.  Data: synthetic (the workload's initial state, built on the GPU).
 Metric: GCUPS = 1e9 cell updates per second (whole job: all ranks).
 
 Keys beside the contract's ones:
-  roofline      the step kernel against measured HBM bandwidth:
-                achieved = 40 B per cell update (read + write 5 FP32 fields)
-                x cells / mean kernel time (CUDA events on the library's
-                stream); traffic = ncu DRAM bytes per launch from the
-                committed profile of the same kernel instantiation
+  roofline      the step against measured HBM bandwidth: achieved = 40 B
+                per cell update (read + write 5 FP32 fields) x cells / mean
+                step time (CUDA events on the library's stream; a step is the
+                interior-tile launch and the frame launch that overlaps its
+                last wave); traffic = ncu DRAM bytes per step from the
+                committed profile of the same kernel pair
                 (profiles/step_traffic.json), else null.
   e2e           the same metric through the C ABI from pinned HOST buffers:
                 upload of the state, K steps reading dt back after each one
@@ -276,11 +277,12 @@ def cpu_oracle_gcups(case, n, nz_sample, steps, warmup=1, rust_like=False):
     return cells / statistics.mean(times) / 1e9, times
 
 
-def ncu_traffic_per_launch(kernel, n):
-    """DRAM bytes per launch of the benchmarked step kernel, from the
-    committed ncu summary (profiles/step_traffic.json): only when that
-    capture is of the same kernel instantiation, and scaled to n^3 cells from
-    the captured grid in proportion to the cells.  None otherwise."""
+def ncu_traffic_per_step(kernel, n):
+    """DRAM bytes per step of the benchmarked kernel pair, from the committed
+    ncu summary (profiles/step_traffic.json): only when that capture is of
+    the same kernels; each launch's bytes per cell scaled to its own cells on
+    an n^3 grid (interior tiles: full 14 x 64 tiles two cells clear of every
+    y and z face; the frame: the rest).  None otherwise."""
     p = ROOT / "profiles" / "step_traffic.json"
     if not p.exists():
         return None
@@ -288,7 +290,9 @@ def ncu_traffic_per_launch(kernel, n):
         d = json.loads(p.read_text())
         if d["kernel"] != kernel:
             return None
-        return float(d["dram_bytes_per_cell"]) * n ** 3
+        ny_in, nz_in = (n - 2) // 14 - 1, (n - 2) // 64 - 1
+        interior = ny_in * 14 * nz_in * 64 * n if ny_in > 0 and nz_in > 0 else 0
+        return float(d["interior_bytes_per_cell"]) * interior + float(d["frame_bytes_per_cell"]) * (n ** 3 - interior)
     except Exception:
         return None
 
@@ -323,7 +327,18 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-STEP_KERNEL = "dg::sweep::sweep_step_kernel<float, 14, 4, 1, false>"
+# The step's launches on grids with interior tiles (512^3: 71 % of the
+# tiles): the interior tiles, then the frame of tiles along the y and z faces.
+STEP_KERNEL = ("dg::sweep::sweep_step_kernel<float, 14, 4, 1, false, true> + "
+               "dg::sweep::sweep_step_kernel<float, 14, 4, 1, false, false>")
+
+
+def step_launches(n):
+    """Launches per step of the sweep on an n^3 grid: two with interior tiles
+    (full 14 x 64 tiles two cells clear of every y and z face), else one."""
+    ny_in = (n - 2) // 14 - 1
+    nz_in = (n - 2) // 64 - 1
+    return 2 if ny_in > 0 and nz_in > 0 else 1
 
 
 def timed_steps(ctx, steps, warmup, local, world, barrier):
@@ -510,7 +525,7 @@ def run_ours(args, world, rank, local):
         return
     peak, peak_kind = peaks()
     achieved = BYTES_PER_CELL["f32"] * cells / (ms_step * 1e-3) / 1e9
-    traffic = ncu_traffic_per_launch(STEP_KERNEL, n)
+    traffic = ncu_traffic_per_step(STEP_KERNEL, n)
     cpu = None
     parity = None
     if not args.no_cpu and world == 1:
@@ -537,11 +552,12 @@ def run_ours(args, world, rank, local):
                    "launch": {"blocks": blocks, "threads": threads, "x_planes_per_block": chunk}},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                     "algorithmic_bytes_per_launch": BYTES_PER_CELL["f32"] * cells},
+                     "algorithmic_bytes_per_step": BYTES_PER_CELL["f32"] * cells,
+                     "launches_per_step": step_launches(n)},
         "cpu_baseline": cpu,
         "e2e": e2e,
         "clocks": clocks,
-        "gpu_launches": args.steps,
+        "gpu_launches": step_launches(n) * args.steps,
         "dt_first_last": [float(dts[0]), float(dts[-1])],
         "status_flags": status,
     }

@@ -111,23 +111,71 @@ inline int step_threads(int kind) {
     return is_sweep(kind) ? 32 * (step_tile_rows(kind) + 2) : 32 * step_tile_rows(kind);
 }
 
-// Blocks of one step launch: (y tiles) x (z tiles) x (x chunks of `chunk`
-// planes).
+// Tiles of a sweep step.  Interior tiles are full tiles (rows x cols) at
+// least two cells clear of every y and z face, so that no row or column of
+// them is on a face or writes a ghost image: they form the rectangle of tile
+// rows [1, 1 + ny) x tile columns [1, 1 + nz) (tile row t starts at cell
+// 2 + t * rows and needs 2 + (t + 1) * rows <= interior cells); ny = nz = 0
+// when either side has none.  The other tiles are the frame.  A step with
+// interior tiles is two launches: the interior tiles, one block per tile
+// marching all of x, built without the owned warps' boundary switches, and
+// the frame in x-chunks (launch_sweep).
+struct InteriorTiles {
+    int tiles_y, tiles_z, ny, nz;
+    __host__ __device__ InteriorTiles(int ghosted_ny, int ghosted_nz, int rows, int cols) {
+        const int iy = ghosted_ny - 4, iz = ghosted_nz - 4;
+        tiles_y = (iy + rows - 1) / rows;
+        tiles_z = (iz + cols - 1) / cols;
+        ny = iy >= 2 ? (iy - 2) / rows - 1 : 0;
+        nz = iz >= 2 ? (iz - 2) / cols - 1 : 0;
+        if (ny <= 0 || nz <= 0) ny = nz = 0;
+    }
+    __host__ __device__ int interior() const { return ny * nz; }
+    __host__ __device__ int frame() const { return tiles_y * tiles_z - ny * nz; }
+    // tile of frame index f: the rows outside the rectangle whole, then the
+    // rectangle's rows left and right of it
+    __host__ __device__ void frame_tile(int f, int &ty, int &tz) const {
+        const int full = (tiles_y - ny) * tiles_z;
+        if (f < full) {
+            const int r = f / tiles_z;
+            tz = f % tiles_z;
+            ty = r < 1 ? r : r + ny;
+        } else {
+            const int g = f - full, w = tiles_z - nz;
+            ty = 1 + g / w;
+            const int c = g % w;
+            tz = c < 1 ? c : c + nz;
+        }
+    }
+};
+
+// Blocks of one step: (y tiles) x (z tiles) x (x chunks of `chunk` planes);
+// for a sweep step with interior tiles, one block per interior tile plus the
+// frame tiles x chunks (both launches together).
 inline int step_grid_blocks(int nx, int ny, int nz, int kind, int chunk) {
     const int ty = step_tile_rows(kind), tzc = step_tile_cols(kind);
+    const int chunks = (nx - 4 + chunk - 1) / chunk;
+    if (is_sweep(kind)) {
+        const InteriorTiles it(ny, nz, ty, tzc);
+        return it.interior() + it.frame() * chunks;
+    }
     const int tiles_z = (nz - 4 + tzc - 1) / tzc;
     const int tiles_y = (ny - 4 + ty - 1) / ty;
-    const int chunks = (nx - 4 + chunk - 1) / chunk;
     return tiles_z * tiles_y * chunks;
 }
 // Default x-planes per block.  Reference-rounding kernels: enough blocks for
 // ~14 waves of resident CTAs (2 per SM), at least 20 planes per block (each
 // block re-stages 4 planes at its ends); measured flat within 1 % from 43
-// to 74 planes on 512^3.  Sweep kernels (one block per SM): the split of x
-// into chunks that minimises waves x (planes per block + 3 re-staged),
-// with at least 24 planes per block.
+// to 74 planes on 512^3.  Sweep kernels (one block per SM): with interior
+// tiles, the frame launch's chunk (the interior launch marches whole
+// columns); without, the split of x into chunks that minimises waves x
+// (planes per block + 3 re-staged), with at least 24 planes per block.
 inline int choose_chunk(int nx, int ny, int nz, int kind) {
     const int ty = step_tile_rows(kind), tzc = step_tile_cols(kind);
+    // sweep steps with interior tiles: the frame's blocks fill the SMs the
+    // interior launch leaves free, in short chunks (32-64 planes measured
+    // 38.2-38.6 GCUPS on 512^3 Sod, whole columns 34.1-34.4)
+    if (is_sweep(kind) && InteriorTiles(ny, nz, ty, tzc).interior() > 0) return nx - 4 < 64 ? nx - 4 : 64;
     const long long tiles = (long long)((ny - 4 + ty - 1) / ty) * ((nz - 4 + tzc - 1) / tzc);
     const int nxi = nx - 4;
     if (is_sweep(kind)) {

@@ -1,6 +1,7 @@
-// dg_sweep_impl.cuh -- the production step kernel: one launch per
-// compute_step (deep-green src/rs/src/physics.rs:595-681) with fused
-// arithmetic (the "fast" policy), in FP32 on packed pairs or in FP64.
+// dg_sweep_impl.cuh -- the production step kernel of compute_step
+// (deep-green src/rs/src/physics.rs:595-681) with fused arithmetic (the
+// "fast" policy), in FP32 on packed pairs or in FP64: one launch per step,
+// or two (interior tiles, frame) on grids with interior tiles.
 //
 // Decomposition.  A block owns a tile of TY rows (y) x 64 columns (z) of
 // cells and marches along x through a chunk of planes.  Each plane arrives by
@@ -465,20 +466,25 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
     // run of code interleaves its long dependency chain (loads, reciprocal,
     // square roots) with the slopes and the prediction of plane m.
     // ---------------------------------------------------------------------
+    //
+    // IN: the tile is interior (InteriorTiles): every row and column is
+    // valid and no y or z face, ghost image or halo rule touches it, so the
+    // boundary switches below are compile-time constants.
+    template <bool IN>
     static __device__ void run_owned(Sm &s, const GridArgs<T> &a, const Tile &t, int r, int lane, T &smax) {
         const unsigned full = 0xffffffffu;
         const K<T> &k = t.k;
         const int col = 2 + 2 * lane;
-        const bool active = r < t.vy;
+        const bool active = IN || r < t.vy;
         const int y = t.y0 + r, z = t.z0 + 2 * lane;
-        const bool val0 = 2 * lane < t.vz, val1 = 2 * lane + 1 < t.vz;
-        const bool edge = lane == t.e;
-        const bool edge_even = edge && !t.odd;
-        const bool yout = r == 0 && t.ylo == kOut;
-        const bool zout = lane == 0 && t.zlo == kOut;
-        const bool zheat = lane == 0 && t.zlo == kWallM && (a.heat & 4);
-        const bool img_y = y <= 3 || y >= a.ny - 4;
-        const bool img_z = z <= 3 || z + 1 >= a.nz - 4;
+        const bool val0 = IN || 2 * lane < t.vz, val1 = IN || 2 * lane + 1 < t.vz;
+        const bool edge = IN ? lane == kTileZ / 2 - 1 : lane == t.e;
+        const bool edge_even = edge && (IN || !t.odd);
+        const bool yout = !IN && r == 0 && t.ylo == kOut;
+        const bool zout = !IN && lane == 0 && t.zlo == kOut;
+        const bool zheat = !IN && lane == 0 && t.zlo == kWallM && (a.heat & 4);
+        const bool img_y = !IN && (y <= 3 || y >= a.ny - 4);
+        const bool img_z = !IN && (z <= 3 || z + 1 >= a.nz - 4);
         // carried along the march: lox, the lower state of the x face ahead
         // (xt + s/2 of the previous plane); acc, the previous plane's flux
         // balance so far; tu, the update term of the plane before it.  The
@@ -515,7 +521,7 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
         const bool even_z = ((a.nz - 4) & 1) == 0 && a.nz - 4 >= 4;   // (width 2: both faces on one pair)
         int zt = -1, zc0 = 0, zc1 = 1;
         bool zflip = false;
-        if (even_z && val1) {
+        if (!IN && even_z && val1) {
             if (z == 2) {
                 if (a.bc[4] == kPeriodic) { zt = a.nz - 2; }
                 else if (a.bc[4] == kOutflow) { zt = 0; zc1 = 0; }
@@ -665,7 +671,7 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
                     half_step(xt, sy, 1.0, st);
 #pragma unroll
                     for (int f = 0; f < 5; ++f) stv(&s.ypl[pm][r + 1][f][2 * lane], st[f]);
-                    if (r == t.vy - 1 && t.yhi != kNormal) {
+                    if (!IN && r == t.vy - 1 && t.yhi != kNormal) {
                         // for the face above the top row (computed by warp B)
                         if (t.yhi == kOut) half_step(xt, sy, -1.0, st);
 #pragma unroll
@@ -676,7 +682,7 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
 #pragma unroll
                         for (int f = 0; f < 5; ++f) {
                             s.zeu[pm][r][f] = xt[f].y + sz[f].y;
-                            s.zex[pm][r][f] = t.zhi == kOut ? xt[f].y - sz[f].y : xt[f].y;
+                            s.zex[pm][r][f] = (!IN && t.zhi == kOut) ? xt[f].y - sz[f].y : xt[f].y;
                         }
                     }
                 }
@@ -693,7 +699,7 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
                 V lo[5], up[5], fyv[5];
 #pragma unroll
                 for (int f = 0; f < 5; ++f) lo[f] = ldv(&s.ypl[pm][r][f][2 * lane]);
-                if (r == 0 && t.ylo == kWallM) {
+                if (!IN && r == 0 && t.ylo == kWallM) {
                     // wall ghost row: mirrored prediction of this row + its own half slope
 #pragma unroll
                     for (int f = 0; f < 5; ++f) lo[f] = vadd(lo[f], mirror(xt[f], f == 2));
@@ -705,7 +711,7 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
                     stv(&s.fy[pm][r][f][2 * lane], fyv[f]);
                     dy[f] = vmul(fyv[f], spl<V>(-1.0));
                 }
-                if (r == 0 && t.ylo == kWallM && (a.heat & 2)) {
+                if (!IN && r == 0 && t.ylo == kWallM && (a.heat & 2)) {
                     // conducting lower y face (the ghost row mirrors row 2)
                     dy[4].x -= heat4(xt[0].x, xt[4].x, k);
                     dy[4].y -= heat4(xt[0].y, xt[4].y, k);
@@ -723,14 +729,14 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
                 // and, for an odd width, by the edge lane)
                 const T mx = f == 3 ? -xt[f].x : xt[f].x;   // wall mirror of the pair's first cell
                 T zlv = s.zl[pm][r][f];
-                if (t.zlo == kWallM) zlv += mx;
+                if (!IN && t.zlo == kWallM) zlv += mx;
                 T zrv = s.zr[pm][r][f];
-                if (t.zhi == kWallM) zrv += mx;
-                if (t.zhi == kOut) zrv = L.x;
+                if (!IN && t.zhi == kWallM) zrv += mx;
+                if (!IN && t.zhi == kOut) zrv = L.x;
                 const T left = __shfl_up_sync(full, U.y, 1);
                 lo[f] = mk(lane == 0 ? zlv : left, U.x);
                 // odd width: the edge lane's second cell is the right ghost column
-                up[f] = mk(L.x, edge && t.odd ? zrv : L.y);
+                up[f] = mk(L.x, !IN && edge && t.odd ? zrv : L.y);
             }
             face<3, GRAV>(lo, up, t.gh, k, fzv);
 #pragma unroll
@@ -981,6 +987,7 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
     // partial result goes to a.part[part_idx]; the last of the grid's
     // nparts items reduces them (next dt).  Returns false after a
     // device-side wait timed out (status flag set).
+    template <bool IN>
     static __device__ bool run_tile(const GridArgs<T> &a, const CUtensorMap *tmap, int tz, int ty, int cx, int chunk,
                                     int part_idx, int nparts, unsigned char *raw) {
         Sm &s = *reinterpret_cast<Sm *>(raw);
@@ -1046,7 +1053,7 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
         }
         T smax = T(0);
         int issued = 0;
-        if (warp < TY) run_owned(s, a, t, warp, lane, smax);
+        if (warp < TY) run_owned<IN>(s, a, t, warp, lane, smax);
         else if (warp == WA) issued = run_a(s, a, tmap, t, lane);
         else run_b(s, a, t, lane);
         __syncthreads();
@@ -1092,18 +1099,37 @@ template <int TY> constexpr int sweep_max_regs() {
     return r > 255 ? 255 : r;
 }
 
-template <class T, int TY, int R, int LIM, bool GRAV>
+// One step's interior launch (IN: one block per interior tile, marching
+// all of x) or frame launch (blocks: frame tiles x chunks), InteriorTiles.
+// The two touch disjoint tiles of the output and read only the input state,
+// so the frame launch may run beside the interior one (programmatic
+// dependent launch, launch_sweep).  They share one reduction: the interior
+// blocks hold partials [0, n_in), the frame blocks the rest, and whichever
+// block of either takes the last ticket advances dt (every block has read
+// the step's dt by then).  Without interior tiles the frame launch is the
+// whole step (n_in = 0).
+template <class T, int TY, int R, int LIM, bool GRAV, bool IN>
 __global__ void __maxnreg__(sweep_max_regs<TY>()) sweep_step_kernel(const GridArgs<T> a,
                                                                       const __grid_constant__ CUtensorMap tmap,
-                                                                      int chunk) {
+                                                                      int chunk, int n_in, int nparts) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    const int tiles_z = (a.nz - 4 + kTileZ - 1) / kTileZ;
-    const int tiles_y = (a.ny - 4 + TY - 1) / TY;
-    int b = blockIdx.x;
-    const int tz = b % tiles_z;
-    b /= tiles_z;
-    const int ty = b % tiles_y;
-    Sweep<T, TY, R, LIM, GRAV>::run_tile(a, &tmap, tz, ty, b / tiles_y, chunk, blockIdx.x, gridDim.x, smem_raw);
+    // the frame launch reads nothing this launch writes: let it start on the
+    // SMs this launch leaves free
+    if constexpr (IN) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    const InteriorTiles it(a.ny, a.nz, TY, kTileZ);
+    int b = blockIdx.x, ty, tz;
+    if constexpr (IN) {
+        tz = 1 + b % it.nz;
+        ty = 1 + b / it.nz;
+        b = 0;
+        chunk = a.nx - 4;
+    } else {
+        const int nf = it.frame();
+        it.frame_tile(b % nf, ty, tz);
+        b /= nf;
+    }
+    const int part = IN ? (int)blockIdx.x : n_in + (int)blockIdx.x;
+    Sweep<T, TY, R, LIM, GRAV>::template run_tile<IN>(a, &tmap, tz, ty, b, chunk, part, nparts, smem_raw);
 }
 
 // Batched step: one persistent launch advances many independent grids by
@@ -1137,7 +1163,7 @@ __global__ void __maxnreg__(sweep_max_regs<TY>()) sweep_batch_kernel(const GridA
             reinterpret_cast<int *>(&s_args)[i] = reinterpret_cast<const int *>(&args[bi.g])[i];
         __syncthreads();
         const GridArgs<float> ga = s_args;
-        const bool ok = Sweep<float, TY, R, LIM, GRAV>::run_tile(ga, &maps[bi.g], bi.tz, bi.ty, bi.cx, chunk,
+        const bool ok = Sweep<float, TY, R, LIM, GRAV>::template run_tile<false>(ga, &maps[bi.g], bi.tz, bi.ty, bi.cx, chunk,
                                                                  bi.local, ga.nparts, smem_raw);
         __syncthreads();
         if (!ok) return;

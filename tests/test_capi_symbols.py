@@ -117,9 +117,12 @@ def test_bench_traffic_figure_belongs_to_the_benchmarked_kernel():
     import bench
     d = json.loads((Path(__file__).resolve().parent.parent / "profiles" / "step_traffic.json").read_text())
     assert d["kernel"] == bench.STEP_KERNEL
-    assert 40 <= d["dram_bytes_per_cell"] < 60
-    assert bench.ncu_traffic_per_launch(bench.STEP_KERNEL, 512) == d["dram_bytes_per_cell"] * 512 ** 3
-    assert bench.ncu_traffic_per_launch("another kernel", 512) is None
+    assert 40 <= d["interior_bytes_per_cell"] < 60 and 40 <= d["frame_bytes_per_cell"] < 70
+    interior = 35 * 14 * 6 * 64 * 512          # 512^3: 35 x 6 interior tiles
+    want = d["interior_bytes_per_cell"] * interior + d["frame_bytes_per_cell"] * (512 ** 3 - interior)
+    assert bench.ncu_traffic_per_step(bench.STEP_KERNEL, 512) == want
+    assert bench.step_launches(512) == 2 and bench.step_launches(128) == 1
+    assert bench.ncu_traffic_per_step("another kernel", 512) is None
 
 
 def test_resolution_norm_scales_only_the_output_scale():
