@@ -162,10 +162,16 @@ int32_t dg_get_dts(dg_ctx *ctx, int32_t nsteps, double *dts);
 int32_t dg_synchronize(dg_ctx *ctx);
 /* The cudaStream_t the context launches on, as void*. */
 int32_t dg_get_stream(dg_ctx *ctx, void **stream);
-/* The grid of the step kernel (blocks, threads per block, x-planes per
- * block); one step is one launch of it.  Any pointer may be NULL. */
+/* The step's blocks (all launches of one step together), threads per
+ * block and x-planes per block.  The production kernel steps a grid that
+ * has interior tiles (full tiles two cells clear of every y and z face) in
+ * two launches: one block per interior tile marching all of x, then the
+ * other tiles in blocks of `chunk` x-planes; otherwise one launch of
+ * `chunk`-plane blocks.  Any pointer may be NULL. */
 int32_t dg_step_launch_shape(dg_ctx *ctx, int32_t *blocks, int32_t *threads, int32_t *chunk);
-/* Override the x-planes per block of the step kernel (0 = automatic). */
+/* Override the x-planes per block of the step kernel (0 = automatic; for
+ * the production kernel on a grid with interior tiles, of the blocks along
+ * the faces). */
 int32_t dg_set_chunk(dg_ctx *ctx, int32_t chunk);
 
 /* The dt the next compute_step will take (calc_timestep, physics.rs:177, of
