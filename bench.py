@@ -333,11 +333,12 @@ STEP_KERNEL = ("dg::sweep::sweep_step_kernel<float, 14, 4, 1, false, true> + "
                "dg::sweep::sweep_step_kernel<float, 14, 4, 1, false, false>")
 
 
-def step_launches(n):
-    """Launches per step of the sweep on an n^3 grid: two with interior tiles
-    (full 14 x 64 tiles two cells clear of every y and z face), else one."""
-    ny_in = (n - 2) // 14 - 1
-    nz_in = (n - 2) // 64 - 1
+def step_launches(n, ny=None, nz=None):
+    """Launches per step of the FP32 sweep on an n x ny x nz grid (ny, nz
+    default to n): two with interior tiles (full 14 x 64 tiles two cells
+    clear of every y and z face), else one."""
+    ny_in = ((n if ny is None else ny) - 2) // 14 - 1
+    nz_in = ((n if nz is None else nz) - 2) // 64 - 1
     return 2 if ny_in > 0 and nz_in > 0 else 1
 
 
@@ -955,7 +956,7 @@ def run_refcuda(args, world, rank, local):
         "speedup_device": value / ref["gcups"], "speedup_host_loop": loop_value / ref["gcups"],
         "parity_step1": {"rel_l1": errs, "max": max(errs.values()), "dt_rel": abs(dt1 - ref_dt1) / ref_dt1,
                          "region": "interior minus the first layer at each wall"},
-        "clocks": clocks, "gpu_launches": args.steps,
+        "clocks": clocks, "gpu_launches": step_launches(*interior) * args.steps,
     }
     print(json.dumps(line), flush=True)
 
