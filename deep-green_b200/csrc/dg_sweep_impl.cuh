@@ -486,13 +486,15 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
         const bool img_y = !IN && (y <= 3 || y >= a.ny - 4);
         const bool img_z = !IN && (z <= 3 || z + 1 >= a.nz - 4);
         // carried along the march: lox, the lower state of the x face ahead
-        // (xt + s/2 of the previous plane); acc, the previous plane's flux
-        // balance so far; tu, the update term of the plane before it.  The
-        // own cell's primitives of the current and the previous plane are
-        // read back from the primitive buffer.
-        V lox[5], acc[5], tu[5];
+        // (xt + s/2 of the previous plane); nacc, the previous plane's flux
+        // balance so far, negated (its lower faces' fluxes enter with a plus
+        // sign, so no flux is negated on its own; negation being exact, the
+        // sums round as the balance itself would); tu, the update term of the
+        // plane before it.  The own cell's primitives of the current and the
+        // previous plane are read back from the primitive buffer.
+        V lox[5], nacc[5], tu[5];
 #pragma unroll
-        for (int f = 0; f < 5; ++f) lox[f] = acc[f] = tu[f] = spl<V>(0.0);
+        for (int f = 0; f < 5; ++f) lox[f] = nacc[f] = tu[f] = spl<V>(0.0);
 
         // Update of plane xu (staged index sl_idx) with the term tu: the new
         // state and its wave speeds (stores are left to the caller).
@@ -609,8 +611,8 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
                         face<1, false>(lox, up, spl<V>(0.0), k, fx);
 #pragma unroll
                         for (int f = 0; f < 5; ++f) {
-                            tu[f] = vadd(acc[f], fx[f]);
-                            acc[f] = vmul(fx[f], spl<V>(-1.0));
+                            tu[f] = vsub(fx[f], nacc[f]);
+                            nacc[f] = fx[f];
                         }
                     }
                 } else {
@@ -652,14 +654,14 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
                         const bool xo = m == 2 && a.bc[0] == kOutflow;
     #pragma unroll
                         for (int f = 0; f < 5; ++f) {
-                            tu[f] = xo_prev ? acc[f] : vadd(acc[f], fx[f]);
-                            acc[f] = xo ? spl<V>(0.0) : vmul(fx[f], spl<V>(-1.0));
+                            tu[f] = xo_prev ? vmul(nacc[f], spl<V>(-1.0)) : vsub(fx[f], nacc[f]);
+                            nacc[f] = xo ? spl<V>(0.0) : fx[f];
                         }
                         if (m == 2 && (a.heat & 1)) {
                             // conducting lower x face: its heat enters plane 2
                             // (the ghost plane's state mirrors plane 2's)
-                            acc[4].x -= heat4(xt[0].x, xt[4].x, k);
-                            acc[4].y -= heat4(xt[0].y, xt[4].y, k);
+                            nacc[4].x += heat4(xt[0].x, xt[4].x, k);
+                            nacc[4].y += heat4(xt[0].y, xt[4].y, k);
                         }
                     }
                 }
@@ -694,7 +696,7 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
             if (!active || !upd) continue;
             // ================= after the barrier: y and z faces of plane m
             const V *xt = xtc;
-            V dy[5];
+            V ndy[5];   // the lower y face's flux (plus the heat of a conducting face)
             if (!yout) {
                 V lo[5], up[5], fyv[5];
 #pragma unroll
@@ -709,16 +711,16 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
 #pragma unroll
                 for (int f = 0; f < 5; ++f) {
                     stv(&s.fy[pm][r][f][2 * lane], fyv[f]);
-                    dy[f] = vmul(fyv[f], spl<V>(-1.0));
+                    ndy[f] = fyv[f];
                 }
                 if (!IN && r == 0 && t.ylo == kWallM && (a.heat & 2)) {
                     // conducting lower y face (the ghost row mirrors row 2)
-                    dy[4].x -= heat4(xt[0].x, xt[4].x, k);
-                    dy[4].y -= heat4(xt[0].y, xt[4].y, k);
+                    ndy[4].x += heat4(xt[0].x, xt[4].x, k);
+                    ndy[4].y += heat4(xt[0].y, xt[4].y, k);
                 }
             } else {
 #pragma unroll
-                for (int f = 0; f < 5; ++f) dy[f] = spl<V>(0.0);
+                for (int f = 0; f < 5; ++f) ndy[f] = spl<V>(0.0);
             }
             V lo[5], up[5], fzv[5];
 #pragma unroll
@@ -747,7 +749,7 @@ template <class T, int TY, int R, int LIM, bool GRAV> struct Sweep {
                 if (zout) dz.x = T(0);
                 // conducting lower z face: the heat of the first column
                 if (f == 4 && zheat) dz.x -= heat4(xt[0].x, xt[4].x, k);
-                acc[f] = vadd(acc[f], vadd(dy[f], dz));
+                nacc[f] = vadd(nacc[f], vsub(ndy[f], dz));
             }
         }
         // the last plane of the chunk: its fluxes arrived with the last barrier
