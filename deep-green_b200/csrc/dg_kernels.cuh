@@ -149,15 +149,24 @@ struct InteriorTiles {
     }
 };
 
+// x-planes per block of a sweep step's interior launch: whole columns when
+// the interior tiles alone fill the SMs at least once (the frame's shorter
+// blocks then fill the interior launch's last wave), else the frame's chunk
+// (a few long blocks would leave most SMs idle).
+inline int interior_chunk(int nx, const InteriorTiles &it, int chunk) {
+    return it.interior() >= kSms ? nx - 4 : chunk;
+}
+
 // Blocks of one step: (y tiles) x (z tiles) x (x chunks of `chunk` planes);
-// for a sweep step with interior tiles, one block per interior tile plus the
-// frame tiles x chunks (both launches together).
+// for a sweep step with interior tiles, the interior tiles x their chunks
+// (interior_chunk) plus the frame tiles x chunks (both launches together).
 inline int step_grid_blocks(int nx, int ny, int nz, int kind, int chunk) {
     const int ty = step_tile_rows(kind), tzc = step_tile_cols(kind);
     const int chunks = (nx - 4 + chunk - 1) / chunk;
     if (is_sweep(kind)) {
         const InteriorTiles it(ny, nz, ty, tzc);
-        return it.interior() + it.frame() * chunks;
+        const int ci = interior_chunk(nx, it, chunk);
+        return it.interior() * ((nx - 4 + ci - 1) / ci) + it.frame() * chunks;
     }
     const int tiles_z = (nz - 4 + tzc - 1) / tzc;
     const int tiles_y = (ny - 4 + ty - 1) / ty;
@@ -172,10 +181,11 @@ inline int step_grid_blocks(int nx, int ny, int nz, int kind, int chunk) {
 // (planes per block + 3 re-staged), with at least 24 planes per block.
 inline int choose_chunk(int nx, int ny, int nz, int kind) {
     const int ty = step_tile_rows(kind), tzc = step_tile_cols(kind);
-    // sweep steps with interior tiles: the frame's blocks fill the SMs the
-    // interior launch leaves free, in short chunks (32-64 planes measured
-    // 38.2-38.6 GCUPS on 512^3 Sod, whole columns 34.1-34.4)
-    if (is_sweep(kind) && InteriorTiles(ny, nz, ty, tzc).interior() > 0) return nx - 4 < 64 ? nx - 4 : 64;
+    // sweep steps whose interior tiles fill the SMs (interior_chunk): the
+    // frame's blocks fill the interior launch's last wave, in short chunks
+    // (32-64 planes measured 38.2-38.6 GCUPS on 512^3 Sod, whole columns
+    // 34.1-34.4)
+    if (is_sweep(kind) && InteriorTiles(ny, nz, ty, tzc).interior() >= kSms) return nx - 4 < 64 ? nx - 4 : 64;
     const long long tiles = (long long)((ny - 4 + ty - 1) / ty) * ((nz - 4 + tzc - 1) / tzc);
     const int nxi = nx - 4;
     if (is_sweep(kind)) {

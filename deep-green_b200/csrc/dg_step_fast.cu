@@ -19,9 +19,10 @@ template <> struct SweepCfg<double> {
 };
 
 // One step: with interior tiles (InteriorTiles) two launches sharing one
-// reduction -- the interior tiles, one block per tile marching all of x,
-// with the owned warps' boundary switches compiled out (10 % faster than the
-// general loop), then the frame in `chunk`-plane blocks, launched as a
+// reduction -- the interior tiles, with the owned warps' boundary switches
+// compiled out (419 instead of 594 instructions per cell), in whole columns
+// when they fill the SMs and else in `chunk`-plane blocks
+// (interior_chunk), then the frame in `chunk`-plane blocks, launched as a
 // programmatic dependent so that it fills the SMs the interior launch's last
 // wave leaves free.  Without interior tiles, one launch of the general
 // kernel over all tiles.  (One kernel body holding both variants of the
@@ -37,14 +38,15 @@ cudaError_t launch_sweep_t(const GridArgs<T> &a, const CUtensorMap *tmap, int ch
     if (e == cudaSuccess) e = ensure_dynamic_smem(k_frame, smem, attr_frame);
     if (e != cudaSuccess) return e;
     const InteriorTiles it(a.ny, a.nz, TY, sweep::kTileZ);
-    const int n_in = it.interior();
+    const int chunk_in = interior_chunk(a.nx, it, chunk);
+    const int n_in = it.interior() * ((a.nx - 4 + chunk_in - 1) / chunk_in);
     const int n_fr = it.frame() * ((a.nx - 4 + chunk - 1) / chunk);
     const int nparts = n_in + n_fr;   // = step_grid_blocks(): the partials' bound
     if (n_in == 0) {
         k_frame<<<n_fr, 32 * (TY + 2), smem, st>>>(a, *tmap, chunk, 0, nparts);
         return cudaGetLastError();
     }
-    k_in<<<n_in, 32 * (TY + 2), smem, st>>>(a, *tmap, chunk, n_in, nparts);
+    k_in<<<n_in, 32 * (TY + 2), smem, st>>>(a, *tmap, chunk_in, n_in, nparts);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};

@@ -1101,8 +1101,9 @@ template <int TY> constexpr int sweep_max_regs() {
     return r > 255 ? 255 : r;
 }
 
-// One step's interior launch (IN: one block per interior tile, marching
-// all of x) or frame launch (blocks: frame tiles x chunks), InteriorTiles.
+// One step's interior launch (IN; blocks: interior tiles x chunks, whole
+// columns when they fill the SMs: interior_chunk) or frame launch (blocks:
+// frame tiles x chunks), InteriorTiles.
 // The two touch disjoint tiles of the output and read only the input state,
 // so the frame launch may run beside the interior one (programmatic
 // dependent launch, launch_sweep).  They share one reduction: the interior
@@ -1122,9 +1123,9 @@ __global__ void __maxnreg__(sweep_max_regs<TY>()) sweep_step_kernel(const GridAr
     int b = blockIdx.x, ty, tz;
     if constexpr (IN) {
         tz = 1 + b % it.nz;
-        ty = 1 + b / it.nz;
-        b = 0;
-        chunk = a.nx - 4;
+        b /= it.nz;
+        ty = 1 + b % it.ny;
+        b /= it.ny;
     } else {
         const int nf = it.frame();
         it.frame_tile(b % nf, ty, tz);
